@@ -1,0 +1,620 @@
+// The Green-function action y = (H - E S) x on sm_100a.
+//
+//  * local part (potential V - E and the finite-difference kinetic energy) in ONE pass:
+//    local_fused_kernel walks the z-lines of cubes of one source column block, keeps the
+//    z-stencil window in registers and stages the current cube and its four x/y neighbour
+//    cubes in shared memory, so y is written exactly once per block (the reference makes
+//    four passes that re-read and re-write y, include/green_action.hxx:159-167).
+//    Plans with a 17-point stencil in some direction use the generic per-direction kernels.
+//  * dyadic part (PAW projectors): projection, atom-matrix multiply, addition
+//    (include/green_dyadic.hxx:856-922), with the image/atom coefficient scratch owned by
+//    the plan instead of being allocated on every call.
+#include "device.cuh"
+
+#include <algorithm>
+
+namespace a43g {
+
+namespace {
+
+constexpr int kBlockReals = 8192;   // 2 x 64 x 64
+
+template <typename T>
+struct Stencil9 { T c[3][5]; };      // per direction, c[0] centre ... c[4] distance 4
+
+template <typename T>
+Stencil9<T> make_stencil9(DevicePlan const &dp) {
+    // 8th-order second derivative {-14350, 8064, -1008, 128, -9}/5040 times -1/(2h^2),
+    // formed in double and rounded to real_t as include/green_kinetic.hxx:37-42 does
+    Stencil9<T> s;
+    double const w[5] = {-14350, 8064, -1008, 128, -9};
+    for (int d = 0; d < 3; ++d) {
+        double const norm = dp.prefactor[d]/5040.;
+        for (int k = 0; k < 5; ++k) s.c[d][k] = T(w[k]*norm);
+        if (dp.FD_range[d] < 1) for (int k = 0; k < 5; ++k) s.c[d][k] = T(0);
+    }
+    return s;
+}
+
+template <typename T>
+struct LocalArgs {
+    Stencil9<T> st;
+    T E_re, E_im;
+    T ph[3][2][2];                   // Bloch phases [dd][left,right][re,im]
+};
+
+// load the 4 points (z = 0..3) at cross-section position yx and column col of a neighbour
+// cube (encoded e), optionally rotated by a phase
+template <typename T>
+__device__ __forceinline__ void load_zcol(T const *__restrict__ x, int32_t e, T pr, T pi,
+                                          int yx, int col, T (&re)[4], T (&im)[4]) {
+    if (-1 == e) {
+#pragma unroll
+        for (int z = 0; z < 4; ++z) { re[z] = T(0); im[z] = T(0); }
+        return;
+    }
+    T const *b = x + size_t(nbr_block(e))*kBlockReals + yx*64 + col;
+#pragma unroll
+    for (int z = 0; z < 4; ++z) { re[z] = __ldg(b + z*16*64); im[z] = __ldg(b + 4096 + z*16*64); }
+    if (e < -1) {
+#pragma unroll
+        for (int z = 0; z < 4; ++z) {
+            T const r = pr*re[z] - pi*im[z], i = pr*im[z] + pi*re[z];
+            re[z] = r; im[z] = i;
+        }
+    }
+}
+
+// list entry (inzb+1, 0, -(inzb+1)) to neighbour code (>= 0 plain, -1 zero, <= -2 phase)
+__device__ __forceinline__ int32_t list_code(int32_t entry) {
+    return (entry > 0) ? entry - 1 : ((entry < 0) ? -(-entry - 1) - 2 : -1);
+}
+
+// One CTA per (z-line, column slice of S columns); thread (j, y, x) owns the 4 points of its
+// (y, x) column in every cube of the line for column j of the slice, both real and imaginary.
+template <typename T, int S>
+__global__ void __launch_bounds__(S*16)
+local_fused_kernel(T *__restrict__ y, T const *__restrict__ x,
+                   uint32_t const *__restrict__ zstart, int32_t const *__restrict__ zlist,
+                   int32_t const *__restrict__ nbr, int32_t const *__restrict__ veff,
+                   T const *__restrict__ Vcell, LocalArgs<T> const a)
+{
+    constexpr int NSL = 64/S;
+    __shared__ T sm[5][2][64][S];    // slots: own cube, x-, x+, y-, y+
+    int const line = blockIdx.x/NSL, slice = blockIdx.x % NSL;
+    int const j = threadIdx.x % S, yx = threadIdx.x/S;
+    int const xq = yx & 3, yq = yx >> 2, col = slice*S + j;
+    int32_t const *L = zlist + zstart[line];
+    int n = 0;
+    while (L[4 + n] > 0) ++n;        // lists end with 4 non-positive entries
+
+    T pre[4], pim[4], cre[4], cim[4], nre[4], nim[4];
+    load_zcol(x, list_code(L[3]), a.ph[2][0][0], a.ph[2][0][1], yx, col, pre, pim);
+    load_zcol(x, L[4] - 1, T(0), T(0), yx, col, cre, cim);
+    T const (&cx)[5] = a.st.c[0];
+    T const (&cy)[5] = a.st.c[1];
+    T const (&cz)[5] = a.st.c[2];
+
+    for (int k = 0; k < n; ++k) {
+        int32_t const b = L[4 + k] - 1;
+        load_zcol(x, list_code(L[5 + k]), a.ph[2][1][0], a.ph[2][1][1], yx, col, nre, nim);
+        int32_t const *nb = nbr + 6*size_t(b);
+        int32_t const e[4] = {nb[0], nb[1], nb[2], nb[3]};
+        __syncthreads();             // previous step finished reading the slots
+#pragma unroll
+        for (int z = 0; z < 4; ++z) { sm[0][0][z*16 + yx][j] = cre[z]; sm[0][1][z*16 + yx][j] = cim[z]; }
+#pragma unroll
+        for (int s = 0; s < 4; ++s) {
+            T tr[4], ti[4];
+            int const dd = s >> 1, side = s & 1;
+            load_zcol(x, e[s], a.ph[dd][side][0], a.ph[dd][side][1], yx, col, tr, ti);
+#pragma unroll
+            for (int z = 0; z < 4; ++z) { sm[1 + s][0][z*16 + yx][j] = tr[z]; sm[1 + s][1][z*16 + yx][j] = ti[z]; }
+        }
+        __syncthreads();
+        int32_t const iloc = veff[b];
+        T *yb = y + size_t(b)*kBlockReals + yx*64 + col;
+#pragma unroll
+        for (int z = 0; z < 4; ++z) {
+            int const i64 = z*16 + yx;
+            T const Vt = ((iloc < 0) ? T(0) : Vcell[size_t(iloc)*64 + i64]) - a.E_re;
+            T accr = Vt*cre[z] + a.E_im*cim[z];
+            T acci = Vt*cim[z] - a.E_im*cre[z];
+            // z direction: window prev | cur | next held in registers
+            accr += cz[0]*cre[z]; acci += cz[0]*cim[z];
+#pragma unroll
+            for (int d = 1; d <= 4; ++d) {
+                int const qm = z - d, qp = z + d;
+                T const mr = (qm < 0) ? pre[qm + 4] : cre[qm], mi = (qm < 0) ? pim[qm + 4] : cim[qm];
+                T const pr = (qp > 3) ? nre[qp - 4] : cre[qp], pi = (qp > 3) ? nim[qp - 4] : cim[qp];
+                accr += cz[d]*(mr + pr); acci += cz[d]*(mi + pi);
+            }
+            // x and y directions from shared memory
+            accr += (cx[0] + cy[0])*cre[z]; acci += (cx[0] + cy[0])*cim[z];
+#pragma unroll
+            for (int d = 1; d <= 4; ++d) {
+                int const xm = xq - d, xp = xq + d, ym = yq - d, yp = yq + d;
+                int const sxm = (xm < 0) ? 1 : 0, sxp = (xp > 3) ? 2 : 0;
+                int const sym = (ym < 0) ? 3 : 0, syp = (yp > 3) ? 4 : 0;
+                int const ixm = z*16 + yq*4 + (xm & 3), ixp = z*16 + yq*4 + (xp & 3);
+                int const iym = z*16 + (ym & 3)*4 + xq, iyp = z*16 + (yp & 3)*4 + xq;
+                accr += cx[d]*(sm[sxm][0][ixm][j] + sm[sxp][0][ixp][j]) + cy[d]*(sm[sym][0][iym][j] + sm[syp][0][iyp][j]);
+                acci += cx[d]*(sm[sxm][1][ixm][j] + sm[sxp][1][ixp][j]) + cy[d]*(sm[sym][1][iym][j] + sm[syp][1][iyp][j]);
+            }
+            yb[z*16*64] = accr;
+            yb[4096 + z*16*64] = acci;
+        }
+#pragma unroll
+        for (int z = 0; z < 4; ++z) { pre[z] = cre[z]; pim[z] = cim[z]; cre[z] = nre[z]; cim[z] = nim[z]; }
+    }
+}
+
+// ---------------------------------------------------------------- generic local path
+
+// y = (V - E) x for every block (include/green_potential.hxx:15-139, collinear)
+template <typename T>
+__global__ void __launch_bounds__(256)
+potential_kernel(T *__restrict__ y, T const *__restrict__ x, int32_t const *__restrict__ veff,
+                 T const *__restrict__ Vcell, uint32_t nnzb, T Er, T Ei)
+{
+    for (uint32_t b = blockIdx.x; b < nnzb; b += gridDim.x) {
+        int32_t const iloc = veff[b];
+        T const *xb = x + size_t(b)*kBlockReals;
+        T *yb = y + size_t(b)*kBlockReals;
+        for (int t = threadIdx.x; t < 4096; t += blockDim.x) {
+            int const i = t >> 6;
+            T const Vt = ((iloc < 0) ? T(0) : Vcell[size_t(iloc)*64 + i]) - Er;
+            T const xr = xb[t], xi = xb[4096 + t];
+            yb[t] = Vt*xr + Ei*xi;
+            yb[4096 + t] = Vt*xi - Ei*xr;
+        }
+    }
+}
+
+// y += T_dd x along the lists of one direction; NH halo cubes (1: 9-point, 2: 17-point stencil).
+// One CTA per (list, cross-section row i16), 64 threads = columns, each for re and im.
+template <typename T>
+struct Coef17 { T c[9]; };
+
+template <typename T, int NH>
+__global__ void __launch_bounds__(64)
+kinetic_list_kernel(T *__restrict__ y, T const *__restrict__ x, uint32_t const *__restrict__ lstart,
+                    int32_t const *__restrict__ lists, int stride, Coef17<T> const coef,
+                    T plr, T pli, T prr, T pri)
+{
+    constexpr int W = 4*(2*NH + 1);   // window points: NH cubes left, current, NH right
+    constexpr int R = 4*NH;           // stencil reach in points
+    int const i16 = blockIdx.y, col = threadIdx.x;
+    int const base = (16 == stride) ? i16 : ((4 == stride) ? (16*(i16 >> 2) + (i16 & 3)) : 4*i16);
+    int32_t const *L = lists + lstart[blockIdx.x];
+    int n = 0;
+    while (L[4 + n] > 0) ++n;
+    T c[R + 1];
+#pragma unroll
+    for (int k = 0; k <= R; ++k) c[k] = coef.c[k];
+    T wr[W], wi[W];
+    // cube at list position p (0-based among the cubes), with halo handling at both ends
+    auto fetch = [&](int p, int slot) {
+        int32_t entry = 0; T pr = T(1), pi = T(0);
+        if (p >= 0 && p < n) entry = L[4 + p];
+        else if (1 == NH && -1 == p) { entry = L[3]; pr = plr; pi = pli; }
+        else if (1 == NH && n == p) { entry = L[4 + n]; pr = prr; pi = pri; }
+        if (0 == entry) {
+#pragma unroll
+            for (int i4 = 0; i4 < 4; ++i4) { wr[slot*4 + i4] = T(0); wi[slot*4 + i4] = T(0); }
+            return;
+        }
+        int32_t const b = (entry > 0) ? entry - 1 : -entry - 1;
+        T const *xb = x + size_t(b)*kBlockReals + base*64 + col;
+#pragma unroll
+        for (int i4 = 0; i4 < 4; ++i4) {
+            T const r = xb[i4*stride*64], i = xb[4096 + i4*stride*64];
+            if (entry < 0) { wr[slot*4 + i4] = pr*r - pi*i; wi[slot*4 + i4] = pr*i + pi*r; }
+            else { wr[slot*4 + i4] = r; wi[slot*4 + i4] = i; }
+        }
+    };
+#pragma unroll
+    for (int s = 0; s < 2*NH + 1; ++s) fetch(s - NH, s);
+    for (int k = 0; k < n; ++k) {
+        int32_t const b = L[4 + k] - 1;
+        T *yb = y + size_t(b)*kBlockReals + base*64 + col;
+#pragma unroll
+        for (int i4 = 0; i4 < 4; ++i4) {
+            int const p = 4*NH + i4;
+            T sr = c[0]*wr[p], si = c[0]*wi[p];
+#pragma unroll
+            for (int d = 1; d <= R; ++d) { sr += c[d]*(wr[p - d] + wr[p + d]); si += c[d]*(wi[p - d] + wi[p + d]); }
+            yb[i4*stride*64] += sr;
+            yb[4096 + i4*stride*64] += si;
+        }
+#pragma unroll
+        for (int q = 0; q < W - 4; ++q) { wr[q] = wr[q + 4]; wi[q] = wi[q + 4]; }
+        fetch(k + 1 + NH, 2*NH);
+    }
+}
+
+// ---------------------------------------------------------------- dyadic part
+
+__host__ __device__ constexpr int nsho_c(int L) { return ((L + 1)*(L + 2)*(L + 3))/6; }
+__host__ __device__ constexpr int n2ho_c(int L) { return ((L + 1)*(L + 2))/2; }
+
+// 1D Hermite-Gauss tables of one (atom image, target cube) pair, computed by 12 threads:
+// H0 = exp(-xi^2/2) inside the projection radius else 0, H_{n+1} = xi H_n - n/2 H_{n-1},
+// xi = ((cube*4 + i4 + 1/2) h - R)/sigma (include/green_dyadic.hxx:33-107); xi^2 also as
+// float for the spherical mask, which is evaluated in float exactly as the reference does.
+template <typename T, int LMAX>
+__device__ __forceinline__ void hermite_tables(T (*H)[3][4], float (*xi2)[4], int tid, int lmax,
+                                               double const *__restrict__ pos, float const *__restrict__ cube,
+                                               double const *__restrict__ grid) {
+    if (tid < 12) {
+        int const d = tid >> 2, i4 = tid & 3;
+        double const R2 = grid[3]*grid[3];
+        double const sinv = pos[3]*pos[3];
+        double const xi = sinv*((double(cube[d])*4 + i4 + 0.5)*grid[d] - pos[d]);
+        double const x2 = xi*xi;
+        xi2[d][i4] = float(x2);
+        double hm = 0, h = (x2 < R2) ? exp(-0.5*x2) : 0.0;
+        H[0][d][i4] = T(h);
+#pragma unroll
+        for (int nu = 0; nu < LMAX; ++nu) {
+            if (nu < lmax) {
+                double const hp = xi*h - 0.5*nu*hm;
+                H[nu + 1][d][i4] = T(hp);
+                hm = h; h = hp;
+            }
+        }
+    }
+}
+
+__device__ __forceinline__ bool in_mask(float const (*xi2)[4], float R2f, int x, int y, int z) {
+    float const d2z = xi2[2][z] - R2f;
+    float const d2yz = xi2[1][y] + d2z;
+    return (xi2[0][x] + d2yz) < 0.f;
+}
+
+
+// apc[(i0 + sho)*nrhs + s][reim][j] = sum over the blocks of source s near image a of the
+// masked projector functions times x (include/green_dyadic.hxx:112-288), for images whose
+// basis size is exactly L (the host launches one grid per distinct L).  Sum-factorized:
+// contract x, then y, then z.  Grid (images of this L, nrhs), 128 threads = (reim, column).
+template <typename T, int L>
+__global__ void __launch_bounds__(128)
+sho_project_kernel(T *__restrict__ apc, T const *__restrict__ x, uint32_t nrhs,
+                   uint32_t const *__restrict__ images, uint32_t nAI,
+                   uint32_t const *__restrict__ prj_start, uint32_t const *__restrict__ prj_col,
+                   uint64_t const *__restrict__ prj_coloff,
+                   double const *__restrict__ img_pos, uint32_t const *__restrict__ img_starts,
+                   uint32_t const *__restrict__ rowindx, float const *__restrict__ cubepos,
+                   double const *__restrict__ grid4)
+{
+    constexpr int NS = nsho_c(L), N2 = n2ho_c(L);
+    __shared__ T H[L + 1][3][4];
+    __shared__ float xi2[3][4];
+    __shared__ double grid[4];
+    uint32_t const a = images[blockIdx.x];
+    int const s = blockIdx.y, tid = threadIdx.x;
+    int const reim = tid >> 6, j = tid & 63;
+    if (tid < 4) grid[tid] = grid4[tid];
+    uint32_t const *start = prj_start + size_t(s)*(nAI + 1);
+    uint32_t const *cols = prj_col + prj_coloff[s];
+    float const R2f = float(grid4[3]*grid4[3]);
+    T acc[NS];
+#pragma unroll
+    for (int i = 0; i < NS; ++i) acc[i] = T(0);
+    for (uint32_t k = start[a]; k < start[a + 1]; ++k) {
+        uint32_t const b = cols[k];
+        __syncthreads();
+        hermite_tables<T, L>(H, xi2, tid, L, img_pos + 4*size_t(a), cubepos + 4*size_t(rowindx[b]), grid);
+        __syncthreads();
+        T const *xb = x + size_t(b)*kBlockReals + reim*4096 + j;
+        for (int z = 0; z < 4; ++z) {
+            float const d2z = xi2[2][z] - R2f;
+            if (!(d2z < 0.f)) continue;
+            T byx[N2];
+#pragma unroll
+            for (int i = 0; i < N2; ++i) byx[i] = T(0);
+            for (int yy = 0; yy < 4; ++yy) {
+                float const d2yz = xi2[1][yy] + d2z;
+                if (!(d2yz < 0.f)) continue;
+                T ax[L + 1];
+#pragma unroll
+                for (int i = 0; i <= L; ++i) ax[i] = T(0);
+#pragma unroll
+                for (int xx = 0; xx < 4; ++xx) {
+                    if (xi2[0][xx] + d2yz < 0.f) {
+                        T const ps = xb[((z*4 + yy)*4 + xx)*64];
+#pragma unroll
+                        for (int ix = 0; ix <= L; ++ix) ax[ix] += ps*H[ix][0][xx];
+                    }
+                }
+#pragma unroll
+                for (int iy = 0, iyx = 0; iy <= L; ++iy) {
+                    T const hy = H[iy][1][yy];
+#pragma unroll
+                    for (int ix = 0; ix <= L - iy; ++ix, ++iyx) byx[iyx] += ax[ix]*hy;
+                }
+            }
+#pragma unroll
+            for (int iz = 0, sho = 0; iz <= L; ++iz) {
+                T const hz = H[iz][2][z];
+#pragma unroll
+                for (int iy = 0, iyx = 0; iy <= L - iz; ++iy) {
+                    iyx = iy*(2*L + 3 - iy)/2;
+#pragma unroll
+                    for (int ix = 0; ix <= L - iz - iy; ++ix, ++sho) acc[sho] += byx[iyx + ix]*hz;
+                }
+            }
+        }
+    }
+    T *out = apc + (size_t(img_starts[a])*nrhs + s)*128 + reim*64 + j;
+#pragma unroll
+    for (int sho = 0; sho < NS; ++sho) out[size_t(sho)*nrhs*128] = acc[sho];
+}
+
+// aac[(a0 + c)*nrhs + s] = sum over the images i of atom A of phase_i * apc[(i0 + c)*nrhs + s]
+// (collect) in double (include/green_dyadic.hxx:600-702).  Grid (nAtoms, nrhs), 64 threads.
+template <typename T>
+__global__ void __launch_bounds__(64)
+sho_collect_kernel(double *__restrict__ aac, T const *__restrict__ apc, uint32_t nrhs,
+                   uint32_t const *__restrict__ atom_starts, int8_t const *__restrict__ atom_lmax,
+                   uint32_t const *__restrict__ sum_start, uint32_t const *__restrict__ sum_col,
+                   uint32_t const *__restrict__ img_starts, double const *__restrict__ img_phase)
+{
+    int const A = blockIdx.x, s = blockIdx.y, j = threadIdx.x;
+    int const nc = nsho_c(atom_lmax[A]);
+    size_t const a0 = atom_starts[A];
+    for (int c = 0; c < nc; ++c) {
+        double re = 0, im = 0;
+        for (uint32_t k = sum_start[A]; k < sum_start[A + 1]; ++k) {
+            uint32_t const i = sum_col[k];
+            double const pr = img_phase[4*i], pi = img_phase[4*i + 1];
+            T const *src = apc + ((size_t(img_starts[i]) + c)*nrhs + s)*128;
+            double const xr = double(src[j]), xi = double(src[64 + j]);
+            re += pr*xr - pi*xi;
+            im += pr*xi + pi*xr;
+        }
+        double *dst = aac + ((a0 + c)*nrhs + s)*128;
+        dst[j] = re; dst[64 + j] = im;
+    }
+}
+
+// out[(a0 + i)*nrhs + s] = sum_k M_A[i][k] in[(a0 + k)*nrhs + s], complex, accumulated in
+// double (include/green_dyadic.hxx:740-826).  Grid (nAtoms, nrhs), 64 threads.
+template <typename Tin, typename Tout>
+__global__ void __launch_bounds__(64)
+sho_mul_kernel(Tout *__restrict__ out, Tin const *__restrict__ in, uint32_t nrhs,
+               uint32_t const *__restrict__ atom_starts, int8_t const *__restrict__ atom_lmax,
+               double const *__restrict__ mats, uint32_t const *__restrict__ mat_off)
+{
+    int const A = blockIdx.x, s = blockIdx.y, j = threadIdx.x;
+    int const nc = nsho_c(atom_lmax[A]);
+    size_t const a0 = atom_starts[A];
+    double const *Mr = mats + mat_off[A], *Mi = Mr + nc*nc;
+    for (int i = 0; i < nc; ++i) {
+        double re = 0, im = 0;
+        for (int k = 0; k < nc; ++k) {
+            Tin const *src = in + ((a0 + k)*nrhs + s)*128;
+            double const xr = double(src[j]), xi = double(src[64 + j]);
+            double const mr = Mr[i*nc + k], mi = Mi[i*nc + k];
+            re += mr*xr - mi*xi;
+            im += mr*xi + mi*xr;
+        }
+        Tout *dst = out + ((a0 + i)*nrhs + s)*128;
+        dst[j] = Tout(re); dst[64 + j] = Tout(im);
+    }
+}
+
+// cad[(i0 + c)*nrhs + s] = conj(phase_i) * cadd[(a0 + c)*nrhs + s] for every image i of atom A
+// (broadcast, include/green_dyadic.hxx:683-694).  Grid (nAtoms, nrhs), 64 threads.
+template <typename T>
+__global__ void __launch_bounds__(64)
+sho_broadcast_kernel(T *__restrict__ cad, double const *__restrict__ cadd, uint32_t nrhs,
+                     uint32_t const *__restrict__ atom_starts, int8_t const *__restrict__ atom_lmax,
+                     uint32_t const *__restrict__ sum_start, uint32_t const *__restrict__ sum_col,
+                     uint32_t const *__restrict__ img_starts, double const *__restrict__ img_phase)
+{
+    int const A = blockIdx.x, s = blockIdx.y, j = threadIdx.x;
+    int const nc = nsho_c(atom_lmax[A]);
+    size_t const a0 = atom_starts[A];
+    for (uint32_t k = sum_start[A]; k < sum_start[A + 1]; ++k) {
+        uint32_t const i = sum_col[k];
+        double const pr = img_phase[4*i], pi = -img_phase[4*i + 1];
+        for (int c = 0; c < nc; ++c) {
+            double const *src = cadd + ((a0 + c)*nrhs + s)*128;
+            double const xr = src[j], xi = src[64 + j];
+            T *dst = cad + ((size_t(img_starts[i]) + c)*nrhs + s)*128;
+            dst[j] = T(pr*xr - pi*xi);
+            dst[64 + j] = T(pr*xi + pi*xr);
+        }
+    }
+}
+
+// y[b] += sum over the images a near block b of the masked projector functions times
+// cad[a, rhs(b)] (include/green_dyadic.hxx:325-518); sum-factorized over z, y, x.
+// One CTA per block, 128 threads = (reim, column); only masked points are written.
+template <typename T>
+__global__ void __launch_bounds__(128)
+sho_add_kernel(T *__restrict__ y, T const *__restrict__ cad, uint32_t nrhs, uint32_t nnzb,
+               uint16_t const *__restrict__ colIndex, uint32_t const *__restrict__ add_start,
+               uint32_t const *__restrict__ add_col, double const *__restrict__ img_pos,
+               int8_t const *__restrict__ img_lmax, uint32_t const *__restrict__ img_starts,
+               uint32_t const *__restrict__ rowindx, float const *__restrict__ cubepos,
+               double const *__restrict__ grid4)
+{
+    constexpr int LM = 7;
+    __shared__ T H[LM + 1][3][4];
+    __shared__ float xi2[3][4];
+    __shared__ double grid[4];
+    uint32_t const b = blockIdx.x;
+    if (add_start[b] >= add_start[b + 1]) return;
+    int const tid = threadIdx.x, reim = tid >> 6, j = tid & 63;
+    if (tid < 4) grid[tid] = grid4[tid];
+    uint32_t const s = colIndex[b];
+    float const *cp = cubepos + 4*size_t(rowindx[b]);
+    float const R2f = float(grid4[3]*grid4[3]);
+    T acc[64];
+#pragma unroll
+    for (int i = 0; i < 64; ++i) acc[i] = T(0);
+    uint64_t mask_all = 0;
+    for (uint32_t k = add_start[b]; k < add_start[b + 1]; ++k) {
+        uint32_t const a = add_col[k];
+        int const lmax = img_lmax[a];
+        __syncthreads();
+        hermite_tables<T, LM>(H, xi2, tid, lmax, img_pos + 4*size_t(a), cp, grid);
+        __syncthreads();
+        T const *c = cad + (size_t(img_starts[a])*nrhs + s)*128 + reim*64 + j;
+        uint64_t mask = 0;
+#pragma unroll
+        for (int z = 0; z < 4; ++z)
+#pragma unroll
+            for (int yy = 0; yy < 4; ++yy)
+#pragma unroll
+                for (int xx = 0; xx < 4; ++xx)
+                    if (in_mask(xi2, R2f, xx, yy, z)) mask |= 1ull << ((z*4 + yy)*4 + xx);
+        if (!mask) continue;
+        mask_all |= mask;
+        int sho = 0;
+        for (int iz = 0; iz <= lmax; ++iz) {
+            T byx[4][4];
+#pragma unroll
+            for (int yy = 0; yy < 4; ++yy)
+#pragma unroll
+                for (int xx = 0; xx < 4; ++xx) byx[yy][xx] = T(0);
+            for (int iy = 0; iy <= lmax - iz; ++iy) {
+                T ax[4] = {T(0), T(0), T(0), T(0)};
+                for (int ix = 0; ix <= lmax - iz - iy; ++ix, ++sho) {
+                    T const ca = c[size_t(sho)*nrhs*128];
+#pragma unroll
+                    for (int xx = 0; xx < 4; ++xx) ax[xx] += H[ix][0][xx]*ca;
+                }
+#pragma unroll
+                for (int yy = 0; yy < 4; ++yy) {
+                    T const hy = H[iy][1][yy];
+#pragma unroll
+                    for (int xx = 0; xx < 4; ++xx) byx[yy][xx] += hy*ax[xx];
+                }
+            }
+#pragma unroll
+            for (int z = 0; z < 4; ++z) {
+                T const hz = H[iz][2][z];
+#pragma unroll
+                for (int yy = 0; yy < 4; ++yy)
+#pragma unroll
+                    for (int xx = 0; xx < 4; ++xx) {
+                        int const p = (z*4 + yy)*4 + xx;
+                        if ((mask >> p) & 1) acc[p] += hz*byx[yy][xx];
+                    }
+            }
+        }
+    }
+    T *yb = y + size_t(b)*kBlockReals + reim*4096 + j;
+#pragma unroll
+    for (int p = 0; p < 64; ++p) if ((mask_all >> p) & 1) yb[p*64] += acc[p];
+}
+
+template <typename T> T const *vcell(DevicePlan &dp);
+template <> double const *vcell<double>(DevicePlan &dp) { return dptr<double>(dp.Vcell64); }
+template <> float const *vcell<float>(DevicePlan &dp) { return dptr<float>(dp.Vcell32); }
+
+template <typename T, int L>
+void launch_project_L(DevicePlan &dp, T const *x, cudaStream_t st) {
+    auto const &g = dp.img_group[L];
+    if (0 == g.count) return;
+    dim3 const grid(g.count, dp.nCols);
+    sho_project_kernel<T, L><<<grid, 128, 0, st>>>(
+        dptr<T>(dp.apc), x, dp.nCols, dptr<uint32_t>(g.images), dp.nAI,
+        dptr<uint32_t>(dp.prj_start), dptr<uint32_t>(dp.prj_col), dptr<uint64_t>(dp.prj_coloff),
+        dptr<double>(dp.img_pos), dptr<uint32_t>(dp.img_starts), dptr<uint32_t>(dp.rowindx),
+        dptr<float>(dp.rowCubePos), dptr<double>(dp.grid_dev));
+}
+
+} // namespace
+
+template <typename T>
+bool launch_local(DevicePlan &dp, T *y, T const *x, cudaStream_t st) {
+    if (0 == dp.nnzb) return true;
+    if (dp.fused_local) {
+        LocalArgs<T> a;
+        a.st = make_stencil9<T>(dp);
+        a.E_re = T(dp.E_re); a.E_im = T(dp.E_im);
+        for (int d = 0; d < 3; ++d) for (int s = 0; s < 2; ++s) for (int c = 0; c < 2; ++c) a.ph[d][s][c] = T(dp.phase[d][s][c]);
+        constexpr int S = (sizeof(T) == 8) ? 8 : 16;
+        unsigned const nblk = dp.nlists[2]*(64/S);
+        if (nblk) local_fused_kernel<T, S><<<nblk, S*16, 0, st>>>(y, x, dptr<uint32_t>(dp.lists_start[2]),
+            dptr<int32_t>(dp.lists[2]), dptr<int32_t>(dp.nbr), dptr<int32_t>(dp.veff_index), vcell<T>(dp), a);
+    } else {
+        unsigned const nb = std::min<uint32_t>(dp.nnzb, 148u*16);
+        potential_kernel<T><<<nb, 256, 0, st>>>(y, x, dptr<int32_t>(dp.veff_index), vcell<T>(dp), dp.nnzb,
+                                                T(dp.E_re), T(dp.E_im));
+        for (int d = 0; d < 3; ++d) {
+            int const nFD = dp.FD_range[d];
+            if (nFD < 1 || 0 == dp.nlists[d]) continue;
+            T const pl_r = T(dp.phase[d][0][0]), pl_i = T(dp.phase[d][0][1]);
+            T const pr_r = T(dp.phase[d][1][0]), pr_i = T(dp.phase[d][1][1]);
+            dim3 const grid(dp.nlists[d], 16);
+            // 8th order {-14350, 8064, -1008, 128, -9}/5040 or 16th order
+            // {-924708642, 538137600, -94174080, 22830080, -5350800, 1053696, -156800, 15360, -735}/302702400,
+            // times -1/(2h^2) (include/green_kinetic.hxx:37-42, 215-225)
+            Coef17<T> coef;
+            if (8 == nFD) {
+                double const w[9] = {-924708642, 538137600, -94174080, 22830080, -5350800, 1053696, -156800, 15360, -735};
+                double const norm = dp.prefactor[d]/302702400.;
+                for (int k = 0; k < 9; ++k) coef.c[k] = T(w[k]*norm);
+            } else {
+                double const w[5] = {-14350, 8064, -1008, 128, -9};
+                double const norm = dp.prefactor[d]/5040.;
+                for (int k = 0; k < 9; ++k) coef.c[k] = T(k < 5 ? w[k]*norm : 0.0);
+            }
+            if (8 == nFD) kinetic_list_kernel<T, 2><<<grid, 64, 0, st>>>(y, x, dptr<uint32_t>(dp.lists_start[d]),
+                              dptr<int32_t>(dp.lists[d]), 1 << (2*d), coef, pl_r, pl_i, pr_r, pr_i);
+            else kinetic_list_kernel<T, 1><<<grid, 64, 0, st>>>(y, x, dptr<uint32_t>(dp.lists_start[d]),
+                              dptr<int32_t>(dp.lists[d]), 1 << (2*d), coef, pl_r, pl_i, pr_r, pr_i);
+        }
+    }
+    A43G_CUDA_TRY(cudaGetLastError());
+    return true;
+}
+
+template <typename T>
+bool launch_dyadic(DevicePlan &dp, T *y, T const *x, uint16_t const *colIndex, cudaStream_t st) {
+    if (dp.nAI < 1 || dp.nCols < 1) return true;
+    if (!ensure_dyadic_scratch(dp, sizeof(T))) return false;
+    launch_project_L<T, 0>(dp, x, st); launch_project_L<T, 1>(dp, x, st);
+    launch_project_L<T, 2>(dp, x, st); launch_project_L<T, 3>(dp, x, st);
+    launch_project_L<T, 4>(dp, x, st); launch_project_L<T, 5>(dp, x, st);
+    launch_project_L<T, 6>(dp, x, st); launch_project_L<T, 7>(dp, x, st);
+    dim3 const ga(dp.nAtoms, dp.nCols);
+    if (dp.nAI > dp.nAtoms) {
+        sho_collect_kernel<T><<<ga, 64, 0, st>>>(dptr<double>(dp.aac), dptr<T>(dp.apc), dp.nCols,
+            dptr<uint32_t>(dp.atom_starts), dptr<int8_t>(dp.atom_lmax), dptr<uint32_t>(dp.sum_start),
+            dptr<uint32_t>(dp.sum_col), dptr<uint32_t>(dp.img_starts), dptr<double>(dp.img_phase));
+        sho_mul_kernel<double, double><<<ga, 64, 0, st>>>(dptr<double>(dp.cadd), dptr<double>(dp.aac), dp.nCols,
+            dptr<uint32_t>(dp.atom_starts), dptr<int8_t>(dp.atom_lmax), dptr<double>(dp.atom_mat), dptr<uint32_t>(dp.atom_mat_off));
+        sho_broadcast_kernel<T><<<ga, 64, 0, st>>>(dptr<T>(dp.cad), dptr<double>(dp.cadd), dp.nCols,
+            dptr<uint32_t>(dp.atom_starts), dptr<int8_t>(dp.atom_lmax), dptr<uint32_t>(dp.sum_start),
+            dptr<uint32_t>(dp.sum_col), dptr<uint32_t>(dp.img_starts), dptr<double>(dp.img_phase));
+    } else {
+        sho_mul_kernel<T, T><<<ga, 64, 0, st>>>(dptr<T>(dp.cad), dptr<T>(dp.apc), dp.nCols,
+            dptr<uint32_t>(dp.atom_starts), dptr<int8_t>(dp.atom_lmax), dptr<double>(dp.atom_mat), dptr<uint32_t>(dp.atom_mat_off));
+    }
+    sho_add_kernel<T><<<dp.nnzb, 128, 0, st>>>(y, dptr<T>(dp.cad), dp.nCols, dp.nnzb, colIndex,
+        dptr<uint32_t>(dp.add_start), dptr<uint32_t>(dp.add_col), dptr<double>(dp.img_pos), dptr<int8_t>(dp.img_lmax),
+        dptr<uint32_t>(dp.img_starts), dptr<uint32_t>(dp.rowindx), dptr<float>(dp.rowCubePos), dptr<double>(dp.grid_dev));
+    A43G_CUDA_TRY(cudaGetLastError());
+    return true;
+}
+
+template <typename T>
+bool launch_action(DevicePlan &dp, T *y, T const *x, uint16_t const *colIndex, cudaStream_t st) {
+    if (!launch_local<T>(dp, y, x, st)) return false;
+    return launch_dyadic<T>(dp, y, x, colIndex, st);
+}
+
+template bool launch_local<double>(DevicePlan &, double *, double const *, cudaStream_t);
+template bool launch_local<float>(DevicePlan &, float *, float const *, cudaStream_t);
+template bool launch_dyadic<double>(DevicePlan &, double *, double const *, uint16_t const *, cudaStream_t);
+template bool launch_dyadic<float>(DevicePlan &, float *, float const *, uint16_t const *, cudaStream_t);
+template bool launch_action<double>(DevicePlan &, double *, double const *, uint16_t const *, cudaStream_t);
+template bool launch_action<float>(DevicePlan &, float *, float const *, uint16_t const *, cudaStream_t);
+
+} // namespace a43g

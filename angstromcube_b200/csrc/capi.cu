@@ -1,0 +1,239 @@
+// extern "C" entry points declared in include/a43g.h.
+#include "../../include/a43g.h"
+#include "device.cuh"
+#include "solver.hpp"
+
+#include <cstring>
+#include <mutex>
+#include <new>
+
+struct a43g_plan {
+    a43g::GreenPlan host;
+    a43g::DevicePlan dev;
+    a43g::SolverWorkspace solver;
+    bool energy_set = false;
+    bool matrices_set = false;
+    int device = -1;
+    std::mutex mtx;                  // calls on one plan are serialised; distinct plans are independent
+};
+
+namespace a43g {
+namespace {
+thread_local std::string g_error;
+}
+void set_error(std::string const &msg) { g_error = msg; }
+} // namespace a43g
+
+using a43g::set_error;
+
+namespace {
+
+int fail(int code, std::string const &msg) { set_error(msg); return code; }
+
+int ensure_device(a43g_plan_t *p) {
+    int dev = 0;
+    if (cudaSuccess != cudaGetDevice(&dev)) return fail(A43G_ERR_CUDA, "no CUDA device available");
+    if (p->device >= 0 && p->device != dev) return fail(A43G_ERR_STATE, "plan was uploaded to another device");
+    if (!p->dev.uploaded) {
+        if (!a43g::upload_plan(p->host, p->dev)) return A43G_ERR_CUDA;
+        p->device = dev;
+    } else if (p->dev.values_dirty) {
+        if (!a43g::upload_values(p->host, p->dev)) return A43G_ERR_CUDA;
+    }
+    return A43G_OK;
+}
+
+} // namespace
+
+extern "C" {
+
+const char *a43g_last_error(void) { return a43g::g_error.c_str(); }
+
+const char *a43g_version(void) { return "a43g 0.1 (sm_100a)"; }
+
+int a43g_plan_build(const a43g_geometry_t *g, a43g_plan_t **plan) {
+    if (!g || !plan) return fail(A43G_ERR_ARGUMENT, "null argument");
+    if (g->natoms < 0 || (g->natoms > 0 && !g->xyzZinso)) return fail(A43G_ERR_ARGUMENT, "atoms missing");
+    auto *p = new (std::nothrow) a43g_plan();
+    if (!p) return fail(A43G_ERR_MEMORY, "host allocation failed");
+    a43g::Geometry geo;
+    for (int d = 0; d < 3; ++d) {
+        geo.ng[d] = g->ng[d]; geo.bc[d] = int8_t(g->bc[d]); geo.hg[d] = g->hg[d]; geo.sources[d] = g->sources[d];
+    }
+    geo.r_trunc = g->r_trunc; geo.nFD = g->nFD; geo.proj_radius = g->proj_radius;
+    geo.xyzZinso.assign(g->xyzZinso, g->xyzZinso + 8*size_t(g->natoms));
+    std::string err;
+    try { err = p->host.build(geo); } catch (std::bad_alloc const &) { err = "host memory exhausted"; }
+    if (!err.empty()) { delete p; return fail(A43G_ERR_ARGUMENT, err); }
+    *plan = p;
+    return A43G_OK;
+}
+
+int a43g_plan_destroy(a43g_plan_t *plan) {
+    if (!plan) return A43G_OK;
+    if (plan->device >= 0) cudaSetDevice(plan->device);
+    delete plan;
+    return A43G_OK;
+}
+
+int a43g_plan_get_sizes(const a43g_plan_t *plan, a43g_plan_sizes_t *s) {
+    if (!plan || !s) return fail(A43G_ERR_ARGUMENT, "null argument");
+    auto const &h = plan->host;
+    s->nnzb = int64_t(h.nnzb()); s->nRows = h.nRows; s->nCols = h.nCols;
+    s->nAtoms = h.nAtoms; s->nAtomImages = h.nAtomImages;
+    s->ncoeff_images = int64_t(h.ncoeff_images()); s->ncoeffs = int64_t(h.ncoeff_atoms());
+    for (int d = 0; d < 3; ++d) {
+        s->nlists[d] = h.kinetic[d].nlists(); s->lists_nnz[d] = int64_t(h.kinetic[d].entry.size());
+        s->FD_range[d] = h.kinetic[d].FD_range;
+    }
+    s->SHOadd_nnz = h.SHOadd.nnz();
+    int64_t n = 0; for (auto const &c : h.SHOprj) n += c.nnz();
+    s->SHOprj_nnz = n;
+    s->SHOsum_nnz = h.SHOsum.nnz();
+    s->ncells = int64_t(h.ncells());
+    return A43G_OK;
+}
+
+int a43g_plan_export(const a43g_plan_t *plan, const a43g_plan_export_t *e) {
+    if (!plan || !e) return fail(A43G_ERR_ARGUMENT, "null argument");
+    auto const &h = plan->host;
+    auto cp = [](void *dst, void const *src, size_t bytes) { if (dst && bytes) std::memcpy(dst, src, bytes); };
+    size_t const nnzb = h.nnzb();
+    cp(e->rowstart, h.rowstart.data(), h.rowstart.size()*4);
+    cp(e->colindx, h.colindx.data(), nnzb*2);
+    cp(e->rowindx, h.rowindx.data(), nnzb*4);
+    cp(e->veff_index, h.veff_index.data(), nnzb*4);
+    cp(e->subset, h.subset.data(), h.subset.size()*4);
+    cp(e->rowCubePos, h.rowCubePos.data(), h.rowCubePos.size()*4);
+    cp(e->colCubePos, h.colCubePos.data(), h.colCubePos.size()*4);
+    cp(e->target_minus_source, h.target_minus_source.data(), h.target_minus_source.size()*2);
+    cp(e->grid_spacing_trunc, h.h_trunc, 24);
+    for (int d = 0; d < 3; ++d) {
+        if (e->kinetic_prefactor) e->kinetic_prefactor[d] = h.kinetic[d].prefactor;
+        cp(e->lists_start[d], h.kinetic[d].start.data(), h.kinetic[d].start.size()*4);
+        cp(e->lists[d], h.kinetic[d].entry.data(), h.kinetic[d].entry.size()*4);
+    }
+    cp(e->AtomStarts, h.AtomStarts.data(), h.AtomStarts.size()*4);
+    cp(e->AtomLmax, h.AtomLmax.data(), h.AtomLmax.size());
+    cp(e->AtomSigma, h.AtomSigma.data(), h.AtomSigma.size()*8);
+    cp(e->global_atom_ids, h.global_atom_ids.data(), h.global_atom_ids.size()*8);
+    cp(e->AtomImageIndex, h.AtomImageIndex.data(), h.AtomImageIndex.size()*4);
+    cp(e->AtomImageStarts, h.AtomImageStarts.data(), h.AtomImageStarts.size()*4);
+    cp(e->AtomImagePos, h.AtomImagePos.data(), h.AtomImagePos.size()*8);
+    cp(e->AtomImageLmax, h.AtomImageLmax.data(), h.AtomImageLmax.size());
+    cp(e->AtomImageShift, h.AtomImageShift.data(), h.AtomImageShift.size());
+    cp(e->AtomImagePhase, h.AtomImagePhase.data(), h.AtomImagePhase.size()*8);
+    cp(e->grid_spacing_dyadic, h.grid_spacing_dyadic, 32);
+    cp(e->SHOadd_start, h.SHOadd.start.data(), h.SHOadd.start.size()*4);
+    cp(e->SHOadd_col, h.SHOadd.col.data(), h.SHOadd.col.size()*4);
+    if (e->SHOprj_start || e->SHOprj_col) {
+        size_t os = 0, oc = 0;
+        for (auto const &c : h.SHOprj) {
+            if (e->SHOprj_start) {
+                if (c.start.empty()) std::memset(e->SHOprj_start + os, 0, (h.nAtomImages + 1)*4);
+                else std::memcpy(e->SHOprj_start + os, c.start.data(), c.start.size()*4);
+            }
+            os += h.nAtomImages + 1;
+            if (e->SHOprj_col) cp(e->SHOprj_col + oc, c.col.data(), c.col.size()*4);
+            oc += c.col.size();
+        }
+    }
+    cp(e->SHOsum_start, h.SHOsum.start.data(), h.SHOsum.start.size()*4);
+    cp(e->SHOsum_col, h.SHOsum.col.data(), h.SHOsum.col.size()*4);
+    cp(e->AtomMatrices, h.AtomMatrices.data(), h.AtomMatrices.size()*8);
+    cp(e->phase, h.phase, 12*8);
+    return A43G_OK;
+}
+
+int a43g_plan_set_potential(a43g_plan_t *plan, const double *V, int layout) {
+    if (!plan || !V) return fail(A43G_ERR_ARGUMENT, "null argument");
+    std::lock_guard<std::mutex> lock(plan->mtx);
+    if (0 == layout) plan->host.set_potential_grid(V);
+    else if (1 == layout) plan->host.set_potential_cells(V);
+    else return fail(A43G_ERR_ARGUMENT, "layout must be 0 (grid) or 1 (cell cubes)");
+    plan->dev.values_dirty = true;
+    return A43G_OK;
+}
+
+int a43g_plan_set_atom_matrices(a43g_plan_t *plan, const double *mats, const int64_t *offsets, int64_t natoms) {
+    if (!plan || (!mats && natoms > 0) || (!offsets && natoms > 0)) return fail(A43G_ERR_ARGUMENT, "null argument");
+    std::lock_guard<std::mutex> lock(plan->mtx);
+    auto const err = plan->host.set_atom_matrices(mats, offsets, natoms);
+    if (!err.empty()) return fail(A43G_ERR_ARGUMENT, err);
+    plan->matrices_set = true;
+    plan->dev.values_dirty = true;
+    return A43G_OK;
+}
+
+int a43g_plan_set_energy(a43g_plan_t *plan, double Er, double Ei, double dVol) {
+    if (!plan) return fail(A43G_ERR_ARGUMENT, "null argument");
+    std::lock_guard<std::mutex> lock(plan->mtx);
+    plan->host.set_energy(Er, Ei, dVol);
+    plan->energy_set = true;
+    plan->dev.values_dirty = true;
+    return A43G_OK;
+}
+
+int a43g_plan_set_kpoint(a43g_plan_t *plan, const double k[3]) {
+    if (!plan || !k) return fail(A43G_ERR_ARGUMENT, "null argument");
+    std::lock_guard<std::mutex> lock(plan->mtx);
+    auto const err = plan->host.set_kpoint(k);
+    if (!err.empty()) return fail(A43G_ERR_ARGUMENT, err);
+    plan->dev.values_dirty = true;
+    return A43G_OK;
+}
+
+int a43g_plan_upload(a43g_plan_t *plan) {
+    if (!plan) return fail(A43G_ERR_ARGUMENT, "null argument");
+    std::lock_guard<std::mutex> lock(plan->mtx);
+    return ensure_device(plan);
+}
+
+int a43g_action_multiply(a43g_plan_t *plan, void *y, const void *x, const uint16_t *colIndex,
+                         uint32_t nnzb, uint32_t nCols, unsigned /*l2nX*/, void *stream, int dtype,
+                         double *flops) {
+    if (!plan || (!y && nnzb) || (!x && nnzb) || (!colIndex && nnzb)) return fail(A43G_ERR_ARGUMENT, "null argument");
+    std::lock_guard<std::mutex> lock(plan->mtx);
+    if (nnzb != plan->host.nnzb()) return fail(A43G_ERR_ARGUMENT, "nnzb does not match the plan");
+    if (nCols != plan->host.nCols) return fail(A43G_ERR_ARGUMENT, "nCols does not match the plan");
+    if (!plan->energy_set) return fail(A43G_ERR_STATE, "energy parameter not set (a43g_plan_set_energy)");
+    if (y == x) return fail(A43G_ERR_ARGUMENT, "y and x must not alias");
+    int const rc = ensure_device(plan);
+    if (rc) return rc;
+    auto const st = (cudaStream_t)stream;
+    bool ok;
+    if (A43G_F64 == dtype) ok = a43g::launch_action<double>(plan->dev, (double*)y, (double const*)x, colIndex, st);
+    else if (A43G_F32 == dtype) ok = a43g::launch_action<float>(plan->dev, (float*)y, (float const*)x, colIndex, st);
+    else return fail(A43G_ERR_ARGUMENT, "dtype must be A43G_F64 or A43G_F32");
+    if (!ok) return A43G_ERR_CUDA;
+    if (flops) *flops = a43g::action_flops(plan->host, (A43G_F64 == dtype) ? 8 : 4);
+    return A43G_OK;
+}
+
+int a43g_solve(a43g_plan_t *plan, const a43g_solve_options_t *opts, void *X, double *rho,
+               a43g_solve_stats_t *stats, void *stream) {
+    if (!plan || !opts) return fail(A43G_ERR_ARGUMENT, "null argument");
+    std::lock_guard<std::mutex> lock(plan->mtx);
+    if (!plan->energy_set) return fail(A43G_ERR_STATE, "energy parameter not set (a43g_plan_set_energy)");
+    int const rc = ensure_device(plan);
+    if (rc) return rc;
+    a43g_solve_stats_t local{};
+    int const r = a43g::solve(plan->host, plan->dev, plan->solver, *opts, X, rho, stats ? stats : &local,
+                              (cudaStream_t)stream);
+    return r;
+}
+
+int a43g_solve_batched(a43g_plan_t *plan, const a43g_solve_options_t *opts, int32_t n,
+                       const double *energies, const double *kpoints, double dVol,
+                       double *rho, a43g_solve_stats_t *stats, void *stream) {
+    if (!plan || !opts || n < 0 || (n > 0 && (!energies || !kpoints || !stats)))
+        return fail(A43G_ERR_ARGUMENT, "null argument");
+    std::lock_guard<std::mutex> lock(plan->mtx);
+    if (!plan->matrices_set && plan->host.nAtoms > 0) return fail(A43G_ERR_STATE, "atom matrices not set");
+    int const rc = ensure_device(plan);
+    if (rc) return rc;
+    return a43g::solve_batched(plan->host, plan->dev, plan->solver, *opts, n, energies, kpoints, dVol,
+                               rho, stats, (cudaStream_t)stream);
+}
+
+} // extern "C"

@@ -1,0 +1,85 @@
+// Device-side plan, scratch buffers and launch interfaces shared by the CUDA sources.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "plan.hpp"
+
+namespace a43g {
+
+// error state of the calling host thread (capi.cu)
+void set_error(std::string const &msg);
+#define A43G_CUDA_TRY(call) do { cudaError_t e_ = (call); if (cudaSuccess != e_) { \
+    ::a43g::set_error(std::string(#call) + ": " + cudaGetErrorString(e_)); return false; } } while (0)
+
+// neighbour encoding in DevicePlan::nbr: -1 no cube (zero), >= 0 plain block index,
+// <= -2 block (-e - 2) seen across a periodic boundary (multiply by the Bloch phase)
+__host__ __device__ inline int32_t nbr_block(int32_t e) { return (e >= 0) ? e : (-e - 2); }
+
+struct DeviceBuffer {
+    void *ptr = nullptr;
+    size_t bytes = 0;
+    bool alloc(size_t n);
+    void release();
+    ~DeviceBuffer() { release(); }
+};
+
+template <typename T> T *dptr(DeviceBuffer const &b) { return (T*)b.ptr; }
+
+struct DevicePlan {
+    bool uploaded = false;       // plan geometry on the device
+    bool values_dirty = true;    // potential / matrices / phases need re-upload
+    uint32_t nnzb = 0, nRows = 0, nCols = 0, nAtoms = 0, nAI = 0;
+    uint32_t ncoeffI = 0, ncoeffA = 0;
+    int lmax_max = -1;
+    int FD_range[3] = {0, 0, 0};
+    double prefactor[3] = {0, 0, 0};
+    double phase[3][2][2] = {};
+    double grid[4] = {0, 0, 0, 0};
+    double E_re = 0, E_im = 0;
+    bool fused_local = false;    // all directions use the 9-point stencil: fused kernel
+    uint32_t nlists[3] = {0, 0, 0};
+
+    DeviceBuffer veff_index;     // int32 [nnzb]
+    DeviceBuffer Vcell64, Vcell32;  // [ncells][64]
+    DeviceBuffer nbr;            // int32 [nnzb][6]  x-, x+, y-, y+, z-, z+
+    DeviceBuffer lists_start[3], lists[3];
+    DeviceBuffer colindx;        // uint16 [nnzb]
+    DeviceBuffer rowindx;        // uint32 [nnzb]
+    DeviceBuffer rowCubePos;     // float [nRows][4]
+    DeviceBuffer prj_start, prj_col;   // [nCols][nAI+1], concatenated cols
+    DeviceBuffer prj_coloff;           // uint64 [nCols]
+    DeviceBuffer add_start, add_col;   // [nnzb+1], [nnz]
+    DeviceBuffer sum_start, sum_col;   // [nAtoms+1], [nnz]
+    DeviceBuffer img_pos, img_lmax, img_starts, img_phase;
+    DeviceBuffer atom_starts, atom_lmax, atom_mat, atom_mat_off;
+    DeviceBuffer grid_dev;       // double [4]: hx, hy, hz, projection radius
+    DeviceBuffer subset_dev;     // uint32 [nCols] diagonal block of each source column
+    struct ImageGroup { uint32_t count = 0; DeviceBuffer images; } img_group[8];  // images by basis size
+    // scratch of the dyadic part (allocated once per plan, never per call)
+    DeviceBuffer apc;            // real_t [ncoeffI*nCols][2][64] image projection coefficients
+    DeviceBuffer aac, cadd;      // double [ncoeffA*nCols][2][64]
+    DeviceBuffer cad;            // real_t [ncoeffI*nCols][2][64] image addition coefficients
+    size_t apc_elem_bytes = 0;   // 4 or 8: precision the apc/cad scratch is sized for
+};
+
+bool upload_plan(GreenPlan const &hp, DevicePlan &dp);
+bool upload_values(GreenPlan const &hp, DevicePlan &dp);
+bool ensure_dyadic_scratch(DevicePlan &dp, size_t elem_bytes);
+
+// the action y = (H - E S) x on real_t = double or float
+template <typename T>
+bool launch_action(DevicePlan &dp, T *y, T const *x, uint16_t const *colIndex, cudaStream_t s);
+
+// parts of the action (tests, VJP and benchmarks use them separately)
+template <typename T>
+bool launch_local(DevicePlan &dp, T *y, T const *x, cudaStream_t s);          // potential + kinetic
+template <typename T>
+bool launch_dyadic(DevicePlan &dp, T *y, T const *x, uint16_t const *colIndex, cudaStream_t s);
+
+double action_flops(GreenPlan const &hp, int real_bytes);
+
+} // namespace a43g

@@ -1,0 +1,87 @@
+"""The operator, mirroring green_action::action_t<real_t,R1C2=2,Noco=1,64>
+(include/green_action.hxx:57-299): multiply(y, x, colIndex, nnzb, nCols, l2nX, stream) over
+R1C2 64-column blocks, returning the reference's flop count.  x, y and colIndex are CUDA
+tensors (or raw device addresses); the arithmetic runs in libangstromcube_b200.so.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from ._lib import check, ptr
+
+
+def _dtype_code(real_t):
+    name = str(real_t)
+    if "float64" in name or "double" in name:
+        return _lib.A43G_F64
+    if "float32" in name or "float" in name:
+        return _lib.A43G_F32
+    raise TypeError("real_t must be float64 or float32, got %s" % name)
+
+
+class action_t:
+    """Implicit linear operator (H - E S) on block-sparse R1C2 data of one plan."""
+
+    def __init__(self, plan, real_t="float64"):
+        self.plan = plan
+        self.real_t = real_t
+        self.dtype = _dtype_code(real_t)
+        self.LM = self.LN = 64
+
+    def multiply(self, y, x, colIndex, nnzb, nCols=1, l2nX=0, stream=0):
+        """y = (H - E S) x; returns the number of floating point operations (reference count)."""
+        flops = ctypes.c_double(0)
+        st = ctypes.c_void_p(stream if isinstance(stream, int) else stream.cuda_stream)
+        check(_lib.lib().a43g_action_multiply(self.plan.handle, ptr(y), ptr(x), ptr(colIndex), int(nnzb), int(nCols),
+                                              int(l2nX), st, self.dtype, ctypes.byref(flops)),
+              "a43g_action_multiply")
+        return flops.value
+
+    def has_preconditioner(self):
+        return False
+
+    def get_plan(self):
+        return self.plan
+
+
+def solve_options(tolerance=1e-9, max_iterations=500, precision="float64", inner_tolerance=1e-4,
+                  max_refinements=8, check_every=10, seed=1):
+    o = _lib.SolveOptions()
+    o.tolerance = tolerance
+    o.max_iterations = max_iterations
+    o.precision = _dtype_code(precision)
+    o.inner_tolerance = inner_tolerance
+    o.max_refinements = max_refinements
+    o.check_every = check_every
+    o.seed = seed
+    return o
+
+
+def solve(plan, X=None, want_rho=True, stream=0, **kw):
+    """tfQMR solve of (H - E S) X = B (B: unit diagonal blocks).  X: optional CUDA tensor
+    [nnzb, 2, 64, 64] receiving the solution (float64).  Returns (stats dict, rho) with
+    rho complex [nCols, 64] = diag(G_diag)/pi as action_t::solve exports it."""
+    opts = solve_options(**kw)
+    stats = _lib.SolveStats()
+    rho = np.zeros((plan.nCols, 64, 2)) if want_rho else None
+    st = ctypes.c_void_p(stream if isinstance(stream, int) else stream.cuda_stream)
+    check(_lib.lib().a43g_solve(plan.handle, ctypes.byref(opts), ptr(X), ptr(rho), ctypes.byref(stats), st),
+          "a43g_solve")
+    return stats.as_dict(), (rho[..., 0] + 1j * rho[..., 1] if want_rho else None)
+
+
+def solve_batched(plan, energies, kpoints, dVol, want_rho=False, stream=0, **kw):
+    """Solves for every (energy, k-point) pair on the plan's geometry."""
+    E = np.ascontiguousarray(np.stack([np.real(energies), np.imag(energies)], axis=-1), dtype=np.float64)
+    K = np.ascontiguousarray(kpoints, dtype=np.float64).reshape(-1, 3)
+    n = len(E)
+    assert len(K) == n
+    opts = solve_options(**kw)
+    stats = (_lib.SolveStats * n)()
+    rho = np.zeros((n, plan.nCols, 64, 2)) if want_rho else None
+    st = ctypes.c_void_p(stream if isinstance(stream, int) else stream.cuda_stream)
+    check(_lib.lib().a43g_solve_batched(plan.handle, ctypes.byref(opts), n, ptr(E), ptr(K), float(dVol), ptr(rho),
+                                        stats, st), "a43g_solve_batched")
+    out = [stats[i].as_dict() for i in range(n)]
+    return out, (rho[..., 0] + 1j * rho[..., 1] if want_rho else None)

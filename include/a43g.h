@@ -1,0 +1,145 @@
+/*
+ * a43g -- B200 (sm_100a) Green-function action and tfQMR solver with a plain C ABI.
+ *
+ * The operator is AngstromCube's block-sparse Green-function action Y = (H - E S) X over
+ * 4x4x4-point cubes.  X and Y hold nnzb blocks of 64x64 complex numbers in the reference's
+ * R1C2 layout  real_t[nnzb][2][64][64]  ([block][re,im][target point][source column],
+ * source columns fastest), so a block vector produced by the reference's action_t can be
+ * handed to a43g_action_multiply unchanged.
+ *
+ * Every entry point returns an a43g status (0 = success) and never exits the process;
+ * a43g_last_error() gives the message of the last failure on the calling thread.
+ * Device pointers are plain CUDA device addresses; streams are cudaStream_t passed as void*.
+ */
+#ifndef A43G_H
+#define A43G_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    A43G_OK = 0,
+    A43G_ERR_ARGUMENT = 1,   /* invalid argument or inconsistent sizes */
+    A43G_ERR_CUDA = 2,       /* a CUDA runtime call failed */
+    A43G_ERR_STATE = 3,      /* missing prerequisite (e.g. no energy set) */
+    A43G_ERR_MEMORY = 4,     /* device allocation failed */
+    A43G_ERR_UNSUPPORTED = 5 /* feature not available for this plan */
+};
+
+enum { A43G_F64 = 0, A43G_F32 = 1 };            /* real_t of the R1C2 block vectors */
+
+typedef struct a43g_plan a43g_plan_t;
+
+/* Cell, boundary conditions, sources, truncation and atoms, i.e. the inputs of
+ * green_function::construct_Green_function (src/green_function.cxx:357-365) plus the
+ * control keys it reads (green_function.truncation.radius, green_function.sources.x/y/z,
+ * green_kinetic.range, green_function.projection.radius). */
+typedef struct {
+    uint32_t ng[3];           /* grid points per direction, multiples of 4 */
+    int32_t  bc[3];           /* 0 isolated, 1 periodic, 2 vacuum, 3 repeat */
+    double   hg[3];           /* grid spacings in Bohr */
+    double   r_trunc;         /* truncation radius in Bohr */
+    double   sources[3];      /* source cubes per direction (box centred in the cell), <0: all */
+    int32_t  nFD;             /* finite-difference range: 4 (8th order) or 8 (16th order) */
+    double   proj_radius;     /* projector cut-off radius in units of sigma (reference default 6) */
+    int32_t  natoms;
+    const double *xyzZinso;   /* [natoms][8]: x,y,z relative to the cell centre, Z, id (= index), numax, sigma, unused */
+} a43g_geometry_t;
+
+/* Plan sizes, same keys as the reference's plan members */
+typedef struct {
+    int64_t nnzb, nRows, nCols, nAtoms, nAtomImages, ncoeff_images, ncoeffs;
+    int64_t nlists[3], lists_nnz[3];
+    int64_t SHOadd_nnz, SHOprj_nnz, SHOsum_nnz;
+    int64_t FD_range[3];
+    int64_t ncells;
+} a43g_plan_sizes_t;
+
+/* Host copies of the plan arrays (each pointer may be NULL to skip it); the layouts are
+ * those of action_plan_t, kinetic_plan_t and dyadic_plan_t (include/action_plan.hxx:32-93,
+ * include/kinetic_plan.hxx:163-199, include/dyadic_plan.hxx:14-47). */
+typedef struct {
+    uint32_t *rowstart; uint16_t *colindx; uint32_t *rowindx; int32_t *veff_index;
+    uint32_t *subset; float *rowCubePos; float *colCubePos; int16_t *target_minus_source;
+    double *grid_spacing_trunc; double *kinetic_prefactor;
+    uint32_t *lists_start[3]; int32_t *lists[3];
+    uint32_t *AtomStarts; int8_t *AtomLmax; double *AtomSigma; int64_t *global_atom_ids;
+    uint32_t *AtomImageIndex; uint32_t *AtomImageStarts; double *AtomImagePos; int8_t *AtomImageLmax;
+    int8_t *AtomImageShift; double *AtomImagePhase; double *grid_spacing_dyadic;
+    uint32_t *SHOadd_start; uint32_t *SHOadd_col; uint32_t *SHOprj_start; uint32_t *SHOprj_col;
+    uint32_t *SHOsum_start; uint32_t *SHOsum_col; double *AtomMatrices; double *phase;
+} a43g_plan_export_t;
+
+/* Solver options and per-solve statistics (tfQMR, Freund 1993, per-column scalars) */
+typedef struct {
+    double   tolerance;       /* relative residual |B - A X| / |B| per column */
+    int32_t  max_iterations;  /* tfQMR iterations (two operator applications each) */
+    int32_t  precision;       /* A43G_F64: plain FP64 tfQMR; A43G_F32: FP32 sweeps inside FP64 refinement */
+    double   inner_tolerance; /* FP32 inner solve tolerance per refinement step (mixed precision) */
+    int32_t  max_refinements; /* FP64 refinement steps (mixed precision) */
+    int32_t  check_every;     /* iterations between convergence checks on the host */
+    uint64_t seed;            /* seed of the random shadow residual */
+} a43g_solve_options_t;
+
+typedef struct {
+    int32_t iterations;       /* tfQMR iterations performed (summed over refinements) */
+    int32_t refinements;      /* FP64 residual recomputations performed */
+    int32_t converged;        /* 1 if every column reached the tolerance */
+    int32_t breakdowns;       /* columns stopped by a rho or sigma breakdown */
+    double  residual_max;     /* max over columns of the true relative residual (FP64) */
+    double  residual_estimate;/* tfQMR residual bound at exit */
+    double  operator_applications; /* action calls made */
+    double  seconds;          /* device time of the solve */
+} a43g_solve_stats_t;
+
+const char *a43g_last_error(void);
+const char *a43g_version(void);
+
+/* ---- plan: replaces construct_Green_function + action_plan_t (src/green_function.cxx:357-1068) */
+int a43g_plan_build(const a43g_geometry_t *geometry, a43g_plan_t **plan);
+int a43g_plan_destroy(a43g_plan_t *plan);
+int a43g_plan_get_sizes(const a43g_plan_t *plan, a43g_plan_sizes_t *sizes);
+int a43g_plan_export(const a43g_plan_t *plan, const a43g_plan_export_t *out);
+/* replaces green_function::update_potential (src/green_function.cxx:114-211) for one rank:
+ * layout 0 = full grid V[(iz*ng_y + iy)*ng_x + ix], layout 1 = cell cubes [ncells][64] */
+int a43g_plan_set_potential(a43g_plan_t *plan, const double *V, int layout);
+/* atom matrices per atom id, concatenated [2][nc][nc] (hmt, ovl), already multiplied by the
+ * SHO prefactors as src/energy_contour.cxx:307-323 does; offsets[natoms] in doubles */
+int a43g_plan_set_atom_matrices(a43g_plan_t *plan, const double *mats, const int64_t *offsets, int64_t natoms);
+/* replaces green_function::update_energy_parameter (src/green_function.cxx:64-109) */
+int a43g_plan_set_energy(a43g_plan_t *plan, double E_re, double E_im, double dVol);
+/* replaces green_function::update_phases (src/green_function.cxx:218-251); k in units of 2 pi/cell */
+int a43g_plan_set_kpoint(a43g_plan_t *plan, const double k[3]);
+/* copies plan, potential and matrices to the device (done implicitly by the calls below) */
+int a43g_plan_upload(a43g_plan_t *plan);
+
+/* ---- the operator: replaces green_action::action_t<real_t,2,1,64>::multiply
+ * (include/green_action.hxx:140-176).  y and x are device pointers to real_t[nnzb][2][64][64];
+ * colIndex is the device array [nnzb] of block columns (as the reference passes it);
+ * nnzb and nCols must match the plan; l2nX is accepted for interface compatibility.
+ * flops (optional) receives the reference's flop count of one application. */
+int a43g_action_multiply(a43g_plan_t *plan, void *y, const void *x, const uint16_t *colIndex,
+                         uint32_t nnzb, uint32_t nCols, unsigned l2nX, void *stream, int dtype,
+                         double *flops);
+
+/* ---- tfQMR solve of (H - E S) X = B with B the unit blocks on the diagonal (plan subset);
+ * replaces tfqmrgpu::solve + action_t::solve (include/green_action.hxx:181-241).
+ * X: optional device pointer real_t[nnzb][2][64][64] (precision of the options) receiving the
+ * solution; rho: optional host array complex double [nCols][64][2] receiving the diagonal
+ * of the diagonal blocks divided by pi, as action_t::solve exports it. */
+int a43g_solve(a43g_plan_t *plan, const a43g_solve_options_t *opts, void *X, double *rho,
+               a43g_solve_stats_t *stats, void *stream);
+
+/* ---- batched solve over (energy, k-point) pairs on one plan geometry: energies[n][2],
+ * kpoints[n][3]; rho (optional) host [n][nCols][64][2]; stats[n] */
+int a43g_solve_batched(a43g_plan_t *plan, const a43g_solve_options_t *opts, int32_t n,
+                       const double *energies, const double *kpoints, double dVol,
+                       double *rho, a43g_solve_stats_t *stats, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* A43G_H */
