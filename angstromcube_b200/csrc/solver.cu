@@ -4,8 +4,9 @@
 //
 // One iteration = two operator applications.  The BLAS-1 work is fused so that every vector
 // is streamed as few times as possible:
-//   K_A   U2 = U1 - a V                 and |W - a V|^2
-//   K_C   W  = W - a (V + AU2)          and |W|^2, rt^H W
+//   K_A   U2 = U1 - a V                 and |W - a AU1|^2
+//   K_C   W  = W - a (AU1 + AU2)        and |W|^2, rt^H W
+// (U1 = y_{2n-1}, U2 = y_{2n}, AU1 = A y_{2n-1}, AU2 = A y_{2n}, V = v_{n-1} in Freund's notation)
 //   K_DX  D, X advanced by both half steps at once;  U1 = W + b U2
 //   K_E   V  = AU1 + b (AU2 + b V)      and rt^H V
 // The shadow residual rt is a counter-based random vector regenerated on the fly, so it is
@@ -107,9 +108,9 @@ __global__ void __launch_bounds__(256) k_init_dots(T const *W, T const *V, uint3
     }
 }
 
-// K_A: U2 = U1 - alpha V ; acc |W - alpha V|^2
+// K_A: U2 = U1 - alpha V ; acc |W - alpha AU1|^2
 template <typename T>
-__global__ void __launch_bounds__(256) k_A(T *U2, T const *U1, T const *V, T const *W, uint32_t nnzb,
+__global__ void __launch_bounds__(256) k_A(T *U2, T const *U1, T const *V, T const *W, T const *AU1, uint32_t nnzb,
                                            uint16_t const *colindx, ColState const *cs, Acc *acc) {
     __shared__ double red[4][64][3];
     int const j = threadIdx.x & 63, q = threadIdx.x >> 6;
@@ -122,16 +123,17 @@ __global__ void __launch_bounds__(256) k_A(T *U2, T const *U1, T const *V, T con
             T const vr = V[o], vi = V[o + 4096];
             double avr, avi; cmul(ar, ai, vr, vi, avr, avi);
             U2[o] = T(double(U1[o]) - avr); U2[o + 4096] = T(double(U1[o + 4096]) - avi);
-            double const wr = double(W[o]) - avr, wi = double(W[o + 4096]) - avi;
+            double aur, aui; cmul(ar, ai, AU1[o], AU1[o + 4096], aur, aui);
+            double const wr = double(W[o]) - aur, wi = double(W[o + 4096]) - aui;
             n2 += wr*wr + wi*wi;
         }
         reduce_cols(red, q, j, n2, 0.0, 0.0, &acc[col], 1);
     }
 }
 
-// K_C: W = W - alpha (V + AU2) ; acc |W|^2 and rt^H W
+// K_C: W = W - alpha (AU1 + AU2) ; acc |W|^2 and rt^H W
 template <typename T>
-__global__ void __launch_bounds__(256) k_C(T *W, T const *V, T const *AU2, uint32_t nnzb,
+__global__ void __launch_bounds__(256) k_C(T *W, T const *AU1, T const *AU2, uint32_t nnzb,
                                            uint16_t const *colindx, ColState const *cs, Acc *acc, uint32_t seed) {
     __shared__ double red[4][64][3];
     int const j = threadIdx.x & 63, q = threadIdx.x >> 6;
@@ -141,7 +143,7 @@ __global__ void __launch_bounds__(256) k_C(T *W, T const *V, T const *AU2, uint3
         double n2 = 0, dr = 0, di = 0;
         for (int i = q*16; i < q*16 + 16; ++i) {
             size_t const o = size_t(b)*kBlk + i*64 + j;
-            double const sr = double(V[o]) + double(AU2[o]), si = double(V[o + 4096]) + double(AU2[o + 4096]);
+            double const sr = double(AU1[o]) + double(AU2[o]), si = double(AU1[o + 4096]) + double(AU2[o + 4096]);
             double const wr = double(W[o]) - (ar*sr - ai*si), wi = double(W[o + 4096]) - (ar*si + ai*sr);
             T const tr_ = T(wr), ti_ = T(wi);
             W[o] = tr_; W[o + 4096] = ti_;
@@ -436,7 +438,8 @@ bool tfqmr_inner(DevicePlan &dp, SolverWorkspace &ws, TfqmrVectors &v, double to
     A43G_CUDA_TRY(cudaMemsetAsync(accA, 0, 2*size_t(ncol)*sizeof(Acc), st));
     A43G_CUDA_TRY(cudaMemsetAsync(cnt, 0, 4*sizeof(int32_t), st));
     // V = A U1
-    if (!launch_action<T>(dp, V, U1, ci, st)) return false;
+    if (!launch_action<T>(dp, AU1, U1, ci, st)) return false;
+    A43G_CUDA_TRY(cudaMemcpyAsync(V, AU1, v.n*sizeof(T), cudaMemcpyDeviceToDevice, st));
     res.applications += 1;
     k_init_dots<T><<<g, 256, 0, st>>>(W, V, nnzb, ci, accA, accB, seed);
     s_init<<<gs, 256, 0, st>>>(cs, accA, accB, ncol, cnt);
@@ -444,10 +447,10 @@ bool tfqmr_inner(DevicePlan &dp, SolverWorkspace &ws, TfqmrVectors &v, double to
     for (it = 1; it <= maxit; ++it) {
         bool const check = (0 == it % check_every) || (it == maxit);
         if (check) A43G_CUDA_TRY(cudaMemsetAsync(cnt, 0, sizeof(int32_t), st));
-        k_A<T><<<g, 256, 0, st>>>(U2, U1, V, W, nnzb, ci, cs, accA);
+        k_A<T><<<g, 256, 0, st>>>(U2, U1, V, W, AU1, nnzb, ci, cs, accA);
         s_half1<<<gs, 256, 0, st>>>(cs, accA, ncol, 2*it - 1, tol);
         if (!launch_action<T>(dp, AU2, U2, ci, st)) return false;
-        k_C<T><<<g, 256, 0, st>>>(W, V, AU2, nnzb, ci, cs, accA, seed);
+        k_C<T><<<g, 256, 0, st>>>(W, AU1, AU2, nnzb, ci, cs, accA, seed);
         s_half2<<<gs, 256, 0, st>>>(cs, accA, ncol, 2*it, tol, cnt);
         k_DX<T><<<g, 256, 0, st>>>(X, D, U1, U2, W, nnzb, ci, cs);
         if (!launch_action<T>(dp, AU1, U1, ci, st)) return false;

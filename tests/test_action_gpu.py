@@ -1,0 +1,127 @@
+"""Parity of the sm_100a action (through the C ABI) with the oracle.
+
+FP64: within 1e-12 relative (max norm) of the restated oracle, which itself matches the
+reference's CPU build to 1e-13.  FP32: within 3e-5 relative (rounding of the FP32 stencil
+and projector sums; the FP32 reference build shows the same order).  Full-size plans are
+checked through size-independent properties: linearity and complex symmetry at k = 0.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from helpers import GEOMETRIES, inputs_for, product_plan, rel_err
+from angstromcube_b200 import green_action, green_function as gf, workloads
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+FP64_TOL = 1e-12
+FP32_TOL = 3e-5
+
+
+def apply(plan, x_np, dtype):
+    x = torch.from_numpy(x_np.astype(dtype)).cuda()
+    y = torch.empty_like(x)
+    ci = torch.from_numpy(plan.export()["colindx"].astype(np.int16)).cuda()
+    op = green_action.action_t(plan, "float64" if dtype == np.float64 else "float32")
+    flops = op.multiply(y, x, ci, plan.nnzb, plan.nCols)
+    torch.cuda.synchronize()
+    assert flops > 0
+    return y.cpu().numpy()
+
+
+@pytest.mark.parametrize("name", sorted(GEOMETRIES))
+def test_action_fp64_fp32_vs_oracle(name):
+    g = GEOMETRIES[name]()
+    Vc, mats, offs, E, k, dVol, na = inputs_for(g)
+    p = product_plan(g, Vc, mats, offs, E, k, dVol)
+    o = oracle.RestatedOracle(p.export(), Vc, E)
+    x = np.random.default_rng(2).standard_normal((p.nnzb, 2, 64, 64))
+    y_ref = o.action(x)
+    y64 = apply(p, x, np.float64)
+    assert rel_err(y64, y_ref) < FP64_TOL
+    y32 = apply(p, x, np.float32)
+    assert rel_err(y32, y_ref) < FP32_TOL
+
+
+def test_action_matches_reference_build():
+    """Directly against the reference's action_t on the same plan inputs (FP64 and FP32)."""
+    if not oracle.ref_available():
+        pytest.skip("oracle/_ref not built")
+    from helpers import reference_plan
+    g = GEOMETRIES["mixed_iso_peri_vac"]()
+    Vc, mats, offs, E, k, dVol, na = inputs_for(g)
+    r = reference_plan(g, Vc, mats, offs, E, k, dVol)
+    p = product_plan(g, Vc, mats, offs, E, k, dVol)
+    x = np.random.default_rng(4).standard_normal((p.nnzb, 2, 64, 64))
+    assert rel_err(apply(p, x, np.float64), r.action(x)) < FP64_TOL
+    assert rel_err(apply(p, x, np.float32), r.action(x.astype(np.float32)).astype(np.float64)) < FP32_TOL
+
+
+def test_action_mid_size_workload():
+    w = workloads.make("periodic8_8atoms_s2x2x1")
+    p = gf.construct_Green_function(w.geometry)
+    gf.update_potential(p, w.Vcell, w.mats, w.offsets, layout="cells")
+    gf.update_energy_parameter(p, w.E, w.dVol)
+    o = oracle.RestatedOracle(p.export(), w.Vcell, w.E)
+    x = np.random.default_rng(3).standard_normal((p.nnzb, 2, 64, 64))
+    y_ref = o.action(x)
+    assert rel_err(apply(p, x, np.float64), y_ref) < FP64_TOL
+    assert rel_err(apply(p, x, np.float32), y_ref) < FP32_TOL
+
+
+def _complex_columns(y):
+    # [nnzb, 2, 64, 64] -> complex [nnzb*64 rows, 64 columns]
+    return (y[:, 0] + 1j * y[:, 1]).reshape(-1, 64)
+
+
+@pytest.mark.parametrize("name", ["periodic16_64atoms"])
+def test_full_size_linearity_and_symmetry(name):
+    """At the benchmark size: A(a x + b z) = a A x + b A z, and u^T A v = v^T A u per column
+    at k = 0 (H real symmetric, the truncated operator complex symmetric)."""
+    w = workloads.make(name)
+    p = gf.construct_Green_function(w.geometry)
+    gf.update_potential(p, w.Vcell, w.mats, w.offsets, layout="cells")
+    gf.update_energy_parameter(p, w.E, w.dVol)
+    ci = torch.from_numpy(p.export()["colindx"].astype(np.int16)).cuda()
+    op = green_action.action_t(p, "float64")
+    gen = torch.Generator(device="cuda").manual_seed(0)
+    shape = (p.nnzb, 2, 64, 64)
+    x = torch.randn(shape, device="cuda", dtype=torch.float64, generator=gen)
+    z = torch.randn(shape, device="cuda", dtype=torch.float64, generator=gen)
+    Ax, Az, As = torch.empty_like(x), torch.empty_like(x), torch.empty_like(x)
+    op.multiply(Ax, x, ci, p.nnzb, p.nCols)
+    op.multiply(Az, z, ci, p.nnzb, p.nCols)
+    op.multiply(As, 0.75 * x - 1.25 * z, ci, p.nnzb, p.nCols)
+    torch.cuda.synchronize()
+    lin = (As - (0.75 * Ax - 1.25 * Az)).abs().max().item() / As.abs().max().item()
+    assert lin < 1e-13
+    # bilinear symmetry per column: sum over rows of x * (A z) == z * (A x), complex arithmetic
+    xc = torch.complex(x[:, 0], x[:, 1]); zc = torch.complex(z[:, 0], z[:, 1])
+    Axc = torch.complex(Ax[:, 0], Ax[:, 1]); Azc = torch.complex(Az[:, 0], Az[:, 1])
+    ci64 = ci.long()
+    s1 = torch.zeros((p.nCols, 64), dtype=torch.complex128, device="cuda")
+    s2 = torch.zeros_like(s1)
+    s1.index_add_(0, ci64, (xc * Azc).sum(dim=1))
+    s2.index_add_(0, ci64, (zc * Axc).sum(dim=1))
+    sym = (s1 - s2).abs().max().item() / s1.abs().max().item()
+    assert sym < 1e-11
+    # FP32 operator on the same input
+    op32 = green_action.action_t(p, "float32")
+    x32 = x.float(); Ax32 = torch.empty_like(x32)
+    op32.multiply(Ax32, x32, ci, p.nnzb, p.nCols)
+    torch.cuda.synchronize()
+    assert ((Ax32.double() - Ax).abs().max() / Ax.abs().max()).item() < FP32_TOL
+
+
+def test_action_rejects_bad_sizes():
+    g = GEOMETRIES["no_atoms"]()
+    Vc, mats, offs, E, k, dVol, na = inputs_for(g)
+    p = product_plan(g, Vc, mats, offs, E, k, dVol)
+    x = torch.zeros((p.nnzb, 2, 64, 64), device="cuda", dtype=torch.float64)
+    ci = torch.zeros(p.nnzb, device="cuda", dtype=torch.int16)
+    op = green_action.action_t(p, "float64")
+    with pytest.raises(RuntimeError, match="nnzb"):
+        op.multiply(torch.empty_like(x), x, ci, p.nnzb + 1, p.nCols)
+    with pytest.raises(RuntimeError, match="alias"):
+        op.multiply(x, x, ci, p.nnzb, p.nCols)

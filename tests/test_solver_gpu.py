@@ -1,0 +1,75 @@
+"""tfQMR solves on the GPU.  Solver parity is anchored on the operator: the true residual
+|B - A X| / |B| of the returned solution is recomputed with the oracle's FP64 action on the
+CPU, and the solution is compared with the numpy tfQMR restatement (oracle/tfqmr.py)."""
+import numpy as np
+import pytest
+
+import oracle
+from angstromcube_b200 import green_action, green_function as gf, workloads
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+
+def setup(name):
+    w = workloads.make(name)
+    p = gf.construct_Green_function(w.geometry)
+    gf.update_potential(p, w.Vcell, w.mats, w.offsets, layout="cells")
+    gf.update_energy_parameter(p, w.E, w.dVol)
+    return w, p
+
+
+def true_residual(p, w, X):
+    a = p.export()
+    o = oracle.RestatedOracle(a, w.Vcell, w.E)
+    AX = o.action(X)
+    B = np.zeros_like(X)
+    for c, b in enumerate(a["subset"]):
+        B[b, 0][np.arange(64), np.arange(64)] = 1.0
+    R = (B - AX)
+    Rc = (R[:, 0] + 1j * R[:, 1])
+    colres = np.zeros((p.nCols, 64))
+    np.add.at(colres, a["colindx"].astype(np.int64), (np.abs(Rc) ** 2).sum(axis=1))
+    return np.sqrt(colres.max())
+
+
+@pytest.mark.parametrize("precision", ["float64", "float32"])
+def test_solve_periodic4_1atom(precision):
+    w, p = setup("periodic4_1atom")
+    X = torch.zeros((p.nnzb, 2, 64, 64), device="cuda", dtype=torch.float64)
+    stats, rho = green_action.solve(p, X=X, tolerance=w.tolerance, max_iterations=w.max_iterations,
+                                    precision=precision, check_every=5)
+    assert stats["converged"] == 1, stats
+    assert stats["residual_max"] <= w.tolerance
+    Xn = X.cpu().numpy()
+    res = true_residual(p, w, Xn)
+    assert res <= 2 * w.tolerance, res
+    a = p.export()
+    d = np.array([Xn[b, 0][np.arange(64), np.arange(64)] + 1j * Xn[b, 1][np.arange(64), np.arange(64)]
+                  for b in a["subset"]]) / np.pi
+    assert np.allclose(rho, d, rtol=0, atol=1e-14)
+
+
+def test_fp64_and_mixed_agree():
+    w, p = setup("periodic4_1atom")
+    X1 = torch.zeros((p.nnzb, 2, 64, 64), device="cuda", dtype=torch.float64)
+    X2 = torch.zeros_like(X1)
+    s1, _ = green_action.solve(p, X=X1, tolerance=1e-10, max_iterations=800, precision="float64")
+    s2, _ = green_action.solve(p, X=X2, tolerance=1e-10, max_iterations=800, precision="float32")
+    assert s1["converged"] and s2["converged"], (s1, s2)
+    err = ((X1 - X2).abs().max() / X1.abs().max()).item()
+    assert err < 1e-7
+
+
+def test_solve_matches_numpy_tfqmr():
+    """Same problem solved by the numpy restatement of tfQMR around the oracle action."""
+    from oracle import tfqmr
+    w, p = setup("periodic4_1atom")
+    a = p.export()
+    o = oracle.RestatedOracle(a, w.Vcell, w.E)
+    X = torch.zeros((p.nnzb, 2, 64, 64), device="cuda", dtype=torch.float64)
+    stats, _ = green_action.solve(p, X=X, tolerance=1e-9, max_iterations=500, precision="float64")
+    Xo, info = tfqmr.solve_blocks(o.action, a["subset"], a["colindx"], p.nnzb, p.nCols, tol=1e-9, maxiter=500)
+    assert info["converged"]
+    Xg = X.cpu().numpy()
+    assert np.abs(Xg - Xo).max() / np.abs(Xo).max() < 1e-6
