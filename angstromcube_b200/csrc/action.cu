@@ -238,40 +238,15 @@ kinetic_list_kernel(T *__restrict__ y, T const *__restrict__ x, uint32_t const *
 __host__ __device__ constexpr int nsho_c(int L) { return ((L + 1)*(L + 2)*(L + 3))/6; }
 __host__ __device__ constexpr int n2ho_c(int L) { return ((L + 1)*(L + 2))/2; }
 
-// 1D Hermite-Gauss tables of one (atom image, target cube) pair, computed by 12 threads:
-// H0 = exp(-xi^2/2) inside the projection radius else 0, H_{n+1} = xi H_n - n/2 H_{n-1},
-// xi = ((cube*4 + i4 + 1/2) h - R)/sigma (include/green_dyadic.hxx:33-107); xi^2 also as
-// float for the spherical mask, which is evaluated in float exactly as the reference does.
-template <typename T, int LMAX>
-__device__ __forceinline__ void hermite_tables(T (*H)[3][4], float (*xi2)[4], int tid, int lmax,
-                                               double const *__restrict__ pos, float const *__restrict__ cube,
-                                               double const *__restrict__ grid) {
-    if (tid < 12) {
-        int const d = tid >> 2, i4 = tid & 3;
-        double const R2 = grid[3]*grid[3];
-        double const sinv = pos[3]*pos[3];
-        double const xi = sinv*((double(cube[d])*4 + i4 + 0.5)*grid[d] - pos[d]);
-        double const x2 = xi*xi;
-        xi2[d][i4] = float(x2);
-        double hm = 0, h = (x2 < R2) ? exp(-0.5*x2) : 0.0;
-        H[0][d][i4] = T(h);
-#pragma unroll
-        for (int nu = 0; nu < LMAX; ++nu) {
-            if (nu < lmax) {
-                double const hp = xi*h - 0.5*nu*hm;
-                H[nu + 1][d][i4] = T(hp);
-                hm = h; h = hp;
-            }
-        }
-    }
+// Projector tables of one (atom image, target row) slot staged in shared memory: the 1D
+// Hermite-Gauss functions H[nu][dir][i4] (unnormalized, H_0 = exp(-xi^2/2) inside the
+// projection radius, H_{n+1} = xi H_n - n/2 H_{n-1}, include/green_dyadic.hxx:33-107) and
+// the 64-point spherical mask, both precomputed by the plan builder.
+template <typename T, int LM>
+__device__ __forceinline__ void stage_table(T (*H)[3][4], double const *__restrict__ slot_H, int stride,
+                                            uint32_t slot, int lmax, int tid) {
+    if (tid < (lmax + 1)*12) (&H[0][0][0])[tid] = T(slot_H[size_t(slot)*stride + tid]);
 }
-
-__device__ __forceinline__ bool in_mask(float const (*xi2)[4], float R2f, int x, int y, int z) {
-    float const d2z = xi2[2][z] - R2f;
-    float const d2yz = xi2[1][y] + d2z;
-    return (xi2[0][x] + d2yz) < 0.f;
-}
-
 
 // apc[(i0 + sho)*nrhs + s][reim][j] = sum over the blocks of source s near image a of the
 // masked projector functions times x (include/green_dyadic.hxx:112-288), for images whose
@@ -282,46 +257,43 @@ __global__ void __launch_bounds__(128)
 sho_project_kernel(T *__restrict__ apc, T const *__restrict__ x, uint32_t nrhs,
                    uint32_t const *__restrict__ images, uint32_t nAI,
                    uint32_t const *__restrict__ prj_start, uint32_t const *__restrict__ prj_col,
-                   uint64_t const *__restrict__ prj_coloff,
-                   double const *__restrict__ img_pos, uint32_t const *__restrict__ img_starts,
-                   uint32_t const *__restrict__ rowindx, float const *__restrict__ cubepos,
-                   double const *__restrict__ grid4)
+                   uint64_t const *__restrict__ prj_coloff, uint32_t const *__restrict__ prj_slot,
+                   double const *__restrict__ slot_H, uint64_t const *__restrict__ slot_mask, int stride,
+                   uint32_t const *__restrict__ img_starts)
 {
     constexpr int NS = nsho_c(L), N2 = n2ho_c(L);
-    __shared__ T H[L + 1][3][4];
-    __shared__ float xi2[3][4];
-    __shared__ double grid[4];
+    __shared__ T Hs[2][L + 1][3][4];
     uint32_t const a = images[blockIdx.x];
     int const s = blockIdx.y, tid = threadIdx.x;
     int const reim = tid >> 6, j = tid & 63;
-    if (tid < 4) grid[tid] = grid4[tid];
     uint32_t const *start = prj_start + size_t(s)*(nAI + 1);
-    uint32_t const *cols = prj_col + prj_coloff[s];
-    float const R2f = float(grid4[3]*grid4[3]);
+    uint64_t const off = prj_coloff[s];
     T acc[NS];
 #pragma unroll
     for (int i = 0; i < NS; ++i) acc[i] = T(0);
-    for (uint32_t k = start[a]; k < start[a + 1]; ++k) {
-        uint32_t const b = cols[k];
-        __syncthreads();
-        hermite_tables<T, L>(H, xi2, tid, L, img_pos + 4*size_t(a), cubepos + 4*size_t(rowindx[b]), grid);
-        __syncthreads();
+    int buf = 0;
+    for (uint32_t k = start[a]; k < start[a + 1]; ++k, buf ^= 1) {
+        uint32_t const b = prj_col[off + k];
+        uint32_t const slot = prj_slot[off + k];
+        stage_table<T, L>(Hs[buf], slot_H, stride, slot, L, tid);
+        uint64_t const mask = slot_mask[slot];
+        __syncthreads();             // double-buffered tables: one barrier per block
+        T (*H)[3][4] = Hs[buf];
         T const *xb = x + size_t(b)*kBlockReals + reim*4096 + j;
         for (int z = 0; z < 4; ++z) {
-            float const d2z = xi2[2][z] - R2f;
-            if (!(d2z < 0.f)) continue;
+            if (0 == ((mask >> (16*z)) & 0xffffu)) continue;
             T byx[N2];
 #pragma unroll
             for (int i = 0; i < N2; ++i) byx[i] = T(0);
             for (int yy = 0; yy < 4; ++yy) {
-                float const d2yz = xi2[1][yy] + d2z;
-                if (!(d2yz < 0.f)) continue;
+                unsigned const row = unsigned(mask >> (16*z + 4*yy)) & 0xfu;
+                if (0 == row) continue;
                 T ax[L + 1];
 #pragma unroll
                 for (int i = 0; i <= L; ++i) ax[i] = T(0);
 #pragma unroll
                 for (int xx = 0; xx < 4; ++xx) {
-                    if (xi2[0][xx] + d2yz < 0.f) {
+                    if ((row >> xx) & 1u) {
                         T const ps = xb[((z*4 + yy)*4 + xx)*64];
 #pragma unroll
                         for (int ix = 0; ix <= L; ++ix) ax[ix] += ps*H[ix][0][xx];
@@ -338,8 +310,8 @@ sho_project_kernel(T *__restrict__ apc, T const *__restrict__ x, uint32_t nrhs,
             for (int iz = 0, sho = 0; iz <= L; ++iz) {
                 T const hz = H[iz][2][z];
 #pragma unroll
-                for (int iy = 0, iyx = 0; iy <= L - iz; ++iy) {
-                    iyx = iy*(2*L + 3 - iy)/2;
+                for (int iy = 0; iy <= L - iz; ++iy) {
+                    int const iyx = iy*(2*L + 3 - iy)/2;
 #pragma unroll
                     for (int ix = 0; ix <= L - iz - iy; ++ix, ++sho) acc[sho] += byx[iyx + ix]*hz;
                 }
@@ -436,43 +408,31 @@ template <typename T>
 __global__ void __launch_bounds__(128)
 sho_add_kernel(T *__restrict__ y, T const *__restrict__ cad, uint32_t nrhs, uint32_t nnzb,
                uint16_t const *__restrict__ colIndex, uint32_t const *__restrict__ add_start,
-               uint32_t const *__restrict__ add_col, double const *__restrict__ img_pos,
-               int8_t const *__restrict__ img_lmax, uint32_t const *__restrict__ img_starts,
-               uint32_t const *__restrict__ rowindx, float const *__restrict__ cubepos,
-               double const *__restrict__ grid4)
+               uint32_t const *__restrict__ add_col, uint32_t const *__restrict__ add_slot,
+               double const *__restrict__ slot_H, uint64_t const *__restrict__ slot_mask, int stride,
+               int8_t const *__restrict__ img_lmax, uint32_t const *__restrict__ img_starts)
 {
     constexpr int LM = 7;
-    __shared__ T H[LM + 1][3][4];
-    __shared__ float xi2[3][4];
-    __shared__ double grid[4];
+    __shared__ T Hs[2][LM + 1][3][4];
     uint32_t const b = blockIdx.x;
     if (add_start[b] >= add_start[b + 1]) return;
     int const tid = threadIdx.x, reim = tid >> 6, j = tid & 63;
-    if (tid < 4) grid[tid] = grid4[tid];
     uint32_t const s = colIndex[b];
-    float const *cp = cubepos + 4*size_t(rowindx[b]);
-    float const R2f = float(grid4[3]*grid4[3]);
     T acc[64];
 #pragma unroll
     for (int i = 0; i < 64; ++i) acc[i] = T(0);
     uint64_t mask_all = 0;
-    for (uint32_t k = add_start[b]; k < add_start[b + 1]; ++k) {
-        uint32_t const a = add_col[k];
+    int buf = 0;
+    for (uint32_t k = add_start[b]; k < add_start[b + 1]; ++k, buf ^= 1) {
+        uint32_t const a = add_col[k], slot = add_slot[k];
         int const lmax = img_lmax[a];
+        stage_table<T, LM>(Hs[buf], slot_H, stride, slot, lmax, tid);
+        uint64_t const mask = slot_mask[slot];
         __syncthreads();
-        hermite_tables<T, LM>(H, xi2, tid, lmax, img_pos + 4*size_t(a), cp, grid);
-        __syncthreads();
-        T const *c = cad + (size_t(img_starts[a])*nrhs + s)*128 + reim*64 + j;
-        uint64_t mask = 0;
-#pragma unroll
-        for (int z = 0; z < 4; ++z)
-#pragma unroll
-            for (int yy = 0; yy < 4; ++yy)
-#pragma unroll
-                for (int xx = 0; xx < 4; ++xx)
-                    if (in_mask(xi2, R2f, xx, yy, z)) mask |= 1ull << ((z*4 + yy)*4 + xx);
         if (!mask) continue;
         mask_all |= mask;
+        T (*H)[3][4] = Hs[buf];
+        T const *c = cad + (size_t(img_starts[a])*nrhs + s)*128 + reim*64 + j;
         int sho = 0;
         for (int iz = 0; iz <= lmax; ++iz) {
             T byx[4][4];
@@ -524,8 +484,9 @@ void launch_project_L(DevicePlan &dp, T const *x, cudaStream_t st) {
     sho_project_kernel<T, L><<<grid, 128, 0, st>>>(
         dptr<T>(dp.apc), x, dp.nCols, dptr<uint32_t>(g.images), dp.nAI,
         dptr<uint32_t>(dp.prj_start), dptr<uint32_t>(dp.prj_col), dptr<uint64_t>(dp.prj_coloff),
-        dptr<double>(dp.img_pos), dptr<uint32_t>(dp.img_starts), dptr<uint32_t>(dp.rowindx),
-        dptr<float>(dp.rowCubePos), dptr<double>(dp.grid_dev));
+        dptr<uint32_t>(dp.prj_slot), dptr<double>(dp.slot_H), dptr<uint64_t>(dp.slot_mask), dp.table_stride,
+        dptr<uint32_t>(dp.img_starts));
+        count_launch();
 }
 
 } // namespace
@@ -540,12 +501,16 @@ bool launch_local(DevicePlan &dp, T *y, T const *x, cudaStream_t st) {
         for (int d = 0; d < 3; ++d) for (int s = 0; s < 2; ++s) for (int c = 0; c < 2; ++c) a.ph[d][s][c] = T(dp.phase[d][s][c]);
         constexpr int S = (sizeof(T) == 8) ? 8 : 16;
         unsigned const nblk = dp.nlists[2]*(64/S);
-        if (nblk) local_fused_kernel<T, S><<<nblk, S*16, 0, st>>>(y, x, dptr<uint32_t>(dp.lists_start[2]),
-            dptr<int32_t>(dp.lists[2]), dptr<int32_t>(dp.nbr), dptr<int32_t>(dp.veff_index), vcell<T>(dp), a);
+        if (nblk) {
+            local_fused_kernel<T, S><<<nblk, S*16, 0, st>>>(y, x, dptr<uint32_t>(dp.lists_start[2]),
+                dptr<int32_t>(dp.lists[2]), dptr<int32_t>(dp.nbr), dptr<int32_t>(dp.veff_index), vcell<T>(dp), a);
+            count_launch();
+        }
     } else {
         unsigned const nb = std::min<uint32_t>(dp.nnzb, 148u*16);
         potential_kernel<T><<<nb, 256, 0, st>>>(y, x, dptr<int32_t>(dp.veff_index), vcell<T>(dp), dp.nnzb,
                                                 T(dp.E_re), T(dp.E_im));
+        count_launch();
         for (int d = 0; d < 3; ++d) {
             int const nFD = dp.FD_range[d];
             if (nFD < 1 || 0 == dp.nlists[d]) continue;
@@ -569,6 +534,7 @@ bool launch_local(DevicePlan &dp, T *y, T const *x, cudaStream_t st) {
                               dptr<int32_t>(dp.lists[d]), 1 << (2*d), coef, pl_r, pl_i, pr_r, pr_i);
             else kinetic_list_kernel<T, 1><<<grid, 64, 0, st>>>(y, x, dptr<uint32_t>(dp.lists_start[d]),
                               dptr<int32_t>(dp.lists[d]), 1 << (2*d), coef, pl_r, pl_i, pr_r, pr_i);
+            count_launch();
         }
     }
     A43G_CUDA_TRY(cudaGetLastError());
@@ -579,27 +545,42 @@ template <typename T>
 bool launch_dyadic(DevicePlan &dp, T *y, T const *x, uint16_t const *colIndex, cudaStream_t st) {
     if (dp.nAI < 1 || dp.nCols < 1) return true;
     if (!ensure_dyadic_scratch(dp, sizeof(T))) return false;
-    launch_project_L<T, 0>(dp, x, st); launch_project_L<T, 1>(dp, x, st);
-    launch_project_L<T, 2>(dp, x, st); launch_project_L<T, 3>(dp, x, st);
-    launch_project_L<T, 4>(dp, x, st); launch_project_L<T, 5>(dp, x, st);
-    launch_project_L<T, 6>(dp, x, st); launch_project_L<T, 7>(dp, x, st);
+    bool const tc = (sizeof(T) == 4) && dp.use_tc && tc_projector_supported(dp);
+    if (tc) {
+        if (!launch_project_tc(dp, (float const*)x, st)) return false;
+    } else {
+        launch_project_L<T, 0>(dp, x, st); launch_project_L<T, 1>(dp, x, st);
+        launch_project_L<T, 2>(dp, x, st); launch_project_L<T, 3>(dp, x, st);
+        launch_project_L<T, 4>(dp, x, st); launch_project_L<T, 5>(dp, x, st);
+        launch_project_L<T, 6>(dp, x, st); launch_project_L<T, 7>(dp, x, st);
+    }
     dim3 const ga(dp.nAtoms, dp.nCols);
     if (dp.nAI > dp.nAtoms) {
         sho_collect_kernel<T><<<ga, 64, 0, st>>>(dptr<double>(dp.aac), dptr<T>(dp.apc), dp.nCols,
             dptr<uint32_t>(dp.atom_starts), dptr<int8_t>(dp.atom_lmax), dptr<uint32_t>(dp.sum_start),
             dptr<uint32_t>(dp.sum_col), dptr<uint32_t>(dp.img_starts), dptr<double>(dp.img_phase));
+        count_launch();
         sho_mul_kernel<double, double><<<ga, 64, 0, st>>>(dptr<double>(dp.cadd), dptr<double>(dp.aac), dp.nCols,
             dptr<uint32_t>(dp.atom_starts), dptr<int8_t>(dp.atom_lmax), dptr<double>(dp.atom_mat), dptr<uint32_t>(dp.atom_mat_off));
+        count_launch();
         sho_broadcast_kernel<T><<<ga, 64, 0, st>>>(dptr<T>(dp.cad), dptr<double>(dp.cadd), dp.nCols,
             dptr<uint32_t>(dp.atom_starts), dptr<int8_t>(dp.atom_lmax), dptr<uint32_t>(dp.sum_start),
             dptr<uint32_t>(dp.sum_col), dptr<uint32_t>(dp.img_starts), dptr<double>(dp.img_phase));
+        count_launch();
     } else {
         sho_mul_kernel<T, T><<<ga, 64, 0, st>>>(dptr<T>(dp.cad), dptr<T>(dp.apc), dp.nCols,
             dptr<uint32_t>(dp.atom_starts), dptr<int8_t>(dp.atom_lmax), dptr<double>(dp.atom_mat), dptr<uint32_t>(dp.atom_mat_off));
+        count_launch();
     }
-    sho_add_kernel<T><<<dp.nnzb, 128, 0, st>>>(y, dptr<T>(dp.cad), dp.nCols, dp.nnzb, colIndex,
-        dptr<uint32_t>(dp.add_start), dptr<uint32_t>(dp.add_col), dptr<double>(dp.img_pos), dptr<int8_t>(dp.img_lmax),
-        dptr<uint32_t>(dp.img_starts), dptr<uint32_t>(dp.rowindx), dptr<float>(dp.rowCubePos), dptr<double>(dp.grid_dev));
+    if (tc) {
+        if (!launch_add_tc(dp, (float*)y, colIndex, st)) return false;
+    } else {
+        sho_add_kernel<T><<<dp.nnzb, 128, 0, st>>>(y, dptr<T>(dp.cad), dp.nCols, dp.nnzb, colIndex,
+            dptr<uint32_t>(dp.add_start), dptr<uint32_t>(dp.add_col), dptr<uint32_t>(dp.add_slot),
+            dptr<double>(dp.slot_H), dptr<uint64_t>(dp.slot_mask), dp.table_stride,
+            dptr<int8_t>(dp.img_lmax), dptr<uint32_t>(dp.img_starts));
+        count_launch();
+    }
     A43G_CUDA_TRY(cudaGetLastError());
     return true;
 }

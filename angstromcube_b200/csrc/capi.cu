@@ -3,6 +3,7 @@
 #include "device.cuh"
 #include "solver.hpp"
 
+#include <atomic>
 #include <cstring>
 #include <mutex>
 #include <new>
@@ -20,8 +21,10 @@ struct a43g_plan {
 namespace a43g {
 namespace {
 thread_local std::string g_error;
+std::atomic<uint64_t> g_launches{0};
 }
 void set_error(std::string const &msg) { g_error = msg; }
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 } // namespace a43g
 
 using a43g::set_error;
@@ -208,6 +211,38 @@ int a43g_action_multiply(a43g_plan_t *plan, void *y, const void *x, const uint16
     if (!ok) return A43G_ERR_CUDA;
     if (flops) *flops = a43g::action_flops(plan->host, (A43G_F64 == dtype) ? 8 : 4);
     return A43G_OK;
+}
+
+int a43g_action_part(a43g_plan_t *plan, int part, void *y, const void *x, void *stream, int dtype) {
+    if (!plan || !y || !x) return fail(A43G_ERR_ARGUMENT, "null argument");
+    std::lock_guard<std::mutex> lock(plan->mtx);
+    if (!plan->energy_set) return fail(A43G_ERR_STATE, "energy parameter not set (a43g_plan_set_energy)");
+    int const rc = ensure_device(plan);
+    if (rc) return rc;
+    auto const st = (cudaStream_t)stream;
+    auto const *ci = a43g::dptr<uint16_t>(plan->dev.colindx);
+    bool ok;
+    if (0 == part && A43G_F64 == dtype) ok = a43g::launch_local<double>(plan->dev, (double*)y, (double const*)x, st);
+    else if (0 == part && A43G_F32 == dtype) ok = a43g::launch_local<float>(plan->dev, (float*)y, (float const*)x, st);
+    else if (1 == part && A43G_F64 == dtype) ok = a43g::launch_dyadic<double>(plan->dev, (double*)y, (double const*)x, ci, st);
+    else if (1 == part && A43G_F32 == dtype) ok = a43g::launch_dyadic<float>(plan->dev, (float*)y, (float const*)x, ci, st);
+    else return fail(A43G_ERR_ARGUMENT, "part must be 0 or 1, dtype A43G_F64 or A43G_F32");
+    return ok ? A43G_OK : A43G_ERR_CUDA;
+}
+
+uint64_t a43g_kernel_launches(void) { return a43g::g_launches.load(); }
+
+int a43g_plan_device_status(a43g_plan_t *plan) {
+    if (!plan) return fail(A43G_ERR_ARGUMENT, "null argument");
+    std::lock_guard<std::mutex> lock(plan->mtx);
+    if (cudaSuccess != cudaDeviceSynchronize()) return fail(A43G_ERR_CUDA, cudaGetErrorString(cudaGetLastError()));
+    if (!plan->dev.dev_error.ptr) return A43G_OK;
+    int32_t code = 0;
+    if (cudaSuccess != cudaMemcpy(&code, plan->dev.dev_error.ptr, 4, cudaMemcpyDeviceToHost)) return fail(A43G_ERR_CUDA, "copy of the error flag");
+    if (0 == code) return A43G_OK;
+    cudaMemset(plan->dev.dev_error.ptr, 0, 4);
+    return fail(A43G_ERR_CUDA, std::string("a kernel recorded error ") + std::to_string(code) +
+                (code <= 2 ? " (tensor-core projector wait timed out)" : ""));
 }
 
 int a43g_solve(a43g_plan_t *plan, const a43g_solve_options_t *opts, void *X, double *rho,

@@ -12,6 +12,8 @@ namespace a43g {
 
 // error state of the calling host thread (capi.cu)
 void set_error(std::string const &msg);
+// kernel launch counter (instrumentation, capi.cu)
+void count_launch();
 #define A43G_CUDA_TRY(call) do { cudaError_t e_ = (call); if (cudaSuccess != e_) { \
     ::a43g::set_error(std::string(#call) + ": " + cudaGetErrorString(e_)); return false; } } while (0)
 
@@ -58,6 +60,10 @@ struct DevicePlan {
     DeviceBuffer atom_starts, atom_lmax, atom_mat, atom_mat_off;
     DeviceBuffer grid_dev;       // double [4]: hx, hy, hz, projection radius
     DeviceBuffer subset_dev;     // uint32 [nCols] diagonal block of each source column
+    DeviceBuffer slot_H, slot_mask, prj_slot, add_slot;   // projector tables per (image, row)
+    int table_stride = 0;        // doubles per slot in slot_H
+    DeviceBuffer dev_error;      // int: first error code recorded by a kernel (0: none)
+    bool use_tc = true;          // FP32 projector on the tensor cores (else SIMT)
     struct ImageGroup { uint32_t count = 0; DeviceBuffer images; } img_group[8];  // images by basis size
     // scratch of the dyadic part (allocated once per plan, never per call)
     DeviceBuffer apc;            // real_t [ncoeffI*nCols][2][64] image projection coefficients
@@ -81,5 +87,10 @@ template <typename T>
 bool launch_dyadic(DevicePlan &dp, T *y, T const *x, uint16_t const *colIndex, cudaStream_t s);
 
 double action_flops(GreenPlan const &hp, int real_bytes);
+
+// tensor-core (tcgen05, 3xTF32) projection and addition of the FP32 action (projector_tc.cu)
+bool tc_projector_supported(DevicePlan const &dp);
+bool launch_project_tc(DevicePlan &dp, float const *x, cudaStream_t st);
+bool launch_add_tc(DevicePlan &dp, float *y, uint16_t const *colIndex, cudaStream_t st);
 
 } // namespace a43g

@@ -2,6 +2,7 @@
 #include "device.cuh"
 
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 
 namespace a43g {
@@ -115,6 +116,15 @@ bool upload_plan(GreenPlan const &hp, DevicePlan &dp) {
         if (!put(dp.img_group[L].images, imgs)) return false;
     }
     if (dp.lmax_max > 7) { set_error("projector basis sizes above numax 7 are not supported"); return false; }
+    dp.table_stride = (hp.table_lmax + 1)*12;
+    if (!put(dp.slot_H, hp.slot_H) || !put(dp.slot_mask, hp.slot_mask)) return false;
+    if (!put(dp.prj_slot, hp.prj_slot) || !put(dp.add_slot, hp.add_slot)) return false;
+    if (!put(dp.subset_dev, hp.subset)) return false;
+    if (!put(dp.dev_error, std::vector<int32_t>(4, 0))) return false;
+    {
+        char const *e = std::getenv("A43G_PROJECTOR");          // "simt" selects the SIMT projector
+        dp.use_tc = !(e && 0 == std::strcmp(e, "simt"));
+    }
     if (!dp.aac.alloc(std::max<size_t>(16, size_t(dp.ncoeffA)*dp.nCols*128*sizeof(double)))) return false;
     if (!dp.cadd.alloc(std::max<size_t>(16, size_t(dp.ncoeffA)*dp.nCols*128*sizeof(double)))) return false;
     dp.uploaded = true;

@@ -90,6 +90,14 @@ struct GreenPlan {
     Csr SHOadd;                                // rows: blocks, cols: atom images
     std::vector<Csr> SHOprj;                   // [nCols] rows: atom images, cols: blocks
     Csr SHOsum;                                // rows: atoms, cols: atom images
+    // projector tables per (atom image, target row) slot, shared by every source column:
+    // 1D Hermite-Gauss functions H[nu][dir][i4] (nu <= lmax_max) and the 64-point spherical mask
+    Csr img_rows;                              // rows: atom images, cols: target rows hit (slot = position)
+    int table_lmax = -1;                       // nu range of the tables
+    std::vector<double>   slot_H;              // [nslots][(table_lmax+1)*12]
+    std::vector<uint64_t> slot_mask;           // [nslots]
+    std::vector<uint32_t> prj_slot;            // aligned with the concatenated SHOprj columns
+    std::vector<uint32_t> add_slot;            // aligned with SHOadd.col
     std::vector<uint32_t> AtomMatOffset;       // [nAtoms + 1] offsets into matrix storage (2*nc*nc each)
     std::vector<double>   AtomMatricesIn;      // per contributing atom: [2][nc][nc] (hmt, ovl) rescaled
     std::vector<double>   AtomMatrices;        // per contributing atom: [2][nc][nc] (re, im) of dVol (H - E S)

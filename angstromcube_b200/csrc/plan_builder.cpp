@@ -407,6 +407,68 @@ std::string GreenPlan::build(Geometry const &g) {
     SHOprj.resize(nrhs);
     for (size_t s = 0; s < nrhs; ++s) SHOprj[s] = to_csr(prj[s]);
 
+    // projector tables per (image, row) slot (include/green_dyadic.hxx:33-107 evaluates them
+    // per (image, block) on the fly; here once, on the host, in the CPU order of operations)
+    img_rows = to_csr(cubes);
+    table_lmax = -1;
+    for (auto const &im : images) table_lmax = std::max(table_lmax, int(g.xyzZinso[im.ia*8 + 5]));
+    {
+        int const nt = (table_lmax + 1)*12;
+        size_t const nslots = img_rows.nnz();
+        slot_H.assign(nslots*size_t(std::max(nt, 1)), 0.0);
+        slot_mask.assign(nslots, 0);
+        double const R2 = g.proj_radius*g.proj_radius;
+        float const R2f = float(R2);
+        for (uint32_t a = 0; a < nAI; ++a) {
+            auto const &im = images[a];
+            int const lmax = int(g.xyzZinso[im.ia*8 + 5]);
+            double const isq = 1./std::sqrt(g.xyzZinso[im.ia*8 + 6]);   // stored as 1/sqrt(sigma)
+            double const sinv = isq*isq;
+            for (uint32_t k = img_rows.start[a]; k < img_rows.start[a + 1]; ++k) {
+                float const *tc = &rowCubePos[4*size_t(img_rows.col[k])];
+                double *H = &slot_H[size_t(k)*nt];
+                float xi2[3][4];
+                for (int d = 0; d < 3; ++d)
+                    for (int i4 = 0; i4 < 4; ++i4) {
+                        double const xi = sinv*((double(tc[d])*4 + i4 + 0.5)*g.hg[d] - im.pos[d]);
+                        double const x2 = xi*xi;
+                        xi2[d][i4] = float(x2);
+                        double hm = 0, h = (x2 < R2) ? std::exp(-0.5*x2) : 0.0;
+                        H[(0*3 + d)*4 + i4] = h;
+                        for (int nu = 0; nu < lmax; ++nu) {
+                            double const hp = xi*h - 0.5*nu*hm;
+                            H[((nu + 1)*3 + d)*4 + i4] = hp;
+                            hm = h; h = hp;
+                        }
+                    }
+                uint64_t mask = 0;   // ((xi2_z - R2) + xi2_y) + xi2_x < 0 in float
+                for (int z = 0; z < 4; ++z) {
+                    float const d2z = xi2[2][z] - R2f;
+                    for (int y = 0; y < 4; ++y) {
+                        float const d2yz = xi2[1][y] + d2z;
+                        for (int x = 0; x < 4; ++x)
+                            if (xi2[0][x] + d2yz < 0.f) mask |= 1ull << ((z*4 + y)*4 + x);
+                    }
+                }
+                slot_mask[k] = mask;
+            }
+        }
+        // slot of every projection and addition pair
+        prj_slot.clear(); add_slot.assign(SHOadd.nnz(), 0);
+        auto slot = [&](uint32_t a, uint32_t row) -> uint32_t {
+            // rows of one image are sorted ascending (target rows scanned in order)
+            auto const b = img_rows.col.begin() + img_rows.start[a], e = img_rows.col.begin() + img_rows.start[a + 1];
+            return uint32_t(std::lower_bound(b, e, row) - img_rows.col.begin());
+        };
+        for (size_t s = 0; s < nrhs; ++s)
+            for (uint32_t a = 0; a < nAI; ++a)
+                for (uint32_t k = SHOprj[s].start[a]; k < SHOprj[s].start[a + 1]; ++k)
+                    prj_slot.push_back(slot(a, rowindx[SHOprj[s].col[k]]));
+        for (uint32_t b = 0; b < nnz; ++b)
+            for (uint32_t k = SHOadd.start[b]; k < SHOadd.start[b + 1]; ++k)
+                add_slot[k] = slot(SHOadd.col[k], rowindx[b]);
+    }
+
     // contributing atom copies, their matrices and the image -> atom relation
     std::vector<int32_t> iac_of_iaa(nAtomCopies, -1);
     global_atom_ids.clear();

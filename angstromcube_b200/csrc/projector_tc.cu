@@ -1,0 +1,324 @@
+// FP32 projector contraction of the action on the sm_100a tensor cores (tcgen05, kind::tf32,
+// 3xTF32 split precision, FP32 accumulation in TMEM).
+//
+// Projection (include/green_dyadic.hxx:112-288), one CTA per (atom image a, source s):
+//     C^T[(reim, j), sho] = sum over the blocks b of s near a:  X[b]^T (128 x 64) . P[a,b]^T (64 x 64)
+//   M = 128 (real and imaginary planes x 64 source columns), N = 64 (nSHO <= 56 padded),
+//   K = 64 grid points per block.
+// Addition (include/green_dyadic.hxx:325-518), one CTA per block b:
+//     D[(reim, j), i] = sum over the images a near b:  Cad[a, s]^T (128 x 64) . P[a,b] (64 x 64)
+//   and y[b] += D^T on the points inside the projection spheres.
+// P[sho][i] = H_ix(x_i) H_iy(y_i) H_iz(z_i) on the mask (tables of the plan), 0 elsewhere.
+// Each operand x is split x = hi + lo with hi = TF32(x); C = A_hi B_hi + A_hi B_lo + A_lo B_hi.
+// Operands are staged by all threads into shared memory (double-buffered stages), one thread
+// issues the MMAs and commits them to an mbarrier; every wait is bounded and a timeout is
+// recorded in the device error flag instead of hanging.
+#include "device.cuh"
+#include "tc_sm100.cuh"
+
+namespace a43g {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kA = 32768;            // bytes of one 128 x 64 FP32 operand
+constexpr int kB = 16384;            // bytes of one 64 x 64 FP32 operand
+constexpr int kStage = 2*kA + 2*kB;  // A_hi, A_lo, B_hi, B_lo
+constexpr int kSmem = 2*kStage + 1024;
+constexpr uint64_t kWaitNs = 2000000000ull;   // 2 s per wait: far beyond any MMA latency
+constexpr uint32_t kIdesc = tc::idesc_tf32(128, 64, true, false);   // A MN-major, B K-major
+
+// byte offset of element (m, k) of a 128 x 64 MN-major operand (core matrices 8 k x 4 m)
+__device__ __forceinline__ uint32_t offA(int m, int k) { return ((k >> 3)*32 + (m >> 2))*128 + ((k & 7)*4 + (m & 3))*4; }
+// byte offset of element (n, k) of a 64 x 64 K-major operand (core matrices 8 n x 4 k)
+__device__ __forceinline__ uint32_t offB(int n, int k) { return ((k >> 2)*8 + (n >> 3))*128 + ((n & 7)*4 + (k & 3))*4; }
+
+// issue the 8 K-steps x 3 split products of one 64-deep chunk
+__device__ __forceinline__ void issue_mmas(uint32_t tmem, uint32_t sA_hi, uint32_t sA_lo, uint32_t sB_hi,
+                                           uint32_t sB_lo, bool first) {
+#pragma unroll
+    for (int s = 0; s < 8; ++s) {
+        uint64_t const ah = tc::smem_desc(sA_hi + s*4096, 4096, 128), al = tc::smem_desc(sA_lo + s*4096, 4096, 128);
+        uint64_t const bh = tc::smem_desc(sB_hi + s*2048, 1024, 128), bl = tc::smem_desc(sB_lo + s*2048, 1024, 128);
+        tc::mma_tf32(tmem, ah, bh, kIdesc, (first && 0 == s) ? 0u : 1u);
+        tc::mma_tf32(tmem, ah, bl, kIdesc, 1u);
+        tc::mma_tf32(tmem, al, bh, kIdesc, 1u);
+    }
+}
+
+// stage a 128 x 64 FP32 matrix, element (m = reim*64 + j, k) at src[reim*plane + k*ld_k + j],
+// as the split MN-major operand; rows k >= kmax are zero
+__device__ __forceinline__ void stage_A(char *sA_hi, char *sA_lo, float const *__restrict__ src, size_t plane,
+                                        size_t ld_k, int kmax, int tid) {
+#pragma unroll 4
+    for (int r = 0; r < 2048/kThreads; ++r) {
+        int const q = r*kThreads + tid;
+        int const kl = q & 7, mg = (q >> 3) & 31, kg = q >> 8;
+        int const k = kg*8 + kl, m = mg*4;
+        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (k < kmax) v = __ldg(reinterpret_cast<float4 const*>(src + (m >> 6)*plane + size_t(k)*ld_k + (m & 63)));
+        float4 h, l;
+        tc::split_tf32(v.x, h.x, l.x); tc::split_tf32(v.y, h.y, l.y);
+        tc::split_tf32(v.z, h.z, l.z); tc::split_tf32(v.w, h.w, l.w);
+        uint32_t const o = offA(m, k);
+        *reinterpret_cast<float4*>(sA_hi + o) = h;
+        *reinterpret_cast<float4*>(sA_lo + o) = l;
+    }
+}
+
+struct ShoIdx { uint8_t ix[64], iy[64], iz[64]; };
+
+__device__ __forceinline__ void fill_sho_index(ShoIdx &t, int lmax, int tid) {
+    if (0 == tid) {
+        int sho = 0;
+        for (int iz = 0; iz <= lmax; ++iz)
+            for (int iy = 0; iy <= lmax - iz; ++iy)
+                for (int ix = 0; ix <= lmax - iz - iy; ++ix, ++sho) { t.ix[sho] = ix; t.iy[sho] = iy; t.iz[sho] = iz; }
+    }
+}
+
+__device__ __forceinline__ float pval(float const (*H)[3][4], ShoIdx const &t, uint64_t mask, int sho, int nsho, int i) {
+    if (sho >= nsho || !((mask >> i) & 1)) return 0.f;
+    return H[t.ix[sho]][0][i & 3]*H[t.iy[sho]][1][(i >> 2) & 3]*H[t.iz[sho]][2][i >> 4];
+}
+
+__device__ __forceinline__ void record_error(int *err, int code) { atomicCAS(err, 0, code); }
+
+// ---------------------------------------------------------------- projection
+
+__global__ void __launch_bounds__(kThreads, 1)
+sho_project_tc_kernel(float *__restrict__ apc, float const *__restrict__ x, uint32_t nrhs,
+                      uint32_t const *__restrict__ images, uint32_t nAI, uint32_t const *__restrict__ prj_start,
+                      uint32_t const *__restrict__ prj_col, uint64_t const *__restrict__ prj_coloff,
+                      uint32_t const *__restrict__ prj_slot, double const *__restrict__ slot_H,
+                      uint64_t const *__restrict__ slot_mask, int stride, uint32_t const *__restrict__ img_starts,
+                      int8_t const *__restrict__ img_lmax, int *err)
+{
+    extern __shared__ __align__(1024) char smem[];
+    __shared__ float Hs[2][8][3][4];
+    __shared__ ShoIdx sidx;
+    __shared__ uint64_t mbar[2];
+    __shared__ uint32_t tmem_base;
+    int const tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    uint32_t const a = images[blockIdx.x];
+    int const s = blockIdx.y;
+    int const lmax = img_lmax[a], nsho = ((lmax + 1)*(lmax + 2)*(lmax + 3))/6;
+    uint32_t const *start = prj_start + size_t(s)*(nAI + 1);
+    uint64_t const off = prj_coloff[s];
+    uint32_t const k0 = start[a], k1 = start[a + 1];
+    float *out = apc + (size_t(img_starts[a])*nrhs + s)*128;
+    if (k0 == k1) {                                  // no block: zero coefficients
+        for (int e = tid; e < nsho*128; e += kThreads) out[size_t(e >> 7)*nrhs*128 + (e & 127)] = 0.f;
+        return;
+    }
+    fill_sho_index(sidx, lmax, tid);
+    if (0 == warp) tc::tmem_alloc(&tmem_base, 64);
+    if (0 == tid) { tc::mbar_init(&mbar[0], 1); tc::mbar_init(&mbar[1], 1); }
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    uint32_t const tmem = tmem_base;
+    bool ok = true;
+    int issued = 0;                                  // commits issued (block-uniform)
+    for (uint32_t k = k0; k < k1; ++k) {
+        int const it = int(k - k0), st = it & 1;
+        char *sA_hi = smem + st*kStage, *sA_lo = sA_hi + kA, *sB_hi = sA_lo + kA, *sB_lo = sB_hi + kB;
+        if (it >= 2) {                               // stage st is free once the MMAs of it-2 completed
+            bool w = true;
+            if (0 == tid) w = tc::mbar_wait(&mbar[st], uint32_t((it - 2) >> 1) & 1u, kWaitNs);
+            ok = __syncthreads_and(w);               // block-uniform decision
+            if (!ok) break;
+        }
+        uint32_t const b = prj_col[off + k], slot = prj_slot[off + k];
+        if (tid < (lmax + 1)*12) (&Hs[st][0][0][0])[tid] = float(slot_H[size_t(slot)*stride + tid]);
+        uint64_t const mask = slot_mask[slot];
+        stage_A(sA_hi, sA_lo, x + size_t(b)*8192, 4096, 64, 64, tid);   // A = X^T: m = (reim, j), k = point i
+        __syncthreads();                             // tables staged
+        // B = P^T: n = sho, k = point i; float4 along k
+#pragma unroll 2
+        for (int r = 0; r < 1024/kThreads; ++r) {
+            int const q = r*kThreads + tid;
+            int const n = ((q >> 3) & 7)*8 + (q & 7), kc = q >> 6;
+            float4 v;
+            v.x = pval(Hs[st], sidx, mask, n, nsho, kc*4 + 0); v.y = pval(Hs[st], sidx, mask, n, nsho, kc*4 + 1);
+            v.z = pval(Hs[st], sidx, mask, n, nsho, kc*4 + 2); v.w = pval(Hs[st], sidx, mask, n, nsho, kc*4 + 3);
+            float4 h, l;
+            tc::split_tf32(v.x, h.x, l.x); tc::split_tf32(v.y, h.y, l.y);
+            tc::split_tf32(v.z, h.z, l.z); tc::split_tf32(v.w, h.w, l.w);
+            uint32_t const o = offB(n, kc*4);
+            *reinterpret_cast<float4*>(sB_hi + o) = h;
+            *reinterpret_cast<float4*>(sB_lo + o) = l;
+        }
+        tc::fence_smem_to_async();
+        __syncthreads();
+        if (0 == tid) {
+            tc::fence_after_sync();
+            issue_mmas(tmem, tc::smem_u32(sA_hi), tc::smem_u32(sA_lo), tc::smem_u32(sB_hi), tc::smem_u32(sB_lo), 0 == it);
+            tc::commit(&mbar[st]);
+        }
+        ++issued;
+    }
+    int const last = issued - 1;
+    if (last >= 0) {
+        bool w = ok;
+        if (0 == tid && ok) w = tc::mbar_wait(&mbar[last & 1], uint32_t(last >> 1) & 1u, kWaitNs);
+        ok = __syncthreads_and(w);
+    }
+    if (!ok && 0 == tid && last >= 0) {
+        record_error(err, 1);
+        // give the tensor core a bounded grace period before the TMEM is released
+        tc::mbar_wait(&mbar[last & 1], uint32_t(last >> 1) & 1u, kWaitNs);
+    }
+    tc::fence_after_sync();
+    if (ok) {
+        // warps w and w+4 share TMEM lane quarter w%4: columns 0-31 and 32-63
+        float v[32];
+        int const quarter = warp & 3, half = warp >> 2;
+        uint32_t const taddr = tmem + (uint32_t(quarter*32) << 16) + uint32_t(half*32);
+        tc::tmem_ld_32x32b_x32(taddr, v);
+        int const m = quarter*32 + lane;
+#pragma unroll
+        for (int c = 0; c < 32; ++c)
+            if (half*32 + c < nsho) out[size_t(half*32 + c)*nrhs*128 + m] = v[c];
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    if (0 == warp) tc::tmem_dealloc(tmem, 64);
+}
+
+// ---------------------------------------------------------------- addition
+
+__global__ void __launch_bounds__(kThreads, 1)
+sho_add_tc_kernel(float *__restrict__ y, float const *__restrict__ cad, uint32_t nrhs,
+                  uint16_t const *__restrict__ colIndex, uint32_t const *__restrict__ add_start,
+                  uint32_t const *__restrict__ add_col, uint32_t const *__restrict__ add_slot,
+                  double const *__restrict__ slot_H, uint64_t const *__restrict__ slot_mask, int stride,
+                  int8_t const *__restrict__ img_lmax, uint32_t const *__restrict__ img_starts, int *err)
+{
+    extern __shared__ __align__(1024) char smem[];
+    __shared__ float Hs[2][8][3][4];
+    __shared__ ShoIdx sidx[2];
+    __shared__ uint64_t mbar[2];
+    __shared__ uint32_t tmem_base;
+    int const tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    uint32_t const b = blockIdx.x;
+    uint32_t const k0 = add_start[b], k1 = add_start[b + 1];
+    if (k0 == k1) return;
+    uint32_t const s = colIndex[b];
+    if (0 == warp) tc::tmem_alloc(&tmem_base, 64);
+    if (0 == tid) { tc::mbar_init(&mbar[0], 1); tc::mbar_init(&mbar[1], 1); }
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    uint32_t const tmem = tmem_base;
+    uint64_t mask_all = 0;
+    bool ok = true;
+    int issued = 0;                                  // commits issued (block-uniform)
+    for (uint32_t k = k0; k < k1; ++k) {
+        int const it = int(k - k0), st = it & 1;
+        char *sA_hi = smem + st*kStage, *sA_lo = sA_hi + kA, *sB_hi = sA_lo + kA, *sB_lo = sB_hi + kB;
+        if (it >= 2) {                               // stage st is free once the MMAs of it-2 completed
+            bool w = true;
+            if (0 == tid) w = tc::mbar_wait(&mbar[st], uint32_t((it - 2) >> 1) & 1u, kWaitNs);
+            ok = __syncthreads_and(w);               // block-uniform decision
+            if (!ok) break;
+        }
+        uint32_t const a = add_col[k], slot = add_slot[k];
+        int const lmax = img_lmax[a], nsho = ((lmax + 1)*(lmax + 2)*(lmax + 3))/6;
+        fill_sho_index(sidx[st], lmax, tid);
+        if (tid < (lmax + 1)*12) (&Hs[st][0][0][0])[tid] = float(slot_H[size_t(slot)*stride + tid]);
+        uint64_t const mask = slot_mask[slot];
+        mask_all |= mask;
+        // A = Cad^T: m = (reim, j), k = sho (rows beyond nsho zero)
+        stage_A(sA_hi, sA_lo, cad + (size_t(img_starts[a])*nrhs + s)*128, 64, size_t(nrhs)*128, nsho, tid);
+        __syncthreads();
+        // B = P: n = point i, k = sho; float4 along sho
+#pragma unroll 2
+        for (int r = 0; r < 1024/kThreads; ++r) {
+            int const q = r*kThreads + tid;
+            int const n = ((q >> 3) & 7)*8 + (q & 7), kc = q >> 6;
+            float4 v;
+            v.x = pval(Hs[st], sidx[st], mask, kc*4 + 0, nsho, n); v.y = pval(Hs[st], sidx[st], mask, kc*4 + 1, nsho, n);
+            v.z = pval(Hs[st], sidx[st], mask, kc*4 + 2, nsho, n); v.w = pval(Hs[st], sidx[st], mask, kc*4 + 3, nsho, n);
+            float4 h, l;
+            tc::split_tf32(v.x, h.x, l.x); tc::split_tf32(v.y, h.y, l.y);
+            tc::split_tf32(v.z, h.z, l.z); tc::split_tf32(v.w, h.w, l.w);
+            uint32_t const o = offB(n, kc*4);
+            *reinterpret_cast<float4*>(sB_hi + o) = h;
+            *reinterpret_cast<float4*>(sB_lo + o) = l;
+        }
+        tc::fence_smem_to_async();
+        __syncthreads();
+        if (0 == tid) {
+            tc::fence_after_sync();
+            issue_mmas(tmem, tc::smem_u32(sA_hi), tc::smem_u32(sA_lo), tc::smem_u32(sB_hi), tc::smem_u32(sB_lo), 0 == it);
+            tc::commit(&mbar[st]);
+        }
+        ++issued;
+    }
+    int const last = issued - 1;
+    if (last >= 0) {
+        bool w = ok;
+        if (0 == tid && ok) w = tc::mbar_wait(&mbar[last & 1], uint32_t(last >> 1) & 1u, kWaitNs);
+        ok = __syncthreads_and(w);
+    }
+    if (!ok && 0 == tid && last >= 0) {
+        record_error(err, 2);
+        // give the tensor core a bounded grace period before the TMEM is released
+        tc::mbar_wait(&mbar[last & 1], uint32_t(last >> 1) & 1u, kWaitNs);
+    }
+    tc::fence_after_sync();
+    if (ok && mask_all) {
+        float v[32];
+        int const quarter = warp & 3, half = warp >> 2;
+        uint32_t const taddr = tmem + (uint32_t(quarter*32) << 16) + uint32_t(half*32);
+        tc::tmem_ld_32x32b_x32(taddr, v);
+        int const m = quarter*32 + lane, reim = m >> 6, j = m & 63;
+        float *yb = y + size_t(b)*8192 + reim*4096 + size_t(half*32)*64 + j;
+        uint32_t const mk = uint32_t(mask_all >> (half*32));
+#pragma unroll
+        for (int i = 0; i < 32; ++i)
+            if ((mk >> i) & 1u) yb[i*64] += v[i];
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    if (0 == warp) tc::tmem_dealloc(tmem, 64);
+}
+
+} // namespace
+
+bool tc_projector_supported(DevicePlan const &dp) { return dp.lmax_max >= 0 && dp.lmax_max <= 5; }
+
+bool launch_project_tc(DevicePlan &dp, float const *x, cudaStream_t st) {
+    static bool attr = false;
+    if (!attr) {
+        A43G_CUDA_TRY(cudaFuncSetAttribute(sho_project_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmem));
+        A43G_CUDA_TRY(cudaFuncSetAttribute(sho_add_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmem));
+        attr = true;
+    }
+    for (int L = 0; L < 8; ++L) {
+        auto const &g = dp.img_group[L];
+        if (0 == g.count) continue;
+        dim3 const grid(g.count, dp.nCols);
+        sho_project_tc_kernel<<<grid, kThreads, kSmem, st>>>(dptr<float>(dp.apc), x, dp.nCols,
+            dptr<uint32_t>(g.images), dp.nAI, dptr<uint32_t>(dp.prj_start), dptr<uint32_t>(dp.prj_col),
+            dptr<uint64_t>(dp.prj_coloff), dptr<uint32_t>(dp.prj_slot), dptr<double>(dp.slot_H),
+            dptr<uint64_t>(dp.slot_mask), dp.table_stride, dptr<uint32_t>(dp.img_starts), dptr<int8_t>(dp.img_lmax),
+            dptr<int>(dp.dev_error));
+        count_launch();
+    }
+    A43G_CUDA_TRY(cudaGetLastError());
+    return true;
+}
+
+bool launch_add_tc(DevicePlan &dp, float *y, uint16_t const *colIndex, cudaStream_t st) {
+    sho_add_tc_kernel<<<dp.nnzb, kThreads, kSmem, st>>>(y, dptr<float>(dp.cad), dp.nCols, colIndex,
+        dptr<uint32_t>(dp.add_start), dptr<uint32_t>(dp.add_col), dptr<uint32_t>(dp.add_slot),
+        dptr<double>(dp.slot_H), dptr<uint64_t>(dp.slot_mask), dp.table_stride, dptr<int8_t>(dp.img_lmax),
+        dptr<uint32_t>(dp.img_starts), dptr<int>(dp.dev_error));
+    count_launch();
+    A43G_CUDA_TRY(cudaGetLastError());
+    return true;
+}
+
+} // namespace a43g

@@ -17,6 +17,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <vector>
 
 namespace a43g {
@@ -158,8 +159,10 @@ __global__ void __launch_bounds__(256) k_C(T *W, T const *AU1, T const *AU2, uin
 }
 
 // K_DX: X += cu1x U1 + cu2x U2 + cdx D ; D = U2 + cu1d U1 + cdd D ; U1 = W + beta U2
-template <typename T>
-__global__ void __launch_bounds__(256) k_DX(T *X, T *D, T *U1, T const *U2, T const *W, uint32_t nnzb,
+// (X may be kept in FP64 while the recurrence vectors are FP32: the solution then carries no
+// FP32 rounding, which lowers the residual floor of an FP32 sweep)
+template <typename T, typename TX>
+__global__ void __launch_bounds__(256) k_DX(TX *X, T *D, T *U1, T const *U2, T const *W, uint32_t nnzb,
                                             uint16_t const *colindx, ColState const *cs) {
     int const j = threadIdx.x & 63, q = threadIdx.x >> 6;
     for (uint32_t b = blockIdx.x; b < nnzb; b += gridDim.x) {
@@ -173,7 +176,7 @@ __global__ void __launch_bounds__(256) k_DX(T *X, T *D, T *U1, T const *U2, T co
             double const dr = D[o], di = D[o + 4096];
             double const xr = double(X[o]) + (ax_r*u1r - ax_i*u1i) + (bx_r*u2r - bx_i*u2i) + (cx_r*dr - cx_i*di);
             double const xi = double(X[o + 4096]) + (ax_r*u1i + ax_i*u1r) + (bx_r*u2i + bx_i*u2r) + (cx_r*di + cx_i*dr);
-            X[o] = T(xr); X[o + 4096] = T(xi);
+            X[o] = TX(xr); X[o + 4096] = TX(xi);
             D[o] = T(u2r + (ad_r*u1r - ad_i*u1i) + (cd_r*dr - cd_i*di));
             D[o + 4096] = T(u2i + (ad_r*u1i + ad_i*u1r) + (cd_r*di + cd_i*dr));
             double const wr = W[o], wi = W[o + 4096];
@@ -358,20 +361,13 @@ __global__ void __launch_bounds__(256) k_residual(double *R, double const *AX, u
     }
 }
 
-// W = U1 = (T) R, D = X = 0  (rhs of a correction solve)
+// W = U1 = (T) R, D = 0  (right-hand side of a correction sweep)
 template <typename T>
-__global__ void __launch_bounds__(256) k_set_from(T *W, T *U1, T *D, T *X, double const *R, size_t n) {
+__global__ void __launch_bounds__(256) k_set_from(T *W, T *U1, T *D, double const *R, size_t n) {
     for (size_t e = blockIdx.x*size_t(blockDim.x) + threadIdx.x; e < n; e += size_t(gridDim.x)*blockDim.x) {
         T const r = T(R[e]);
-        W[e] = r; U1[e] = r; D[e] = T(0); X[e] = T(0);
+        W[e] = r; U1[e] = r; D[e] = T(0);
     }
-}
-
-// X64 += (double) dX
-template <typename T>
-__global__ void __launch_bounds__(256) k_accumulate(double *X64, T const *dX, size_t n) {
-    for (size_t e = blockIdx.x*size_t(blockDim.x) + threadIdx.x; e < n; e += size_t(gridDim.x)*blockDim.x)
-        X64[e] += double(dX[e]);
 }
 
 __global__ void k_max_ratio(double const *colnorm, uint32_t ncol, double *out) {
@@ -422,10 +418,12 @@ namespace {
 
 struct InnerResult { int iterations = 0; int converged = 0; int breakdowns = 0; double estimate = 0; double applications = 0; };
 
-// tfQMR on the vectors of precision T whose W, U1 hold the right-hand side and D, X are zero
-template <typename T>
-bool tfqmr_inner(DevicePlan &dp, SolverWorkspace &ws, TfqmrVectors &v, double tol, int maxit, int check_every,
-                 uint32_t seed, cudaStream_t st, InnerResult &res) {
+// tfQMR on the vectors of precision T whose W, U1 hold the right-hand side and D is zero;
+// the solution is accumulated into Xs (precision TX), which holds the starting guess of the
+// correction (zero for a plain solve)
+template <typename T, typename TX>
+bool tfqmr_inner(DevicePlan &dp, SolverWorkspace &ws, TfqmrVectors &v, TX *Xs, double tol, int maxit, int check_every,
+                 uint32_t seed, cudaStream_t st, InnerResult &res, int echo) {
     uint32_t const nnzb = dp.nnzb, ncol = dp.nCols*64;
     uint16_t const *ci = dptr<uint16_t>(dp.colindx);
     auto *cs = dptr<ColState>(ws.colstate);
@@ -433,7 +431,8 @@ bool tfqmr_inner(DevicePlan &dp, SolverWorkspace &ws, TfqmrVectors &v, double to
     auto *accB = accA + ncol;
     int32_t *cnt = dptr<int32_t>(ws.counters);
     unsigned const g = grid_for(nnzb), gs = (ncol + 255)/256;
-    T *X = dptr<T>(v.X), *W = dptr<T>(v.W), *U1 = dptr<T>(v.U1), *U2 = dptr<T>(v.U2), *V = dptr<T>(v.V);
+    TX *X = Xs;
+    T *W = dptr<T>(v.W), *U1 = dptr<T>(v.U1), *U2 = dptr<T>(v.U2), *V = dptr<T>(v.V);
     T *D = dptr<T>(v.D), *AU1 = dptr<T>(v.AU1), *AU2 = dptr<T>(v.AU2);
     A43G_CUDA_TRY(cudaMemsetAsync(accA, 0, 2*size_t(ncol)*sizeof(Acc), st));
     A43G_CUDA_TRY(cudaMemsetAsync(cnt, 0, 4*sizeof(int32_t), st));
@@ -442,24 +441,35 @@ bool tfqmr_inner(DevicePlan &dp, SolverWorkspace &ws, TfqmrVectors &v, double to
     A43G_CUDA_TRY(cudaMemcpyAsync(V, AU1, v.n*sizeof(T), cudaMemcpyDeviceToDevice, st));
     res.applications += 1;
     k_init_dots<T><<<g, 256, 0, st>>>(W, V, nnzb, ci, accA, accB, seed);
+    count_launch();
     s_init<<<gs, 256, 0, st>>>(cs, accA, accB, ncol, cnt);
+    count_launch();
     int it = 0;
     for (it = 1; it <= maxit; ++it) {
         bool const check = (0 == it % check_every) || (it == maxit);
         if (check) A43G_CUDA_TRY(cudaMemsetAsync(cnt, 0, sizeof(int32_t), st));
         k_A<T><<<g, 256, 0, st>>>(U2, U1, V, W, AU1, nnzb, ci, cs, accA);
+        count_launch();
         s_half1<<<gs, 256, 0, st>>>(cs, accA, ncol, 2*it - 1, tol);
+        count_launch();
         if (!launch_action<T>(dp, AU2, U2, ci, st)) return false;
         k_C<T><<<g, 256, 0, st>>>(W, AU1, AU2, nnzb, ci, cs, accA, seed);
+        count_launch();
         s_half2<<<gs, 256, 0, st>>>(cs, accA, ncol, 2*it, tol, cnt);
-        k_DX<T><<<g, 256, 0, st>>>(X, D, U1, U2, W, nnzb, ci, cs);
+        count_launch();
+        k_DX<T, TX><<<g, 256, 0, st>>>(X, D, U1, U2, W, nnzb, ci, cs);
+        count_launch();
         if (!launch_action<T>(dp, AU1, U1, ci, st)) return false;
         k_E<T><<<g, 256, 0, st>>>(V, AU1, AU2, nnzb, ci, cs, accA, seed);
+        count_launch();
         s_alpha<<<gs, 256, 0, st>>>(cs, accA, ncol, cnt);
+        count_launch();
         res.applications += 2;
         if (check) {
             A43G_CUDA_TRY(cudaMemcpyAsync(ws.host_counters, cnt, 4*sizeof(int32_t), cudaMemcpyDeviceToHost, st));
             A43G_CUDA_TRY(cudaStreamSynchronize(st));
+            if (echo > 1) std::printf("# tfqmr<%s> iteration %d: %d of %u columns active, %d breakdowns\n",
+                                      sizeof(T) == 8 ? "f64" : "f32", it, ws.host_counters[0], ncol, ws.host_counters[1]);
             if (0 == ws.host_counters[0]) break;
         }
     }
@@ -467,6 +477,7 @@ bool tfqmr_inner(DevicePlan &dp, SolverWorkspace &ws, TfqmrVectors &v, double to
     A43G_CUDA_TRY(cudaGetLastError());
     double *est = dptr<double>(ws.colnorm) + ncol;     // one spare double after the column norms
     s_estimate<<<1, 256, 0, st>>>(cs, ncol, 2*std::min(it, maxit), est);
+    count_launch();
     A43G_CUDA_TRY(cudaMemcpyAsync(ws.host_counters, cnt, 4*sizeof(int32_t), cudaMemcpyDeviceToHost, st));
     double e = 0;
     A43G_CUDA_TRY(cudaMemcpyAsync(&e, est, sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -474,6 +485,8 @@ bool tfqmr_inner(DevicePlan &dp, SolverWorkspace &ws, TfqmrVectors &v, double to
     res.estimate = e;
     res.breakdowns += ws.host_counters[1];
     res.converged = (e <= tol) ? 1 : 0;
+    if (echo > 0) std::printf("# tfqmr<%s> %d iterations, residual estimate %.3e (tolerance %.1e)\n",
+                              sizeof(T) == 8 ? "f64" : "f32", std::min(it, maxit), e, tol);
     return true;
 }
 
@@ -497,7 +510,9 @@ bool residual64(DevicePlan &dp, SolverWorkspace &ws, double const *X64, double *
     A43G_CUDA_TRY(cudaMemsetAsync(cn, 0, (ncol + 8)*sizeof(double), st));
     k_residual<<<grid_for(dp.nnzb), 256, 0, st>>>(R64, AX64, dp.nnzb, dptr<uint16_t>(dp.colindx),
                                                   dptr<uint32_t>(dp.subset_dev), cn);
+                                                  count_launch();
     k_max_ratio<<<1, 256, 0, st>>>(cn, ncol, cn + ncol);
+    count_launch();
     A43G_CUDA_TRY(cudaMemcpyAsync(&rmax, cn + ncol, sizeof(double), cudaMemcpyDeviceToHost, st));
     A43G_CUDA_TRY(cudaStreamSynchronize(st));
     return true;
@@ -529,7 +544,8 @@ int solve(GreenPlan &hp, DevicePlan &dp, SolverWorkspace &ws, a43g_solve_options
         for (DeviceBuffer *b : {&v.W, &v.U1, &v.D, &v.X})
             if (cudaSuccess != cudaMemsetAsync(b->ptr, 0, n*8, st)) { set_error("memset"); return A43G_ERR_CUDA; }
         k_set_diag<double><<<dp.nCols, 64, 0, st>>>(dptr<double>(v.W), dptr<double>(v.U1), dptr<uint32_t>(dp.subset_dev), dp.nCols);
-        if (!tfqmr_inner<double>(dp, ws, v, opt.tolerance, opt.max_iterations, check, seed, st, res)) return A43G_ERR_CUDA;
+        count_launch();
+        if (!tfqmr_inner<double, double>(dp, ws, v, dptr<double>(v.X), opt.tolerance, opt.max_iterations, check, seed, st, res, opt.echo)) return A43G_ERR_CUDA;
         // true residual of the FP64 solution (uses U2/AU1 as scratch)
         double rmax = 0;
         if (!residual64(dp, ws, dptr<double>(v.X), dptr<double>(v.U2), dptr<double>(v.AU1), st, rmax, res.applications)) return A43G_ERR_CUDA;
@@ -539,6 +555,7 @@ int solve(GreenPlan &hp, DevicePlan &dp, SolverWorkspace &ws, a43g_solve_options
         if (rho) {
             DeviceBuffer rb; if (!rb.alloc(size_t(dp.nCols)*128*8)) return A43G_ERR_MEMORY;
             k_export_rho<double><<<dp.nCols, 64, 0, st>>>(dptr<double>(rb), dptr<double>(v.X), dptr<uint32_t>(dp.subset_dev), dp.nCols);
+            count_launch();
             cudaMemcpyAsync(rho, rb.ptr, size_t(dp.nCols)*128*8, cudaMemcpyDeviceToHost, st);
             cudaStreamSynchronize(st);
         }
@@ -556,14 +573,17 @@ int solve(GreenPlan &hp, DevicePlan &dp, SolverWorkspace &ws, a43g_solve_options
         double const inner_tol = (opt.inner_tolerance > 0) ? opt.inner_tolerance : 1e-4;
         int ref = 0;
         for (ref = 0; ref < maxref && rmax > opt.tolerance; ++ref) {
-            k_set_from<float><<<g*8, 256, 0, st>>>(dptr<float>(v.W), dptr<float>(v.U1), dptr<float>(v.D), dptr<float>(v.X), R64, n);
+            k_set_from<float><<<g*8, 256, 0, st>>>(dptr<float>(v.W), dptr<float>(v.U1), dptr<float>(v.D), R64, n);
+            count_launch();
             int const left = opt.max_iterations - res.iterations;
             if (left < 1) break;
             // relative inner tolerance, not tighter than needed for the outer target
             double const itol = std::max(inner_tol, 0.5*opt.tolerance/rmax);
-            if (!tfqmr_inner<float>(dp, ws, v, itol, left, check, seed + 7919u*uint32_t(ref + 1), st, res)) return A43G_ERR_CUDA;
-            k_accumulate<float><<<g*8, 256, 0, st>>>(X64, dptr<float>(v.X), n);
+            // the FP32 sweep advances the FP64 solution X64 directly
+            if (!tfqmr_inner<float, double>(dp, ws, v, X64, itol, left, check, seed + 7919u*uint32_t(ref + 1), st, res, opt.echo)) return A43G_ERR_CUDA;
             if (!residual64(dp, ws, X64, R64, AX64, st, rmax, res.applications)) return A43G_ERR_CUDA;
+            if (opt.echo > 0) std::printf("# refinement %d: FP64 residual %.3e after %d iterations in total\n",
+                                          ref + 1, rmax, res.iterations);
         }
         stats->refinements = ref;
         stats->residual_max = rmax;
@@ -571,6 +591,7 @@ int solve(GreenPlan &hp, DevicePlan &dp, SolverWorkspace &ws, a43g_solve_options
         if (rho) {
             DeviceBuffer rb; if (!rb.alloc(size_t(dp.nCols)*128*8)) return A43G_ERR_MEMORY;
             k_export_rho<double><<<dp.nCols, 64, 0, st>>>(dptr<double>(rb), X64, dptr<uint32_t>(dp.subset_dev), dp.nCols);
+            count_launch();
             cudaMemcpyAsync(rho, rb.ptr, size_t(dp.nCols)*128*8, cudaMemcpyDeviceToHost, st);
             cudaStreamSynchronize(st);
         }

@@ -46,7 +46,7 @@ class action_t:
 
 
 def solve_options(tolerance=1e-9, max_iterations=500, precision="float64", inner_tolerance=1e-4,
-                  max_refinements=8, check_every=10, seed=1):
+                  max_refinements=8, check_every=10, seed=1, echo=0):
     o = _lib.SolveOptions()
     o.tolerance = tolerance
     o.max_iterations = max_iterations
@@ -55,6 +55,7 @@ def solve_options(tolerance=1e-9, max_iterations=500, precision="float64", inner
     o.max_refinements = max_refinements
     o.check_every = check_every
     o.seed = seed
+    o.echo = echo
     return o
 
 

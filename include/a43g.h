@@ -82,6 +82,7 @@ typedef struct {
     int32_t  max_refinements; /* FP64 refinement steps (mixed precision) */
     int32_t  check_every;     /* iterations between convergence checks on the host */
     uint64_t seed;            /* seed of the random shadow residual */
+    int32_t  echo;            /* log level: > 0 prints one line per refinement / convergence check to stdout */
 } a43g_solve_options_t;
 
 typedef struct {
@@ -124,6 +125,20 @@ int a43g_plan_upload(a43g_plan_t *plan);
 int a43g_action_multiply(a43g_plan_t *plan, void *y, const void *x, const uint16_t *colIndex,
                          uint32_t nnzb, uint32_t nCols, unsigned l2nX, void *stream, int dtype,
                          double *flops);
+
+/* ---- one part of the operator, for profiling and for the adjoint kernels (no reference
+ * counterpart; the reference applies the parts only together inside action_t::multiply):
+ * part 0: y = (V - E) x + T x  (local potential and kinetic energy, include/green_potential.hxx
+ *         and include/green_kinetic.hxx);  part 1: y += sum_a p_a M_a p_a^T x  (projectors,
+ *         include/green_dyadic.hxx:856-922). */
+int a43g_action_part(a43g_plan_t *plan, int part, void *y, const void *x, void *stream, int dtype);
+
+/* synchronizes the device and reports an error a kernel of this plan recorded (for example a
+ * bounded wait of the tensor-core projector that timed out); clears the record */
+int a43g_plan_device_status(a43g_plan_t *plan);
+
+/* number of CUDA kernels this library has launched in this process (instrumentation) */
+uint64_t a43g_kernel_launches(void);
 
 /* ---- tfQMR solve of (H - E S) X = B with B the unit blocks on the diagonal (plan subset);
  * replaces tfqmrgpu::solve + action_t::solve (include/green_action.hxx:181-241).
