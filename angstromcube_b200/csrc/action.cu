@@ -43,24 +43,62 @@ struct LocalArgs {
     T ph[3][2][2];                   // Bloch phases [dd][left,right][re,im]
 };
 
-// load the 4 points (z = 0..3) at cross-section position yx and column col of a neighbour
-// cube (encoded e), optionally rotated by a phase
+// 4 consecutive points (x = 0..3 of one (z, y) row) of one column from shared memory
+template <typename T> struct Row4 { T v[4]; };
 template <typename T>
-__device__ __forceinline__ void load_zcol(T const *__restrict__ x, int32_t e, T pr, T pi,
-                                          int yx, int col, T (&re)[4], T (&im)[4]) {
+__device__ __forceinline__ Row4<T> lds_row(T const *p) {
+    Row4<T> r;
+    if (sizeof(T) == 4) {
+        float4 const a = *reinterpret_cast<float4 const*>(p);
+        r.v[0] = T(a.x); r.v[1] = T(a.y); r.v[2] = T(a.z); r.v[3] = T(a.w);
+    } else {
+        double2 const a = *reinterpret_cast<double2 const*>(p), b = *reinterpret_cast<double2 const*>(p + 2);
+        r.v[0] = T(a.x); r.v[1] = T(a.y); r.v[2] = T(b.x); r.v[3] = T(b.y);
+    }
+    return r;
+}
+template <typename T>
+__device__ __forceinline__ void sts_row(T *p, T const (&v)[4]) {
+    if (sizeof(T) == 4) {
+        *reinterpret_cast<float4*>(p) = make_float4(float(v[0]), float(v[1]), float(v[2]), float(v[3]));
+    } else {
+        *reinterpret_cast<double2*>(p) = make_double2(double(v[0]), double(v[1]));
+        *reinterpret_cast<double2*>(p + 2) = make_double2(double(v[2]), double(v[3]));
+    }
+}
+
+// 4 contiguous values from global memory (one potential row)
+template <typename T>
+__device__ __forceinline__ Row4<T> lds_row_global(T const *__restrict__ p) {
+    Row4<T> r;
+    if (sizeof(T) == 4) {
+        float4 const a = __ldg(reinterpret_cast<float4 const*>(p));
+        r.v[0] = T(a.x); r.v[1] = T(a.y); r.v[2] = T(a.z); r.v[3] = T(a.w);
+    } else {
+        double2 const a = __ldg(reinterpret_cast<double2 const*>(p)), b = __ldg(reinterpret_cast<double2 const*>(p) + 1);
+        r.v[0] = T(a.x); r.v[1] = T(a.y); r.v[2] = T(b.x); r.v[3] = T(b.y);
+    }
+    return r;
+}
+
+// the row (z, y) = r of one cube (encoded e) for column col: 4 points x = 0..3, real and
+// imaginary part, optionally rotated by a Bloch phase (pr, pi)
+template <typename T>
+__device__ __forceinline__ void load_row(T const *__restrict__ x, int32_t e, T pr, T pi, int r, int col,
+                                         T (&re)[4], T (&im)[4]) {
     if (-1 == e) {
 #pragma unroll
-        for (int z = 0; z < 4; ++z) { re[z] = T(0); im[z] = T(0); }
+        for (int i = 0; i < 4; ++i) { re[i] = T(0); im[i] = T(0); }
         return;
     }
-    T const *b = x + size_t(nbr_block(e))*kBlockReals + yx*64 + col;
+    T const *b = x + size_t(nbr_block(e))*kBlockReals + (r*4)*64 + col;
 #pragma unroll
-    for (int z = 0; z < 4; ++z) { re[z] = __ldg(b + z*16*64); im[z] = __ldg(b + 4096 + z*16*64); }
+    for (int i = 0; i < 4; ++i) { re[i] = __ldg(b + i*64); im[i] = __ldg(b + 4096 + i*64); }
     if (e < -1) {
 #pragma unroll
-        for (int z = 0; z < 4; ++z) {
-            T const r = pr*re[z] - pi*im[z], i = pr*im[z] + pi*re[z];
-            re[z] = r; im[z] = i;
+        for (int i = 0; i < 4; ++i) {
+            T const a = pr*re[i] - pi*im[i], c = pr*im[i] + pi*re[i];
+            re[i] = a; im[i] = c;
         }
     }
 }
@@ -70,8 +108,12 @@ __device__ __forceinline__ int32_t list_code(int32_t entry) {
     return (entry > 0) ? entry - 1 : ((entry < 0) ? -(-entry - 1) - 2 : -1);
 }
 
-// One CTA per (z-line, column slice of S columns); thread (j, y, x) owns the 4 points of its
-// (y, x) column in every cube of the line for column j of the slice, both real and imaginary.
+// One CTA per (z-line of cubes, slice of S columns).  Thread (j, r) owns row r = (z, y) of
+// every cube of the line for column j: the x-stencil runs in registers (with the x-neighbour
+// rows loaded directly), the y- and z-stencils read whole rows from shared memory, where the
+// previous, current and next cube of the line and the two y-neighbour cubes are staged.
+// Shared rows are padded to 68 points, so the 128-bit row accesses of a quarter warp hit
+// distinct banks.
 template <typename T, int S>
 __global__ void __launch_bounds__(S*16)
 local_fused_kernel(T *__restrict__ y, T const *__restrict__ x,
@@ -79,73 +121,92 @@ local_fused_kernel(T *__restrict__ y, T const *__restrict__ x,
                    int32_t const *__restrict__ nbr, int32_t const *__restrict__ veff,
                    T const *__restrict__ Vcell, LocalArgs<T> const a)
 {
-    constexpr int NSL = 64/S;
-    __shared__ T sm[5][2][64][S];    // slots: own cube, x-, x+, y-, y+
+    constexpr int NSL = 64/S, PAD = 68;
+    __shared__ __align__(16) T sm[5][2][S][PAD];   // slots: 3 rotating z-slots, y-, y+
     int const line = blockIdx.x/NSL, slice = blockIdx.x % NSL;
-    int const j = threadIdx.x % S, yx = threadIdx.x/S;
-    int const xq = yx & 3, yq = yx >> 2, col = slice*S + j;
+    int const j = threadIdx.x % S, r = threadIdx.x/S;       // r = z*4 + y
+    int const zq = r >> 2, yq = r & 3, col = slice*S + j;
     int32_t const *L = zlist + zstart[line];
     int n = 0;
     while (L[4 + n] > 0) ++n;        // lists end with 4 non-positive entries
-
-    T pre[4], pim[4], cre[4], cim[4], nre[4], nim[4];
-    load_zcol(x, list_code(L[3]), a.ph[2][0][0], a.ph[2][0][1], yx, col, pre, pim);
-    load_zcol(x, L[4] - 1, T(0), T(0), yx, col, cre, cim);
     T const (&cx)[5] = a.st.c[0];
     T const (&cy)[5] = a.st.c[1];
     T const (&cz)[5] = a.st.c[2];
+    T const c0 = cx[0] + cy[0] + cz[0];
+
+    T cre[4], cim[4], nre[4], nim[4];
+    {   // left z-halo into slot 0, first cube into slot 1
+        T pre[4], pim[4];
+        load_row(x, list_code(L[3]), a.ph[2][0][0], a.ph[2][0][1], r, col, pre, pim);
+        sts_row(&sm[0][0][j][r*4], pre); sts_row(&sm[0][1][j][r*4], pim);
+    }
+    load_row(x, L[4] - 1, T(0), T(0), r, col, cre, cim);
+    sts_row(&sm[1][0][j][r*4], cre); sts_row(&sm[1][1][j][r*4], cim);
+    int sp = 0, sc = 1, sn = 2;                      // rotating slots: previous, current, next cube
 
     for (int k = 0; k < n; ++k) {
         int32_t const b = L[4 + k] - 1;
-        load_zcol(x, list_code(L[5 + k]), a.ph[2][1][0], a.ph[2][1][1], yx, col, nre, nim);
         int32_t const *nb = nbr + 6*size_t(b);
-        int32_t const e[4] = {nb[0], nb[1], nb[2], nb[3]};
-        __syncthreads();             // previous step finished reading the slots
+        int32_t const exm = nb[0], exp_ = nb[1], eym = nb[2], eyp = nb[3];
+        load_row(x, list_code(L[5 + k]), a.ph[2][1][0], a.ph[2][1][1], r, col, nre, nim);
+        T ymr[4], ymi[4], ypr[4], ypi[4];
+        load_row(x, eym, a.ph[1][0][0], a.ph[1][0][1], r, col, ymr, ymi);
+        load_row(x, eyp, a.ph[1][1][0], a.ph[1][1][1], r, col, ypr, ypi);
+        T lr[12], li[12];                            // x-line: left row | own row | right row
+        load_row(x, exm, a.ph[0][0][0], a.ph[0][0][1], r, col, *reinterpret_cast<T(*)[4]>(&lr[0]), *reinterpret_cast<T(*)[4]>(&li[0]));
+        load_row(x, exp_, a.ph[0][1][0], a.ph[0][1][1], r, col, *reinterpret_cast<T(*)[4]>(&lr[8]), *reinterpret_cast<T(*)[4]>(&li[8]));
 #pragma unroll
-        for (int z = 0; z < 4; ++z) { sm[0][0][z*16 + yx][j] = cre[z]; sm[0][1][z*16 + yx][j] = cim[z]; }
-#pragma unroll
-        for (int s = 0; s < 4; ++s) {
-            T tr[4], ti[4];
-            int const dd = s >> 1, side = s & 1;
-            load_zcol(x, e[s], a.ph[dd][side][0], a.ph[dd][side][1], yx, col, tr, ti);
-#pragma unroll
-            for (int z = 0; z < 4; ++z) { sm[1 + s][0][z*16 + yx][j] = tr[z]; sm[1 + s][1][z*16 + yx][j] = ti[z]; }
-        }
+        for (int i = 0; i < 4; ++i) { lr[4 + i] = cre[i]; li[4 + i] = cim[i]; }
+        __syncthreads();                             // previous step finished reading the slots
+        sts_row(&sm[sn][0][j][r*4], nre); sts_row(&sm[sn][1][j][r*4], nim);
+        sts_row(&sm[3][0][j][r*4], ymr); sts_row(&sm[3][1][j][r*4], ymi);
+        sts_row(&sm[4][0][j][r*4], ypr); sts_row(&sm[4][1][j][r*4], ypi);
         __syncthreads();
-        int32_t const iloc = veff[b];
-        T *yb = y + size_t(b)*kBlockReals + yx*64 + col;
+        T accr[4], acci[4];
+        {
+            int32_t const iloc = veff[b];
+            T V[4];
+            if (iloc < 0) { V[0] = V[1] = V[2] = V[3] = T(0); }
+            else { Row4<T> const v = lds_row_global(Vcell + size_t(iloc)*64 + r*4); V[0] = v.v[0]; V[1] = v.v[1]; V[2] = v.v[2]; V[3] = v.v[3]; }
 #pragma unroll
-        for (int z = 0; z < 4; ++z) {
-            int const i64 = z*16 + yx;
-            T const Vt = ((iloc < 0) ? T(0) : Vcell[size_t(iloc)*64 + i64]) - a.E_re;
-            T accr = Vt*cre[z] + a.E_im*cim[z];
-            T acci = Vt*cim[z] - a.E_im*cre[z];
-            // z direction: window prev | cur | next held in registers
-            accr += cz[0]*cre[z]; acci += cz[0]*cim[z];
-#pragma unroll
-            for (int d = 1; d <= 4; ++d) {
-                int const qm = z - d, qp = z + d;
-                T const mr = (qm < 0) ? pre[qm + 4] : cre[qm], mi = (qm < 0) ? pim[qm + 4] : cim[qm];
-                T const pr = (qp > 3) ? nre[qp - 4] : cre[qp], pi = (qp > 3) ? nim[qp - 4] : cim[qp];
-                accr += cz[d]*(mr + pr); acci += cz[d]*(mi + pi);
+            for (int i = 0; i < 4; ++i) {
+                T const Vt = V[i] - a.E_re;
+                accr[i] = Vt*cre[i] + a.E_im*cim[i] + c0*cre[i];
+                acci[i] = Vt*cim[i] - a.E_im*cre[i] + c0*cim[i];
             }
-            // x and y directions from shared memory
-            accr += (cx[0] + cy[0])*cre[z]; acci += (cx[0] + cy[0])*cim[z];
-#pragma unroll
-            for (int d = 1; d <= 4; ++d) {
-                int const xm = xq - d, xp = xq + d, ym = yq - d, yp = yq + d;
-                int const sxm = (xm < 0) ? 1 : 0, sxp = (xp > 3) ? 2 : 0;
-                int const sym = (ym < 0) ? 3 : 0, syp = (yp > 3) ? 4 : 0;
-                int const ixm = z*16 + yq*4 + (xm & 3), ixp = z*16 + yq*4 + (xp & 3);
-                int const iym = z*16 + (ym & 3)*4 + xq, iyp = z*16 + (yp & 3)*4 + xq;
-                accr += cx[d]*(sm[sxm][0][ixm][j] + sm[sxp][0][ixp][j]) + cy[d]*(sm[sym][0][iym][j] + sm[syp][0][iyp][j]);
-                acci += cx[d]*(sm[sxm][1][ixm][j] + sm[sxp][1][ixp][j]) + cy[d]*(sm[sym][1][iym][j] + sm[syp][1][iyp][j]);
-            }
-            yb[z*16*64] = accr;
-            yb[4096 + z*16*64] = acci;
         }
+        // x direction in registers
 #pragma unroll
-        for (int z = 0; z < 4; ++z) { pre[z] = cre[z]; pim[z] = cim[z]; cre[z] = nre[z]; cim[z] = nim[z]; }
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int d = 1; d <= 4; ++d) {
+                accr[i] += cx[d]*(lr[4 + i - d] + lr[4 + i + d]);
+                acci[i] += cx[d]*(li[4 + i - d] + li[4 + i + d]);
+            }
+        // y and z directions: whole rows from shared memory
+#pragma unroll
+        for (int d = 1; d <= 4; ++d) {
+            int const ym = yq - d, yp = yq + d, zm = zq - d, zp = zq + d;
+            int const s_ym = (ym < 0) ? 3 : sc, s_yp = (yp > 3) ? 4 : sc;
+            int const s_zm = (zm < 0) ? sp : sc, s_zp = (zp > 3) ? sn : sc;
+            int const o_ym = (zq*4 + (ym & 3))*4, o_yp = (zq*4 + (yp & 3))*4;
+            int const o_zm = ((zm & 3)*4 + yq)*4, o_zp = ((zp & 3)*4 + yq)*4;
+            Row4<T> const r1 = lds_row(&sm[s_ym][0][j][o_ym]), r2 = lds_row(&sm[s_yp][0][j][o_yp]);
+            Row4<T> const r3 = lds_row(&sm[s_zm][0][j][o_zm]), r4 = lds_row(&sm[s_zp][0][j][o_zp]);
+            Row4<T> const i1 = lds_row(&sm[s_ym][1][j][o_ym]), i2 = lds_row(&sm[s_yp][1][j][o_yp]);
+            Row4<T> const i3 = lds_row(&sm[s_zm][1][j][o_zm]), i4 = lds_row(&sm[s_zp][1][j][o_zp]);
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                accr[i] += cy[d]*(r1.v[i] + r2.v[i]) + cz[d]*(r3.v[i] + r4.v[i]);
+                acci[i] += cy[d]*(i1.v[i] + i2.v[i]) + cz[d]*(i3.v[i] + i4.v[i]);
+            }
+        }
+        T *yb = y + size_t(b)*kBlockReals + (r*4)*64 + col;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) { yb[i*64] = accr[i]; yb[4096 + i*64] = acci[i]; }
+        int const t = sp; sp = sc; sc = sn; sn = t;  // rotate the z-slots
+#pragma unroll
+        for (int i = 0; i < 4; ++i) { cre[i] = nre[i]; cim[i] = nim[i]; }
     }
 }
 

@@ -10,6 +10,8 @@
 //   and y[b] += D^T on the points inside the projection spheres.
 // P[sho][i] = H_ix(x_i) H_iy(y_i) H_iz(z_i) on the mask (tables of the plan), 0 elsewhere.
 // Each operand x is split x = hi + lo with hi = TF32(x); C = A_hi B_hi + A_hi B_lo + A_lo B_hi.
+// Both operands are K-major in shared memory (no swizzle; an MN-major TF32 A operand in this
+// layout produced zeros on B200, so the data tiles are transposed while they are staged).
 // Operands are staged by all threads into shared memory (double-buffered stages), one thread
 // issues the MMAs and commits them to an mbarrier; every wait is bounded and a timeout is
 // recorded in the device error flag instead of hanging.
@@ -26,10 +28,11 @@ constexpr int kB = 16384;            // bytes of one 64 x 64 FP32 operand
 constexpr int kStage = 2*kA + 2*kB;  // A_hi, A_lo, B_hi, B_lo
 constexpr int kSmem = 2*kStage + 1024;
 constexpr uint64_t kWaitNs = 2000000000ull;   // 2 s per wait: far beyond any MMA latency
-constexpr uint32_t kIdesc = tc::idesc_tf32(128, 64, true, false);   // A MN-major, B K-major
+constexpr uint32_t kIdesc = tc::idesc_tf32(128, 64, false, false);  // A and B K-major
 
-// byte offset of element (m, k) of a 128 x 64 MN-major operand (core matrices 8 k x 4 m)
-__device__ __forceinline__ uint32_t offA(int m, int k) { return ((k >> 3)*32 + (m >> 2))*128 + ((k & 7)*4 + (m & 3))*4; }
+// byte offset of element (m, k) of a 128 x 64 K-major operand (core matrices 8 m x 4 k;
+// K chunks 2048 bytes apart, 8-row groups 128 bytes apart)
+__device__ __forceinline__ uint32_t offA(int m, int k) { return ((k >> 2)*16 + (m >> 3))*128 + ((m & 7)*4 + (k & 3))*4; }
 // byte offset of element (n, k) of a 64 x 64 K-major operand (core matrices 8 n x 4 k)
 __device__ __forceinline__ uint32_t offB(int n, int k) { return ((k >> 2)*8 + (n >> 3))*128 + ((n & 7)*4 + (k & 3))*4; }
 
@@ -38,7 +41,7 @@ __device__ __forceinline__ void issue_mmas(uint32_t tmem, uint32_t sA_hi, uint32
                                            uint32_t sB_lo, bool first) {
 #pragma unroll
     for (int s = 0; s < 8; ++s) {
-        uint64_t const ah = tc::smem_desc(sA_hi + s*4096, 4096, 128), al = tc::smem_desc(sA_lo + s*4096, 4096, 128);
+        uint64_t const ah = tc::smem_desc(sA_hi + s*4096, 2048, 128), al = tc::smem_desc(sA_lo + s*4096, 2048, 128);
         uint64_t const bh = tc::smem_desc(sB_hi + s*2048, 1024, 128), bl = tc::smem_desc(sB_lo + s*2048, 1024, 128);
         tc::mma_tf32(tmem, ah, bh, kIdesc, (first && 0 == s) ? 0u : 1u);
         tc::mma_tf32(tmem, ah, bl, kIdesc, 1u);
@@ -47,22 +50,31 @@ __device__ __forceinline__ void issue_mmas(uint32_t tmem, uint32_t sA_hi, uint32
 }
 
 // stage a 128 x 64 FP32 matrix, element (m = reim*64 + j, k) at src[reim*plane + k*ld_k + j],
-// as the split MN-major operand; rows k >= kmax are zero
+// as the split K-major operand; rows k >= kmax are zero.  Each thread reads a 4 (k) x 4 (m)
+// tile with four coalesced float4 loads along m and stores it transposed, 4 k-values per
+// 16-byte chunk.
 __device__ __forceinline__ void stage_A(char *sA_hi, char *sA_lo, float const *__restrict__ src, size_t plane,
                                         size_t ld_k, int kmax, int tid) {
-#pragma unroll 4
-    for (int r = 0; r < 2048/kThreads; ++r) {
+#pragma unroll
+    for (int r = 0; r < 512/kThreads; ++r) {
         int const q = r*kThreads + tid;
-        int const kl = q & 7, mg = (q >> 3) & 31, kg = q >> 8;
-        int const k = kg*8 + kl, m = mg*4;
-        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (k < kmax) v = __ldg(reinterpret_cast<float4 const*>(src + (m >> 6)*plane + size_t(k)*ld_k + (m & 63)));
-        float4 h, l;
-        tc::split_tf32(v.x, h.x, l.x); tc::split_tf32(v.y, h.y, l.y);
-        tc::split_tf32(v.z, h.z, l.z); tc::split_tf32(v.w, h.w, l.w);
-        uint32_t const o = offA(m, k);
-        *reinterpret_cast<float4*>(sA_hi + o) = h;
-        *reinterpret_cast<float4*>(sA_lo + o) = l;
+        int const m0 = (q & 31)*4, k0 = (q >> 5)*4;
+        float t[4][4];                               // t[kk][mm]
+#pragma unroll
+        for (int kk = 0; kk < 4; ++kk) {
+            float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (k0 + kk < kmax) v = __ldg(reinterpret_cast<float4 const*>(src + (m0 >> 6)*plane + size_t(k0 + kk)*ld_k + (m0 & 63)));
+            t[kk][0] = v.x; t[kk][1] = v.y; t[kk][2] = v.z; t[kk][3] = v.w;
+        }
+#pragma unroll
+        for (int mm = 0; mm < 4; ++mm) {
+            float4 h, l;
+            tc::split_tf32(t[0][mm], h.x, l.x); tc::split_tf32(t[1][mm], h.y, l.y);
+            tc::split_tf32(t[2][mm], h.z, l.z); tc::split_tf32(t[3][mm], h.w, l.w);
+            uint32_t const o = offA(m0 + mm, k0);
+            *reinterpret_cast<float4*>(sA_hi + o) = h;
+            *reinterpret_cast<float4*>(sA_lo + o) = l;
+        }
     }
 }
 
