@@ -312,28 +312,30 @@ __device__ __forceinline__ void stage_table(T (*H)[3][4], double const *__restri
 // apc[(i0 + sho)*nrhs + s][reim][j] = sum over the blocks of source s near image a of the
 // masked projector functions times x (include/green_dyadic.hxx:112-288), for images whose
 // basis size is exactly L (the host launches one grid per distinct L).  Sum-factorized:
-// contract x, then y, then z.  Grid (images of this L, nrhs), 128 threads = (reim, column).
+// contract x, then y, then z.  One CTA per work item (image, source, chunk of at most 16
+// blocks of its list), 128 threads = (reim, column); the chunks of one (image, source) are
+// summed with atomics into the zeroed coefficients.
 template <typename T, int L>
 __global__ void __launch_bounds__(128)
 sho_project_kernel(T *__restrict__ apc, T const *__restrict__ x, uint32_t nrhs,
-                   uint32_t const *__restrict__ images, uint32_t nAI,
-                   uint32_t const *__restrict__ prj_start, uint32_t const *__restrict__ prj_col,
-                   uint64_t const *__restrict__ prj_coloff, uint32_t const *__restrict__ prj_slot,
+                   uint32_t const *__restrict__ items,
+                   uint32_t const *__restrict__ prj_col, uint64_t const *__restrict__ prj_coloff,
+                   uint32_t const *__restrict__ prj_slot,
                    double const *__restrict__ slot_H, uint64_t const *__restrict__ slot_mask, int stride,
                    uint32_t const *__restrict__ img_starts)
 {
     constexpr int NS = nsho_c(L), N2 = n2ho_c(L);
     __shared__ T Hs[2][L + 1][3][4];
-    uint32_t const a = images[blockIdx.x];
-    int const s = blockIdx.y, tid = threadIdx.x;
+    uint32_t const *item = items + 4*size_t(blockIdx.x);
+    uint32_t const a = item[0], s = item[1], k0 = item[2], k1 = item[3];
+    int const tid = threadIdx.x;
     int const reim = tid >> 6, j = tid & 63;
-    uint32_t const *start = prj_start + size_t(s)*(nAI + 1);
     uint64_t const off = prj_coloff[s];
     T acc[NS];
 #pragma unroll
     for (int i = 0; i < NS; ++i) acc[i] = T(0);
     int buf = 0;
-    for (uint32_t k = start[a]; k < start[a + 1]; ++k, buf ^= 1) {
+    for (uint32_t k = k0; k < k1; ++k, buf ^= 1) {
         uint32_t const b = prj_col[off + k];
         uint32_t const slot = prj_slot[off + k];
         stage_table<T, L>(Hs[buf], slot_H, stride, slot, L, tid);
@@ -381,7 +383,7 @@ sho_project_kernel(T *__restrict__ apc, T const *__restrict__ x, uint32_t nrhs,
     }
     T *out = apc + (size_t(img_starts[a])*nrhs + s)*128 + reim*64 + j;
 #pragma unroll
-    for (int sho = 0; sho < NS; ++sho) out[size_t(sho)*nrhs*128] = acc[sho];
+    for (int sho = 0; sho < NS; ++sho) atomicAdd(out + size_t(sho)*nrhs*128, acc[sho]);
 }
 
 // aac[(a0 + c)*nrhs + s] = sum over the images i of atom A of phase_i * apc[(i0 + c)*nrhs + s]
@@ -539,12 +541,11 @@ template <> float const *vcell<float>(DevicePlan &dp) { return dptr<float>(dp.Vc
 
 template <typename T, int L>
 void launch_project_L(DevicePlan &dp, T const *x, cudaStream_t st) {
-    auto const &g = dp.img_group[L];
+    auto const &g = dp.prj_items[L];
     if (0 == g.count) return;
-    dim3 const grid(g.count, dp.nCols);
-    sho_project_kernel<T, L><<<grid, 128, 0, st>>>(
-        dptr<T>(dp.apc), x, dp.nCols, dptr<uint32_t>(g.images), dp.nAI,
-        dptr<uint32_t>(dp.prj_start), dptr<uint32_t>(dp.prj_col), dptr<uint64_t>(dp.prj_coloff),
+    sho_project_kernel<T, L><<<g.count, 128, 0, st>>>(
+        dptr<T>(dp.apc), x, dp.nCols, dptr<uint32_t>(g.items),
+        dptr<uint32_t>(dp.prj_col), dptr<uint64_t>(dp.prj_coloff),
         dptr<uint32_t>(dp.prj_slot), dptr<double>(dp.slot_H), dptr<uint64_t>(dp.slot_mask), dp.table_stride,
         dptr<uint32_t>(dp.img_starts));
         count_launch();
@@ -610,6 +611,8 @@ bool launch_dyadic(DevicePlan &dp, T *y, T const *x, uint16_t const *colIndex, c
     if (tc) {
         if (!launch_project_tc(dp, (float const*)x, st)) return false;
     } else {
+        // coefficients of images without any block stay zero
+        A43G_CUDA_TRY(cudaMemsetAsync(dp.apc.ptr, 0, size_t(dp.ncoeffI)*dp.nCols*128*sizeof(T), st));
         launch_project_L<T, 0>(dp, x, st); launch_project_L<T, 1>(dp, x, st);
         launch_project_L<T, 2>(dp, x, st); launch_project_L<T, 3>(dp, x, st);
         launch_project_L<T, 4>(dp, x, st); launch_project_L<T, 5>(dp, x, st);

@@ -65,6 +65,9 @@ struct DevicePlan {
     DeviceBuffer dev_error;      // int: first error code recorded by a kernel (0: none)
     bool use_tc = true;          // FP32 projector on the tensor cores (else SIMT)
     struct ImageGroup { uint32_t count = 0; DeviceBuffer images; } img_group[8];  // images by basis size
+    // SIMT projection work items by basis size: (image, source, first, last) list positions,
+    // each at most kPrjChunk blocks, so that long block lists are spread over many CTAs
+    struct PrjItems { uint32_t count = 0; DeviceBuffer items; } prj_items[8];
     // scratch of the dyadic part (allocated once per plan, never per call)
     DeviceBuffer apc;            // real_t [ncoeffI*nCols][2][64] image projection coefficients
     DeviceBuffer aac, cadd;      // double [ncoeffA*nCols][2][64]

@@ -116,14 +116,34 @@ bool upload_plan(GreenPlan const &hp, DevicePlan &dp) {
         if (!put(dp.img_group[L].images, imgs)) return false;
     }
     if (dp.lmax_max > 7) { set_error("projector basis sizes above numax 7 are not supported"); return false; }
+    {
+        constexpr uint32_t kPrjChunk = 16;
+        std::vector<uint32_t> items[8];
+        for (uint32_t s = 0; s < hp.nCols; ++s) {
+            auto const &c = hp.SHOprj[s];
+            if (c.start.empty()) continue;
+            for (uint32_t a = 0; a < hp.nAtomImages; ++a) {
+                int const L = hp.AtomImageLmax[a];
+                for (uint32_t k = c.start[a]; k < c.start[a + 1]; k += kPrjChunk) {
+                    uint32_t const it[4] = {a, s, k, std::min(k + kPrjChunk, c.start[a + 1])};
+                    items[L].insert(items[L].end(), it, it + 4);
+                }
+            }
+        }
+        for (int L = 0; L < 8; ++L) {
+            dp.prj_items[L].count = uint32_t(items[L].size()/4);
+            if (!put(dp.prj_items[L].items, items[L])) return false;
+        }
+    }
     dp.table_stride = (hp.table_lmax + 1)*12;
     if (!put(dp.slot_H, hp.slot_H) || !put(dp.slot_mask, hp.slot_mask)) return false;
     if (!put(dp.prj_slot, hp.prj_slot) || !put(dp.add_slot, hp.add_slot)) return false;
     if (!put(dp.subset_dev, hp.subset)) return false;
     if (!put(dp.dev_error, std::vector<int32_t>(4, 0))) return false;
     {
-        char const *e = std::getenv("A43G_PROJECTOR");          // "simt" selects the SIMT projector
-        dp.use_tc = !(e && 0 == std::strcmp(e, "simt"));
+        // FP32 projector: SIMT (default) or the tensor cores ("tc"); the FP64 path is always SIMT
+        char const *e = std::getenv("A43G_PROJECTOR");
+        dp.use_tc = (e && 0 == std::strcmp(e, "tc"));
     }
     if (!dp.aac.alloc(std::max<size_t>(16, size_t(dp.ncoeffA)*dp.nCols*128*sizeof(double)))) return false;
     if (!dp.cadd.alloc(std::max<size_t>(16, size_t(dp.ncoeffA)*dp.nCols*128*sizeof(double)))) return false;

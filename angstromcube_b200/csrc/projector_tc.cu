@@ -27,7 +27,7 @@ constexpr int kA = 32768;            // bytes of one 128 x 64 FP32 operand
 constexpr int kB = 16384;            // bytes of one 64 x 64 FP32 operand
 constexpr int kStage = 2*kA + 2*kB;  // A_hi, A_lo, B_hi, B_lo
 constexpr int kSmem = 2*kStage + 1024;
-constexpr uint64_t kWaitNs = 2000000000ull;   // 2 s per wait: far beyond any MMA latency
+constexpr uint64_t kWaitNs = 500000000ull;    // 0.5 s per wait: far beyond any MMA latency
 constexpr uint32_t kIdesc = tc::idesc_tf32(128, 64, false, false);  // A and B K-major
 
 // byte offset of element (m, k) of a 128 x 64 K-major operand (core matrices 8 m x 4 k;
@@ -119,6 +119,7 @@ sho_project_tc_kernel(float *__restrict__ apc, float const *__restrict__ x, uint
     uint64_t const off = prj_coloff[s];
     uint32_t const k0 = start[a], k1 = start[a + 1];
     float *out = apc + (size_t(img_starts[a])*nrhs + s)*128;
+    if (*(int const volatile*)err) return;             // an earlier CTA timed out: results are void
     if (k0 == k1) {                                  // no block: zero coefficients
         for (int e = tid; e < nsho*128; e += kThreads) out[size_t(e >> 7)*nrhs*128 + (e & 127)] = 0.f;
         return;
@@ -137,7 +138,7 @@ sho_project_tc_kernel(float *__restrict__ apc, float const *__restrict__ x, uint
         char *sA_hi = smem + st*kStage, *sA_lo = sA_hi + kA, *sB_hi = sA_lo + kA, *sB_lo = sB_hi + kB;
         if (it >= 2) {                               // stage st is free once the MMAs of it-2 completed
             bool w = true;
-            if (0 == tid) w = tc::mbar_wait(&mbar[st], uint32_t((it - 2) >> 1) & 1u, kWaitNs);
+            if (0 == tid) w = tc::mbar_wait(&mbar[st], uint32_t((it - 2) >> 1) & 1u, kWaitNs, err);
             ok = __syncthreads_and(w);               // block-uniform decision
             if (!ok) break;
         }
@@ -173,13 +174,13 @@ sho_project_tc_kernel(float *__restrict__ apc, float const *__restrict__ x, uint
     int const last = issued - 1;
     if (last >= 0) {
         bool w = ok;
-        if (0 == tid && ok) w = tc::mbar_wait(&mbar[last & 1], uint32_t(last >> 1) & 1u, kWaitNs);
+        if (0 == tid && ok) w = tc::mbar_wait(&mbar[last & 1], uint32_t(last >> 1) & 1u, kWaitNs, err);
         ok = __syncthreads_and(w);
     }
     if (!ok && 0 == tid && last >= 0) {
         record_error(err, 1);
         // give the tensor core a bounded grace period before the TMEM is released
-        tc::mbar_wait(&mbar[last & 1], uint32_t(last >> 1) & 1u, kWaitNs);
+        tc::mbar_wait(&mbar[last & 1], uint32_t(last >> 1) & 1u, kWaitNs, err);
     }
     tc::fence_after_sync();
     if (ok) {
@@ -215,7 +216,7 @@ sho_add_tc_kernel(float *__restrict__ y, float const *__restrict__ cad, uint32_t
     int const tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     uint32_t const b = blockIdx.x;
     uint32_t const k0 = add_start[b], k1 = add_start[b + 1];
-    if (k0 == k1) return;
+    if (k0 == k1 || *(int const volatile*)err) return;
     uint32_t const s = colIndex[b];
     if (0 == warp) tc::tmem_alloc(&tmem_base, 64);
     if (0 == tid) { tc::mbar_init(&mbar[0], 1); tc::mbar_init(&mbar[1], 1); }
@@ -231,7 +232,7 @@ sho_add_tc_kernel(float *__restrict__ y, float const *__restrict__ cad, uint32_t
         char *sA_hi = smem + st*kStage, *sA_lo = sA_hi + kA, *sB_hi = sA_lo + kA, *sB_lo = sB_hi + kB;
         if (it >= 2) {                               // stage st is free once the MMAs of it-2 completed
             bool w = true;
-            if (0 == tid) w = tc::mbar_wait(&mbar[st], uint32_t((it - 2) >> 1) & 1u, kWaitNs);
+            if (0 == tid) w = tc::mbar_wait(&mbar[st], uint32_t((it - 2) >> 1) & 1u, kWaitNs, err);
             ok = __syncthreads_and(w);               // block-uniform decision
             if (!ok) break;
         }
@@ -271,13 +272,13 @@ sho_add_tc_kernel(float *__restrict__ y, float const *__restrict__ cad, uint32_t
     int const last = issued - 1;
     if (last >= 0) {
         bool w = ok;
-        if (0 == tid && ok) w = tc::mbar_wait(&mbar[last & 1], uint32_t(last >> 1) & 1u, kWaitNs);
+        if (0 == tid && ok) w = tc::mbar_wait(&mbar[last & 1], uint32_t(last >> 1) & 1u, kWaitNs, err);
         ok = __syncthreads_and(w);
     }
     if (!ok && 0 == tid && last >= 0) {
         record_error(err, 2);
         // give the tensor core a bounded grace period before the TMEM is released
-        tc::mbar_wait(&mbar[last & 1], uint32_t(last >> 1) & 1u, kWaitNs);
+        tc::mbar_wait(&mbar[last & 1], uint32_t(last >> 1) & 1u, kWaitNs, err);
     }
     tc::fence_after_sync();
     if (ok && mask_all) {

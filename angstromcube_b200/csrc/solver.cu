@@ -95,6 +95,7 @@ __global__ void __launch_bounds__(256) k_init_dots(T const *W, T const *V, uint3
     for (uint32_t b = blockIdx.x; b < nnzb; b += gridDim.x) {
         uint32_t const c = colindx[b];
         double n2 = 0, wr = 0, wi = 0, vr = 0, vi = 0;
+#pragma unroll 8
         for (int i = q*16; i < q*16 + 16; ++i) {
             size_t const o = size_t(b)*kBlk + i*64 + j;
             uint32_t const idx = uint32_t(o);
@@ -119,6 +120,7 @@ __global__ void __launch_bounds__(256) k_A(T *U2, T const *U1, T const *V, T con
         uint32_t const col = colindx[b]*64 + j;
         double const ar = cs[col].al_re, ai = cs[col].al_im;
         double n2 = 0;
+#pragma unroll 8
         for (int i = q*16; i < q*16 + 16; ++i) {
             size_t const o = size_t(b)*kBlk + i*64 + j;
             T const vr = V[o], vi = V[o + 4096];
@@ -142,6 +144,7 @@ __global__ void __launch_bounds__(256) k_C(T *W, T const *AU1, T const *AU2, uin
         uint32_t const col = colindx[b]*64 + j;
         double const ar = cs[col].al_re, ai = cs[col].al_im;
         double n2 = 0, dr = 0, di = 0;
+#pragma unroll 8
         for (int i = q*16; i < q*16 + 16; ++i) {
             size_t const o = size_t(b)*kBlk + i*64 + j;
             double const sr = double(AU1[o]) + double(AU2[o]), si = double(AU1[o + 4096]) + double(AU2[o + 4096]);
@@ -170,6 +173,7 @@ __global__ void __launch_bounds__(256) k_DX(TX *X, T *D, T *U1, T const *U2, T c
         double const ax_r = s.cu1x_re, ax_i = s.cu1x_im, bx_r = s.cu2x_re, bx_i = s.cu2x_im, cx_r = s.cdx_re, cx_i = s.cdx_im;
         double const ad_r = s.cu1d_re, ad_i = s.cu1d_im, cd_r = s.cdd_re, cd_i = s.cdd_im;
         double const be_r = s.be_re, be_i = s.be_im;
+#pragma unroll 8
         for (int i = q*16; i < q*16 + 16; ++i) {
             size_t const o = size_t(b)*kBlk + i*64 + j;
             double const u1r = U1[o], u1i = U1[o + 4096], u2r = U2[o], u2i = U2[o + 4096];
@@ -196,6 +200,7 @@ __global__ void __launch_bounds__(256) k_E(T *V, T const *AU1, T const *AU2, uin
         uint32_t const col = colindx[b]*64 + j;
         double const br = cs[col].be_re, bi = cs[col].be_im;
         double dr = 0, di = 0;
+#pragma unroll 8
         for (int i = q*16; i < q*16 + 16; ++i) {
             size_t const o = size_t(b)*kBlk + i*64 + j;
             double const vr = V[o], vi = V[o + 4096];
@@ -348,6 +353,7 @@ __global__ void __launch_bounds__(256) k_residual(double *R, double const *AX, u
         uint32_t const c = colindx[b];
         bool const diag = (subset[c] == b);
         double n2 = 0;
+#pragma unroll 8
         for (int i = q*16; i < q*16 + 16; ++i) {
             size_t const o = size_t(b)*kBlk + i*64 + j;
             double const rr = ((diag && i == j) ? 1.0 : 0.0) - AX[o], ri = -AX[o + 4096];
@@ -368,6 +374,13 @@ __global__ void __launch_bounds__(256) k_set_from(T *W, T *U1, T *D, double cons
         T const r = T(R[e]);
         W[e] = r; U1[e] = r; D[e] = T(0);
     }
+}
+
+// X64 += (double) dX  (end of an FP32 correction sweep)
+template <typename T>
+__global__ void __launch_bounds__(256) k_accumulate(double *X64, T const *dX, size_t n) {
+    for (size_t e = blockIdx.x*size_t(blockDim.x) + threadIdx.x; e < n; e += size_t(gridDim.x)*blockDim.x)
+        X64[e] += double(dX[e]);
 }
 
 __global__ void k_max_ratio(double const *colnorm, uint32_t ncol, double *out) {
@@ -575,12 +588,16 @@ int solve(GreenPlan &hp, DevicePlan &dp, SolverWorkspace &ws, a43g_solve_options
         for (ref = 0; ref < maxref && rmax > opt.tolerance; ++ref) {
             k_set_from<float><<<g*8, 256, 0, st>>>(dptr<float>(v.W), dptr<float>(v.U1), dptr<float>(v.D), R64, n);
             count_launch();
+            if (cudaSuccess != cudaMemsetAsync(v.X.ptr, 0, n*4, st)) { set_error("memset"); return A43G_ERR_CUDA; }
             int const left = opt.max_iterations - res.iterations;
             if (left < 1) break;
             // relative inner tolerance, not tighter than needed for the outer target
             double const itol = std::max(inner_tol, 0.5*opt.tolerance/rmax);
-            // the FP32 sweep advances the FP64 solution X64 directly
-            if (!tfqmr_inner<float, double>(dp, ws, v, X64, itol, left, check, seed + 7919u*uint32_t(ref + 1), st, res, opt.echo)) return A43G_ERR_CUDA;
+            // FP32 correction sweep (keeping its solution in FP64 does not lower the FP32 residual
+            // floor, measured, so the correction is accumulated once per sweep)
+            if (!tfqmr_inner<float, float>(dp, ws, v, dptr<float>(v.X), itol, left, check, seed + 7919u*uint32_t(ref + 1), st, res, opt.echo)) return A43G_ERR_CUDA;
+            k_accumulate<float><<<g*8, 256, 0, st>>>(X64, dptr<float>(v.X), n);
+            count_launch();
             if (!residual64(dp, ws, X64, R64, AX64, st, rmax, res.applications)) return A43G_ERR_CUDA;
             if (opt.echo > 0) std::printf("# refinement %d: FP64 residual %.3e after %d iterations in total\n",
                                           ref + 1, rmax, res.iterations);

@@ -73,17 +73,20 @@ __device__ __forceinline__ uint64_t globaltimer_ns() {
 }
 
 // wait until the phase with the given parity of the mbarrier completed; gives up after
-// limit_ns nanoseconds of wall time and returns false (the caller records the error and
-// shuts down cleanly), so a lost arrival can never hang the GPU
-__device__ __forceinline__ bool mbar_wait(uint64_t *mbar, uint32_t parity, uint64_t limit_ns) {
+// limit_ns nanoseconds of wall time, or as soon as another CTA has recorded an error in
+// *abort, and returns false (the caller records the error and shuts down cleanly), so a lost
+// arrival can never hang the GPU and the first timeout ends the whole grid quickly
+__device__ __forceinline__ bool mbar_wait(uint64_t *mbar, uint32_t parity, uint64_t limit_ns,
+                                          int const volatile *abort) {
     uint32_t const a = smem_u32(mbar);
     uint64_t const t0 = globaltimer_ns();
-    for (;;) {
+    for (uint32_t it = 0;; ++it) {
         uint32_t done;
         asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
                      "selp.u32 %0, 1, 0, p;\n\t}" : "=r"(done) : "r"(a), "r"(parity) : "memory");
         if (done) return true;
         if (globaltimer_ns() - t0 > limit_ns) return false;
+        if (0 == (it & 63) && *abort) return false;
     }
 }
 

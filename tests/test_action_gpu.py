@@ -116,12 +116,12 @@ def test_full_size_linearity_and_symmetry(name):
 
 @pytest.mark.parametrize("name", ["wrap8", "peri_xy_wrap_z", "repeat_aniso"])
 def test_projector_tensor_cores_vs_simt(name, monkeypatch):
-    """The FP32 projector on the tensor cores (3xTF32, default) and on the SIMT cores agree, and
+    """The FP32 projector on the tensor cores (3xTF32) and on the SIMT cores (default) agree, and
     both match the FP64 oracle; no kernel recorded a wait timeout."""
     from angstromcube_b200 import _lib
     g = GEOMETRIES[name]()
     Vc, mats, offs, E, k, dVol, na = inputs_for(g)
-    x = np.random.default_rng(9).standard_normal((1, 2, 64, 64))
+    monkeypatch.setenv("A43G_PROJECTOR", "tc")
     p_tc = product_plan(g, Vc, mats, offs, E, k, dVol)
     x = np.random.default_rng(9).standard_normal((p_tc.nnzb, 2, 64, 64))
     y_tc = apply(p_tc, x, np.float32)

@@ -37,8 +37,10 @@ def true_residual(p, w, X):
 def test_solve_periodic4_1atom(precision):
     w, p = setup("periodic4_1atom")
     X = torch.zeros((p.nnzb, 2, 64, 64), device="cuda", dtype=torch.float64)
-    stats, rho = green_action.solve(p, X=X, tolerance=w.tolerance, max_iterations=w.max_iterations,
-                                    precision=precision, check_every=5)
+    # the mixed solver restarts tfQMR once per FP32 sweep (about 3 digits each): larger budget
+    maxit = w.max_iterations if precision == "float64" else 3*w.max_iterations
+    stats, rho = green_action.solve(p, X=X, tolerance=w.tolerance, max_iterations=maxit,
+                                    precision=precision, check_every=5, max_refinements=6)
     assert stats["converged"] == 1, stats
     assert stats["residual_max"] <= w.tolerance
     Xn = X.cpu().numpy()
@@ -55,7 +57,7 @@ def test_fp64_and_mixed_agree():
     X1 = torch.zeros((p.nnzb, 2, 64, 64), device="cuda", dtype=torch.float64)
     X2 = torch.zeros_like(X1)
     s1, _ = green_action.solve(p, X=X1, tolerance=1e-10, max_iterations=800, precision="float64")
-    s2, _ = green_action.solve(p, X=X2, tolerance=1e-10, max_iterations=800, precision="float32")
+    s2, _ = green_action.solve(p, X=X2, tolerance=1e-10, max_iterations=2000, precision="float32")
     assert s1["converged"] and s2["converged"], (s1, s2)
     err = ((X1 - X2).abs().max() / X1.abs().max()).item()
     assert err < 1e-7
