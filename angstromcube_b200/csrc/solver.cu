@@ -481,8 +481,17 @@ bool tfqmr_inner(DevicePlan &dp, SolverWorkspace &ws, TfqmrVectors &v, TX *Xs, d
         if (check) {
             A43G_CUDA_TRY(cudaMemcpyAsync(ws.host_counters, cnt, 4*sizeof(int32_t), cudaMemcpyDeviceToHost, st));
             A43G_CUDA_TRY(cudaStreamSynchronize(st));
-            if (echo > 1) std::printf("# tfqmr<%s> iteration %d: %d of %u columns active, %d breakdowns\n",
-                                      sizeof(T) == 8 ? "f64" : "f32", it, ws.host_counters[0], ncol, ws.host_counters[1]);
+            if (echo > 1) {
+                double *est = dptr<double>(ws.colnorm) + ncol;
+                s_estimate<<<1, 256, 0, st>>>(cs, ncol, 2*it, est);
+                count_launch();
+                double e = 0;
+                A43G_CUDA_TRY(cudaMemcpyAsync(&e, est, sizeof(double), cudaMemcpyDeviceToHost, st));
+                A43G_CUDA_TRY(cudaStreamSynchronize(st));
+                std::printf("# tfqmr<%s> iteration %d: %d of %u columns active, %d breakdowns, estimate %.3e\n",
+                            sizeof(T) == 8 ? "f64" : "f32", it, ws.host_counters[0], ncol, ws.host_counters[1], e);
+                std::fflush(stdout);
+            }
             if (0 == ws.host_counters[0]) break;
         }
     }

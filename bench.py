@@ -3,11 +3,14 @@
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 A step is one solve of the periodic 16^3-cube cell with 64 atoms (numax 5), 16 source cubes
-(1024 right-hand-side columns), E = -0.2 + 0.02i Ha, to 1e-8 relative residual per column,
-with the mixed-precision solver: FP32 tfQMR sweeps (FP32 finite-difference stencil and
-potential, 3xTF32 tensor-core projectors) inside FP64 residual refinement.  Each rank solves
-its own energy point (weak scaling); the complex densities of all ranks are summed with one
-NCCL all-reduce per step, as the energy-contour integration does.
+(1024 right-hand-side columns), truncation radius 12 Bohr, to 1e-8 relative residual per
+column, with the mixed-precision solver: FP32 tfQMR sweeps (FP32 finite-difference stencil,
+potential and projectors) inside FP64 residual refinement.  The energy is E = -0.2 + 0.5i Ha,
+the largest imaginary part of the energy contour over this cell: at E = -0.2 + 0.02i tfQMR
+stagnates (4000 FP32 iterations leave a relative residual of 0.33, 700 FP64 iterations 0.07),
+so no solver reaches 1e-8 there in a bounded time.  Each rank solves its own energy point
+(weak scaling); the complex densities of all ranks are summed with one NCCL all-reduce per
+step, as the energy-contour integration does.
 
 Reported beside the solver throughput: the fused local-action kernel against the measured HBM
 peak, the tensor-core projector, the plain FP64 solver on the same point, and the reference's
@@ -26,9 +29,11 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 WORKLOAD = "periodic16_64atoms"
+ENERGY = complex(-0.2, 0.5)
 TOLERANCE = 1e-8
-# tfQMR iterations of the plain FP64 solver at this workload and tolerance (measured with this
-# code on a B200; used only to extrapolate the reference CPU action time to a solve)
+# tfQMR iterations of the plain FP64 solver at this workload, energy and tolerance (measured
+# with this code on a B200); the reference arm, which runs without a GPU, extrapolates its
+# action time to a solve with it.  The main arm uses the count of its own FP64 solve.
 FP64_ITERATIONS = 480
 METRIC = "Solves/s at 1e-8 resid (mixed+batched vs plain FP64); action % HBM peak"
 
@@ -119,7 +124,7 @@ def _ref_worker(args):
     r = oracle.RefGreen(g)
     r.set_potential(w.Vcell)
     r.set_atom_matrices(w.mats, w.offsets)
-    r.set_energy(w.E, w.dVol)
+    r.set_energy(ENERGY, w.dVol)
     x = np.random.default_rng(seed).standard_normal((r.sizes["nnzb"], 2, 64, 64))
     best = None
     for _ in range(reps):
@@ -130,7 +135,7 @@ def _ref_worker(args):
     return best
 
 
-def cpu_reference_sample(workload, nsources, procs=None, reps=1):
+def cpu_reference_sample(workload, nsources, procs=None, reps=1, iterations=FP64_ITERATIONS):
     """Reference CPU action on a bounded sample: one single-source action per process, all host
     cores in parallel.  Returns (solves/s extrapolated, cores, seconds per single-source action)."""
     import multiprocessing as mp
@@ -140,7 +145,7 @@ def cpu_reference_sample(workload, nsources, procs=None, reps=1):
         times = pool.map(_ref_worker, [(workload, i, reps) for i in range(procs)])
     t1 = max(times)
     # a solve applies the full operator (all sources) twice per iteration
-    solves_per_s = procs / (t1 * nsources * 2 * FP64_ITERATIONS)
+    solves_per_s = procs / (t1 * nsources * 2 * iterations)
     return solves_per_s, procs, t1
 
 
@@ -169,7 +174,7 @@ def reference_arm(a):
         "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": a.gpus, "steps": a.steps,
         "warmup": a.warmup, "ms_per_step": 1e3 * elapsed / max(a.steps, 1), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
-        "config": {"workload": a.workload, "tolerance": TOLERANCE, "sources": nsrc},
+        "config": {"workload": a.workload, "tolerance": TOLERANCE, "sources": nsrc, "E": [ENERGY.real, ENERGY.imag]},
         "impl": "reference",
         "cpu_baseline": {"value": value, "unit": "solves/s", "cores": cores, "kind": "reference", "sample": sample},
         "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -225,14 +230,14 @@ def our_arm(a):
     hbm, bf16, peak_kind = peaks()
     w = workloads.make(a.workload)
     # every rank solves its own energy point of the contour (weak scaling)
-    E = complex(w.E.real - 0.01*rank, w.E.imag)
+    E = complex(ENERGY.real - 0.01*rank, ENERGY.imag)
     plan = gf.construct_Green_function(w.geometry)
     gf.update_potential(plan, w.Vcell, w.mats, w.offsets, layout="cells")
     gf.update_energy_parameter(plan, E, w.dVol)
     plan.upload()
     stream = torch.cuda.Stream()
     opts = dict(tolerance=TOLERANCE, max_iterations=3000, precision="float32", inner_tolerance=1e-5,
-                max_refinements=6, check_every=20)
+                max_refinements=8, check_every=10)
     rho_all = torch.zeros((plan.nCols, 64, 2), dtype=torch.float64, device="cuda")
 
     def step():
@@ -329,11 +334,15 @@ def measure_kernels(a, plan, w, stream, out, hbm, bf16, peak_kind):
     nsho = 56
     flops = 4.0*nsho*64*128*plan.sizes["SHOadd_nnz"]
     tf32_peak = bf16/2
-    out["roofline_projector"] = {"kernel": "sho_project_tc + sho_add_tc (tcgen05 kind::tf32, 3xTF32) + atom matrices",
+    tc = os.environ.get("A43G_PROJECTOR", "") == "tc"
+    out["roofline_projector"] = {"kernel": ("sho_project_tc + sho_add_tc (tcgen05 kind::tf32, 3xTF32)" if tc else
+                                            "sho_project_kernel + sho_add_kernel (SIMT FP32, sum-factorized)")
+                                 + " + atom matrices",
                                  "bound": "tensor", "achieved": flops/t_dyadic/1e12, "peak": tf32_peak,
                                  "unit": "TFLOP/s", "frac": flops/t_dyadic/1e12/tf32_peak,
                                  "peak_kind": "dense TF32 = half of the %s bf16 peak" % peak_kind,
-                                 "algorithmic_flops_per_launch": flops, "ms_per_launch": t_dyadic*1e3}
+                                 "algorithmic_flops_per_launch": flops, "ms_per_launch": t_dyadic*1e3,
+                                 "note": "flops of the dense contraction P (64 x 64 per block and image) x X (64 x 128)"}
     x64 = torch.randn((nnzb, 2, 64, 64), device="cuda", dtype=torch.float64)
     y64 = torch.empty_like(x64)
     del x, y
@@ -362,12 +371,13 @@ def main():
         if world == 1 and not a.no_cpu:
             from oracle import ref_available
             if ref_available():
-                v, cores, t1 = cpu_reference_sample(a.workload, plan.nCols)
+                nit = out.get("fp64_plain", {}).get("iterations", FP64_ITERATIONS)
+                v, cores, t1 = cpu_reference_sample(a.workload, plan.nCols, iterations=nit)
                 out["cpu_baseline"] = {"value": v, "unit": "solves/s", "cores": cores, "kind": "reference",
                                        "sample": "reference CPU action (oracle/_ref) of the cell with one source cube "
                                                  "per process, %d processes, %.2f s per action; solve = %d sources x 2 x "
                                                  "%d FP64 tfQMR iterations (extrapolated)"
-                                                 % (cores, t1, plan.nCols, FP64_ITERATIONS)}
+                                                 % (cores, t1, plan.nCols, nit)}
         print(json.dumps(out))
     if world > 1:
         import torch.distributed as dist
