@@ -38,6 +38,18 @@ FP64_ITERATIONS = 480
 METRIC = "Solves/s at 1e-8 resid (mixed+batched vs plain FP64); action % HBM peak"
 
 
+def _json_default(o):
+    """numpy scalars and arrays in the result line"""
+    if hasattr(o, "tolist"):
+        return o.tolist()
+    return str(o)
+
+
+def emit(obj):
+    sys.stdout.write(json.dumps(obj, default=_json_default) + "\n")
+    sys.stdout.flush()
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -112,6 +124,9 @@ def _ref_worker(args):
     """One process: the reference's action_t<double,2,1>::multiply (its CPU build in
     oracle/_ref) on the benchmark cell with ONE source cube; returns seconds per action."""
     workload, seed, reps = args
+    # the reference's plan builder prints warnings on stdout: keep the JSON line alone there
+    devnull = os.open(os.devnull, os.O_WRONLY)
+    os.dup2(devnull, 1)
     import tempfile
     import numpy as np
     os.chdir(tempfile.mkdtemp())                 # the reference plan builder writes an SVG file
@@ -155,7 +170,7 @@ def reference_arm(a):
         return
     from oracle import ref_available
     if not ref_available():
-        print(json.dumps({"impl": "reference", "unavailable": "reference CPU build oracle/_ref not built"}))
+        emit({"impl": "reference", "unavailable": "reference CPU build oracle/_ref not built"})
         return
     nsrc = 16
     for _ in range(a.warmup):
@@ -170,7 +185,7 @@ def reference_arm(a):
     sample = ("reference action_t<double,2,1>::multiply (oracle/_ref CPU build) of the %s cell with one source "
               "cube per process, %d processes, %.2f s per action; solve = 16 sources x 2 x %d FP64 tfQMR "
               "iterations (extrapolated)" % (a.workload, cores, t1, FP64_ITERATIONS))
-    print(json.dumps({
+    emit({
         "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": a.gpus, "steps": a.steps,
         "warmup": a.warmup, "ms_per_step": 1e3 * elapsed / max(a.steps, 1), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
@@ -178,7 +193,7 @@ def reference_arm(a):
         "impl": "reference",
         "cpu_baseline": {"value": value, "unit": "solves/s", "cores": cores, "kind": "reference", "sample": sample},
         "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-    }))
+    })
 
 
 # ------------------------------------------------------------------ our arm
@@ -378,7 +393,7 @@ def main():
                                                  "per process, %d processes, %.2f s per action; solve = %d sources x 2 x "
                                                  "%d FP64 tfQMR iterations (extrapolated)"
                                                  % (cores, t1, plan.nCols, nit)}
-        print(json.dumps(out))
+        emit(out)
     if world > 1:
         import torch.distributed as dist
         dist.barrier()
