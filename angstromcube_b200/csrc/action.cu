@@ -607,9 +607,14 @@ template <typename T>
 bool launch_dyadic(DevicePlan &dp, T *y, T const *x, uint16_t const *colIndex, cudaStream_t st) {
     if (dp.nAI < 1 || dp.nCols < 1) return true;
     if (!ensure_dyadic_scratch(dp, sizeof(T))) return false;
-    bool const tc = (sizeof(T) == 4) && dp.use_tc && tc_projector_supported(dp);
+    // both FP32 projector paths stage x with 16-byte loads; other x take the generic kernels
+    bool const aligned16 = 0 == (reinterpret_cast<uintptr_t>(x) & 15u);
+    bool const tc = (sizeof(T) == 4) && dp.use_tc && aligned16 && tc_projector_supported(dp);
+    bool const simt32 = (sizeof(T) == 4) && !tc && simt_f32_projector_supported(dp, x);
     if (tc) {
         if (!launch_project_tc(dp, (float const*)x, st)) return false;
+    } else if (simt32) {
+        if (!launch_project_f32(dp, (float const*)x, st)) return false;
     } else {
         // coefficients of images without any block stay zero
         A43G_CUDA_TRY(cudaMemsetAsync(dp.apc.ptr, 0, size_t(dp.ncoeffI)*dp.nCols*128*sizeof(T), st));
@@ -638,6 +643,8 @@ bool launch_dyadic(DevicePlan &dp, T *y, T const *x, uint16_t const *colIndex, c
     }
     if (tc) {
         if (!launch_add_tc(dp, (float*)y, colIndex, st)) return false;
+    } else if (simt32) {
+        if (!launch_add_f32(dp, (float*)y, colIndex, st)) return false;
     } else {
         sho_add_kernel<T><<<dp.nnzb, 128, 0, st>>>(y, dptr<T>(dp.cad), dp.nCols, dp.nnzb, colIndex,
             dptr<uint32_t>(dp.add_start), dptr<uint32_t>(dp.add_col), dptr<uint32_t>(dp.add_slot),

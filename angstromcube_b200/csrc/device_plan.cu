@@ -137,6 +137,7 @@ bool upload_plan(GreenPlan const &hp, DevicePlan &dp) {
     }
     dp.table_stride = (hp.table_lmax + 1)*12;
     if (!put(dp.slot_H, hp.slot_H) || !put(dp.slot_mask, hp.slot_mask)) return false;
+    if (!put(dp.slot_H32, std::vector<float>(hp.slot_H.begin(), hp.slot_H.end()))) return false;
     if (!put(dp.prj_slot, hp.prj_slot) || !put(dp.add_slot, hp.add_slot)) return false;
     if (!put(dp.subset_dev, hp.subset)) return false;
     if (!put(dp.dev_error, std::vector<int32_t>(4, 0))) return false;

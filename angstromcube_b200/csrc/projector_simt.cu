@@ -1,0 +1,284 @@
+// FP32 projector contraction of the action on the CUDA cores, sum-factorized
+// (include/green_dyadic.hxx:112-288 projection, :325-518 addition).
+//
+// The projector functions are separable on the spherical mask,
+//     P_(ix,iy,iz)(x, y, z) = H_ix(x) H_iy(y) H_iz(z)   for points inside the projection radius,
+// so one (block, image) pair costs 64*(L+1) + 16*(L+1)(L+2)/2 + 4*nSHO fused multiply-adds per
+// column instead of 64*nSHO for the dense product (944 instead of 3584 at numax 5).
+//
+// Both kernels keep the 1D tables of the current (image, row) slot and the per-thread partial
+// sums in registers (loops fully unrolled for the basis size L), one thread per (real/imaginary
+// plane, right-hand-side column):
+//   * projection: one CTA per work item (image, source, up to 16 blocks of its list); the
+//     blocks stream through a double-buffered shared-memory stage filled with cp.async
+//     (16-byte copies, so x must be 16-byte aligned), and the partial coefficients of the item
+//     are added to the zeroed image coefficients with one atomic per coefficient;
+//   * addition: one CTA per block b, summing the contributions of all images near b in
+//     registers and updating y[b] once.
+#include "device.cuh"
+
+namespace a43g {
+
+namespace {
+
+constexpr int kBlk = 8192;            // floats per block: 2 planes x 64 points x 64 columns
+constexpr int kThreads = 128;
+
+__host__ __device__ constexpr int nsho_of(int L) { return ((L + 1)*(L + 2)*(L + 3))/6; }
+__host__ __device__ constexpr int n2_of(int L) { return ((L + 1)*(L + 2))/2; }
+
+__device__ __forceinline__ uint32_t smem_addr(void const *p) { return uint32_t(__cvta_generic_to_shared(p)); }
+
+__device__ __forceinline__ void cp_async16(void *dst, void const *src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" :: "r"(smem_addr(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+
+// the 1D tables of one slot: T[nu][dir][i] at tab[(nu*3 + dir)*4 + i], dir 0/1/2 = x/y/z
+template <int L>
+struct Tables { float h[L + 1][3][4]; };
+
+template <int L>
+__device__ __forceinline__ void load_tables(Tables<L> &t, float const *__restrict__ tab) {
+#pragma unroll
+    for (int nu = 0; nu <= L; ++nu)
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            float4 const v = __ldg(reinterpret_cast<float4 const*>(tab + (nu*3 + d)*4));
+            t.h[nu][d][0] = v.x; t.h[nu][d][1] = v.y; t.h[nu][d][2] = v.z; t.h[nu][d][3] = v.w;
+        }
+}
+
+// ---------------------------------------------------------------- projection
+
+template <int L>
+__global__ void __launch_bounds__(kThreads, 3)
+sho_project_f32_kernel(float *__restrict__ apc, float const *__restrict__ x, uint32_t nrhs,
+                       uint32_t const *__restrict__ items, uint32_t const *__restrict__ prj_col,
+                       uint64_t const *__restrict__ prj_coloff, uint32_t const *__restrict__ prj_slot,
+                       float const *__restrict__ slot_H, uint64_t const *__restrict__ slot_mask, int stride,
+                       uint32_t const *__restrict__ img_starts)
+{
+    constexpr int NS = nsho_of(L), N2 = n2_of(L);
+    extern __shared__ __align__(16) float xs[];       // [2][kBlk]
+    uint32_t const *item = items + 4*size_t(blockIdx.x);
+    uint32_t const a = item[0], s = item[1], k0 = item[2], k1 = item[3];
+    int const tid = threadIdx.x, reim = tid >> 6, j = tid & 63;
+    uint64_t const off = prj_coloff[s];
+
+    auto stage = [&](uint32_t k, int buf) {
+        char const *src = reinterpret_cast<char const*>(x + size_t(prj_col[off + k])*kBlk);
+        char *dst = reinterpret_cast<char*>(xs + buf*kBlk);
+#pragma unroll
+        for (int r = 0; r < kBlk*4/(16*kThreads); ++r) {
+            int const o = (r*kThreads + tid)*16;
+            cp_async16(dst + o, src + o);
+        }
+    };
+
+    float acc[NS];
+#pragma unroll
+    for (int i = 0; i < NS; ++i) acc[i] = 0.f;
+
+    stage(k0, 0);
+    cp_async_commit();
+    int buf = 0;
+    for (uint32_t k = k0; k < k1; ++k, buf ^= 1) {
+        if (k + 1 < k1) stage(k + 1, buf ^ 1);
+        cp_async_commit();
+        cp_async_wait1();                            // block k has landed (this thread's copies)
+        __syncthreads();                             // ... and everybody else's
+        uint32_t const slot = prj_slot[off + k];
+        Tables<L> t;
+        load_tables<L>(t, slot_H + size_t(slot)*stride);
+        uint64_t const mask = slot_mask[slot];
+        float const *xb = xs + buf*kBlk + reim*4096 + j;
+#pragma unroll
+        for (int z = 0; z < 4; ++z) {
+            if (0 == ((mask >> (16*z)) & 0xffffu)) continue;     // uniform: plane outside the sphere
+            float byx[N2];
+#pragma unroll
+            for (int i = 0; i < N2; ++i) byx[i] = 0.f;
+#pragma unroll
+            for (int yy = 0; yy < 4; ++yy) {
+                float ax[L + 1];
+#pragma unroll
+                for (int i = 0; i <= L; ++i) ax[i] = 0.f;
+#pragma unroll
+                for (int xx = 0; xx < 4; ++xx) {
+                    int const p = (z*4 + yy)*4 + xx;
+                    float const v = ((mask >> p) & 1u) ? xb[p*64] : 0.f;
+#pragma unroll
+                    for (int ix = 0; ix <= L; ++ix) ax[ix] = fmaf(v, t.h[ix][0][xx], ax[ix]);
+                }
+#pragma unroll
+                for (int iy = 0, iyx = 0; iy <= L; ++iy) {
+                    float const hy = t.h[iy][1][yy];
+#pragma unroll
+                    for (int ix = 0; ix <= L - iy; ++ix, ++iyx) byx[iyx] = fmaf(ax[ix], hy, byx[iyx]);
+                }
+            }
+#pragma unroll
+            for (int iz = 0, sho = 0; iz <= L; ++iz) {
+                float const hz = t.h[iz][2][z];
+#pragma unroll
+                for (int iy = 0; iy <= L - iz; ++iy) {
+                    int const iyx = iy*(2*L + 3 - iy)/2;
+#pragma unroll
+                    for (int ix = 0; ix <= L - iz - iy; ++ix, ++sho) acc[sho] = fmaf(byx[iyx + ix], hz, acc[sho]);
+                }
+            }
+        }
+        __syncthreads();                             // buffer buf is free for block k + 2
+    }
+    float *out = apc + (size_t(img_starts[a])*nrhs + s)*128 + reim*64 + j;
+#pragma unroll
+    for (int sho = 0; sho < NS; ++sho) atomicAdd(out + size_t(sho)*nrhs*128, acc[sho]);
+}
+
+// ---------------------------------------------------------------- addition
+
+// contribution of one image with basis size L to the 64 point sums of this thread
+template <int L, bool FULL>
+__device__ __forceinline__ void add_image(float (&acc)[64], Tables<L> const &t, uint64_t mask,
+                                          float const *__restrict__ c, size_t cstride) {
+#pragma unroll
+    for (int iz = 0, sho = 0; iz <= L; ++iz) {
+        float byx[16];
+#pragma unroll
+        for (int i = 0; i < 16; ++i) byx[i] = 0.f;
+#pragma unroll
+        for (int iy = 0; iy <= L - iz; ++iy) {
+            float ax[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+            for (int ix = 0; ix <= L - iz - iy; ++ix, ++sho) {
+                float const cv = __ldg(c + size_t(sho)*cstride);
+#pragma unroll
+                for (int xx = 0; xx < 4; ++xx) ax[xx] = fmaf(t.h[ix][0][xx], cv, ax[xx]);
+            }
+#pragma unroll
+            for (int yy = 0; yy < 4; ++yy) {
+                float const hy = t.h[iy][1][yy];
+#pragma unroll
+                for (int xx = 0; xx < 4; ++xx) byx[yy*4 + xx] = fmaf(hy, ax[xx], byx[yy*4 + xx]);
+            }
+        }
+#pragma unroll
+        for (int z = 0; z < 4; ++z) {
+            float const hz = t.h[iz][2][z];
+#pragma unroll
+            for (int q = 0; q < 16; ++q) {
+                int const p = z*16 + q;
+                if (FULL) acc[p] = fmaf(hz, byx[q], acc[p]);
+                else acc[p] = ((mask >> p) & 1u) ? fmaf(hz, byx[q], acc[p]) : acc[p];
+            }
+        }
+    }
+}
+
+template <int L>
+__device__ __forceinline__ void add_image_L(float (&acc)[64], float const *__restrict__ tab, uint64_t mask,
+                                            float const *__restrict__ c, size_t cstride) {
+    Tables<L> t;
+    load_tables<L>(t, tab);
+    if (~0ull == mask) add_image<L, true>(acc, t, mask, c, cstride);
+    else add_image<L, false>(acc, t, mask, c, cstride);
+}
+
+// LMAX: largest basis size of the plan (the switch below instantiates no larger one)
+template <int LMAX>
+__global__ void __launch_bounds__(kThreads, 3)
+sho_add_f32_kernel(float *__restrict__ y, float const *__restrict__ cad, uint32_t nrhs,
+                   uint16_t const *__restrict__ colIndex, uint32_t const *__restrict__ add_start,
+                   uint32_t const *__restrict__ add_col, uint32_t const *__restrict__ add_slot,
+                   float const *__restrict__ slot_H, uint64_t const *__restrict__ slot_mask, int stride,
+                   int8_t const *__restrict__ img_lmax, uint32_t const *__restrict__ img_starts)
+{
+    uint32_t const b = blockIdx.x;
+    uint32_t const k0 = add_start[b], k1 = add_start[b + 1];
+    if (k0 >= k1) return;
+    int const tid = threadIdx.x, reim = tid >> 6, j = tid & 63;
+    uint32_t const s = colIndex[b];
+    size_t const cstride = size_t(nrhs)*128;
+    float acc[64];
+#pragma unroll
+    for (int i = 0; i < 64; ++i) acc[i] = 0.f;
+    uint64_t mask_all = 0;
+    for (uint32_t k = k0; k < k1; ++k) {
+        uint32_t const a = add_col[k], slot = add_slot[k];
+        uint64_t const mask = slot_mask[slot];
+        if (!mask) continue;
+        mask_all |= mask;
+        float const *tab = slot_H + size_t(slot)*stride;
+        float const *c = cad + (size_t(img_starts[a])*nrhs + s)*128 + reim*64 + j;
+        int const L = img_lmax[a];                 // uniform over the CTA
+        if (L == LMAX) add_image_L<LMAX>(acc, tab, mask, c, cstride);
+        else if (LMAX > 0 && L == 0) add_image_L<0>(acc, tab, mask, c, cstride);
+        else if (LMAX > 1 && L == 1) add_image_L<(LMAX > 1 ? 1 : 0)>(acc, tab, mask, c, cstride);
+        else if (LMAX > 2 && L == 2) add_image_L<(LMAX > 2 ? 2 : 0)>(acc, tab, mask, c, cstride);
+        else if (LMAX > 3 && L == 3) add_image_L<(LMAX > 3 ? 3 : 0)>(acc, tab, mask, c, cstride);
+        else if (LMAX > 4 && L == 4) add_image_L<(LMAX > 4 ? 4 : 0)>(acc, tab, mask, c, cstride);
+        else if (LMAX > 5 && L == 5) add_image_L<(LMAX > 5 ? 5 : 0)>(acc, tab, mask, c, cstride);
+        else if (LMAX > 6 && L == 6) add_image_L<(LMAX > 6 ? 6 : 0)>(acc, tab, mask, c, cstride);
+    }
+    float *yb = y + size_t(b)*kBlk + reim*4096 + j;
+#pragma unroll
+    for (int p = 0; p < 64; ++p) if ((mask_all >> p) & 1u) yb[p*64] += acc[p];
+}
+
+template <int L>
+void launch_project_f32_L(DevicePlan &dp, float const *x, cudaStream_t st) {
+    auto const &g = dp.prj_items[L];
+    if (0 == g.count) return;
+    constexpr int smem = 2*kBlk*int(sizeof(float));
+    // 64 KB of dynamic shared memory (a per-device attribute, so set on every launch)
+    cudaFuncSetAttribute(sho_project_f32_kernel<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    sho_project_f32_kernel<L><<<g.count, kThreads, smem, st>>>(
+        dptr<float>(dp.apc), x, dp.nCols, dptr<uint32_t>(g.items), dptr<uint32_t>(dp.prj_col),
+        dptr<uint64_t>(dp.prj_coloff), dptr<uint32_t>(dp.prj_slot), dptr<float>(dp.slot_H32),
+        dptr<uint64_t>(dp.slot_mask), dp.table_stride, dptr<uint32_t>(dp.img_starts));
+    count_launch();
+}
+
+} // namespace
+
+bool simt_f32_projector_supported(DevicePlan const &dp, void const *x) {
+    return dp.slot_H32.ptr && dp.lmax_max <= 7 && 0 == (reinterpret_cast<uintptr_t>(x) & 15u);
+}
+
+bool launch_project_f32(DevicePlan &dp, float const *x, cudaStream_t st) {
+    A43G_CUDA_TRY(cudaMemsetAsync(dp.apc.ptr, 0, size_t(dp.ncoeffI)*dp.nCols*128*sizeof(float), st));
+    launch_project_f32_L<0>(dp, x, st); launch_project_f32_L<1>(dp, x, st);
+    launch_project_f32_L<2>(dp, x, st); launch_project_f32_L<3>(dp, x, st);
+    launch_project_f32_L<4>(dp, x, st); launch_project_f32_L<5>(dp, x, st);
+    launch_project_f32_L<6>(dp, x, st); launch_project_f32_L<7>(dp, x, st);
+    A43G_CUDA_TRY(cudaGetLastError());
+    return true;
+}
+
+template <int LMAX>
+void launch_add_f32_L(DevicePlan &dp, float *y, uint16_t const *colIndex, cudaStream_t st) {
+    sho_add_f32_kernel<LMAX><<<dp.nnzb, kThreads, 0, st>>>(y, dptr<float>(dp.cad), dp.nCols, colIndex,
+        dptr<uint32_t>(dp.add_start), dptr<uint32_t>(dp.add_col), dptr<uint32_t>(dp.add_slot),
+        dptr<float>(dp.slot_H32), dptr<uint64_t>(dp.slot_mask), dp.table_stride,
+        dptr<int8_t>(dp.img_lmax), dptr<uint32_t>(dp.img_starts));
+}
+
+bool launch_add_f32(DevicePlan &dp, float *y, uint16_t const *colIndex, cudaStream_t st) {
+    switch (dp.lmax_max) {
+        case 0: launch_add_f32_L<0>(dp, y, colIndex, st); break;
+        case 1: launch_add_f32_L<1>(dp, y, colIndex, st); break;
+        case 2: launch_add_f32_L<2>(dp, y, colIndex, st); break;
+        case 3: launch_add_f32_L<3>(dp, y, colIndex, st); break;
+        case 4: launch_add_f32_L<4>(dp, y, colIndex, st); break;
+        case 5: launch_add_f32_L<5>(dp, y, colIndex, st); break;
+        case 6: launch_add_f32_L<6>(dp, y, colIndex, st); break;
+        default: launch_add_f32_L<7>(dp, y, colIndex, st); break;
+    }
+    count_launch();
+    A43G_CUDA_TRY(cudaGetLastError());
+    return true;
+}
+
+} // namespace a43g
