@@ -10,7 +10,8 @@
 //   K_DX  D, X advanced by both half steps at once;  U1 = W + b U2
 //   K_E   V  = AU1 + b (AU2 + b V)      and rt^H V
 // The shadow residual rt is a counter-based random vector regenerated on the fly, so it is
-// never stored.  Per-column reductions end in double atomics; the scalar recurrences run in
+// never stored.  FP32 sweeps do the vector arithmetic in FP32 and accumulate the inner
+// products in FP64.  Per-column reductions end in double atomics; the scalar recurrences run in
 // FP64 in one thread per column.  Finished columns (converged or broken down) get zero
 // coefficients, which freezes X and keeps all vectors finite.
 #include "solver.hpp"
@@ -53,6 +54,11 @@ __device__ __forceinline__ uint32_t mix32(uint32_t h) {
 // shadow residual element for (block, reim, i, j): uniform in [-1, 1)
 __device__ __forceinline__ double shadow(uint32_t seed, uint32_t idx) {
     return double(int32_t(mix32(idx*0x9E3779B9u + seed))) * (1.0/2147483648.0);
+}
+
+// the same element in FP32 (the double value above rounded to float)
+__device__ __forceinline__ float shadow32(uint32_t seed, uint32_t idx) {
+    return float(int32_t(mix32(idx*0x9E3779B9u + seed))) * (1.0f/2147483648.0f);
 }
 
 template <typename T>
@@ -99,7 +105,9 @@ __global__ void __launch_bounds__(256) k_init_dots(T const *W, T const *V, uint3
         for (int i = q*16; i < q*16 + 16; ++i) {
             size_t const o = size_t(b)*kBlk + i*64 + j;
             uint32_t const idx = uint32_t(o);
-            double const tr = shadow(seed, idx), ti = shadow(seed, idx + 4096u);
+            // FP32 sweeps use the shadow vector rounded to FP32 throughout
+            double const tr = (sizeof(T) == 4) ? double(shadow32(seed, idx)) : shadow(seed, idx);
+            double const ti = (sizeof(T) == 4) ? double(shadow32(seed, idx + 4096u)) : shadow(seed, idx + 4096u);
             double const xr = W[o], xi = W[o + 4096], yr = V[o], yi = V[o + 4096];
             n2 += xr*xr + xi*xi;
             wr += tr*xr + ti*xi; wi += tr*xi - ti*xr;     // conj(rt) w
@@ -120,6 +128,20 @@ __global__ void __launch_bounds__(256) k_A(T *U2, T const *U1, T const *V, T con
         uint32_t const col = colindx[b]*64 + j;
         double const ar = cs[col].al_re, ai = cs[col].al_im;
         double n2 = 0;
+        if constexpr (sizeof(T) == 4) {
+            // FP32 sweep: vector arithmetic in FP32, the norm accumulated in FP64
+            float const fr = float(ar), fi = float(ai);
+#pragma unroll 8
+            for (int i = q*16; i < q*16 + 16; ++i) {
+                size_t const o = size_t(b)*kBlk + i*64 + j;
+                float const vr = V[o], vi = V[o + 4096];
+                U2[o] = fmaf(fi, vi, fmaf(-fr, vr, U1[o]));
+                U2[o + 4096] = fmaf(-fi, vr, fmaf(-fr, vi, U1[o + 4096]));
+                float const ur = AU1[o], ui = AU1[o + 4096];
+                float const wr = fmaf(fi, ui, fmaf(-fr, ur, W[o])), wi = fmaf(-fi, ur, fmaf(-fr, ui, W[o + 4096]));
+                n2 += double(fmaf(wr, wr, wi*wi));
+            }
+        } else {
 #pragma unroll 8
         for (int i = q*16; i < q*16 + 16; ++i) {
             size_t const o = size_t(b)*kBlk + i*64 + j;
@@ -129,6 +151,7 @@ __global__ void __launch_bounds__(256) k_A(T *U2, T const *U1, T const *V, T con
             double aur, aui; cmul(ar, ai, AU1[o], AU1[o + 4096], aur, aui);
             double const wr = double(W[o]) - aur, wi = double(W[o + 4096]) - aui;
             n2 += wr*wr + wi*wi;
+        }
         }
         reduce_cols(red, q, j, n2, 0.0, 0.0, &acc[col], 1);
     }
@@ -144,6 +167,20 @@ __global__ void __launch_bounds__(256) k_C(T *W, T const *AU1, T const *AU2, uin
         uint32_t const col = colindx[b]*64 + j;
         double const ar = cs[col].al_re, ai = cs[col].al_im;
         double n2 = 0, dr = 0, di = 0;
+        if constexpr (sizeof(T) == 4) {
+            float const fr = float(ar), fi = float(ai);
+#pragma unroll 8
+            for (int i = q*16; i < q*16 + 16; ++i) {
+                size_t const o = size_t(b)*kBlk + i*64 + j;
+                float const sr = AU1[o] + AU2[o], si = AU1[o + 4096] + AU2[o + 4096];
+                float const wr = fmaf(fi, si, fmaf(-fr, sr, W[o])), wi = fmaf(-fi, sr, fmaf(-fr, si, W[o + 4096]));
+                W[o] = wr; W[o + 4096] = wi;
+                uint32_t const idx = uint32_t(o);
+                float const tr = shadow32(seed, idx), ti = shadow32(seed, idx + 4096u);
+                n2 += double(fmaf(wr, wr, wi*wi));
+                dr += double(fmaf(tr, wr, ti*wi)); di += double(fmaf(tr, wi, -ti*wr));
+            }
+        } else
 #pragma unroll 8
         for (int i = q*16; i < q*16 + 16; ++i) {
             size_t const o = size_t(b)*kBlk + i*64 + j;
@@ -173,6 +210,26 @@ __global__ void __launch_bounds__(256) k_DX(TX *X, T *D, T *U1, T const *U2, T c
         double const ax_r = s.cu1x_re, ax_i = s.cu1x_im, bx_r = s.cu2x_re, bx_i = s.cu2x_im, cx_r = s.cdx_re, cx_i = s.cdx_im;
         double const ad_r = s.cu1d_re, ad_i = s.cu1d_im, cd_r = s.cdd_re, cd_i = s.cdd_im;
         double const be_r = s.be_re, be_i = s.be_im;
+        if constexpr (sizeof(T) == 4 && sizeof(TX) == 4) {
+            float const a_r = ax_r, a_i = ax_i, b_r = bx_r, b_i = bx_i, c_r = cx_r, c_i = cx_i;
+            float const d_r = ad_r, d_i = ad_i, e_r = cd_r, e_i = cd_i, g_r = be_r, g_i = be_i;
+#pragma unroll 8
+            for (int i = q*16; i < q*16 + 16; ++i) {
+                size_t const o = size_t(b)*kBlk + i*64 + j;
+                float const u1r = U1[o], u1i = U1[o + 4096], u2r = U2[o], u2i = U2[o + 4096];
+                float const dr = D[o], di = D[o + 4096];
+                float xr = X[o], xi = X[o + 4096];
+                xr = fmaf(a_r, u1r, fmaf(-a_i, u1i, xr)); xi = fmaf(a_r, u1i, fmaf(a_i, u1r, xi));
+                xr = fmaf(b_r, u2r, fmaf(-b_i, u2i, xr)); xi = fmaf(b_r, u2i, fmaf(b_i, u2r, xi));
+                xr = fmaf(c_r, dr, fmaf(-c_i, di, xr));   xi = fmaf(c_r, di, fmaf(c_i, dr, xi));
+                X[o] = xr; X[o + 4096] = xi;
+                D[o] = fmaf(d_r, u1r, fmaf(-d_i, u1i, fmaf(e_r, dr, fmaf(-e_i, di, u2r))));
+                D[o + 4096] = fmaf(d_r, u1i, fmaf(d_i, u1r, fmaf(e_r, di, fmaf(e_i, dr, u2i))));
+                U1[o] = fmaf(g_r, u2r, fmaf(-g_i, u2i, W[o]));
+                U1[o + 4096] = fmaf(g_r, u2i, fmaf(g_i, u2r, W[o + 4096]));
+            }
+            continue;
+        }
 #pragma unroll 8
         for (int i = q*16; i < q*16 + 16; ++i) {
             size_t const o = size_t(b)*kBlk + i*64 + j;
@@ -200,6 +257,20 @@ __global__ void __launch_bounds__(256) k_E(T *V, T const *AU1, T const *AU2, uin
         uint32_t const col = colindx[b]*64 + j;
         double const br = cs[col].be_re, bi = cs[col].be_im;
         double dr = 0, di = 0;
+        if constexpr (sizeof(T) == 4) {
+            float const fr = float(br), fi = float(bi);
+#pragma unroll 8
+            for (int i = q*16; i < q*16 + 16; ++i) {
+                size_t const o = size_t(b)*kBlk + i*64 + j;
+                float const vr = V[o], vi = V[o + 4096];
+                float const t1r = fmaf(-fi, vi, fmaf(fr, vr, AU2[o])), t1i = fmaf(fi, vr, fmaf(fr, vi, AU2[o + 4096]));
+                float const sr = fmaf(-fi, t1i, fmaf(fr, t1r, AU1[o])), si = fmaf(fi, t1r, fmaf(fr, t1i, AU1[o + 4096]));
+                V[o] = sr; V[o + 4096] = si;
+                uint32_t const idx = uint32_t(o);
+                float const tr = shadow32(seed, idx), ti = shadow32(seed, idx + 4096u);
+                dr += double(fmaf(tr, sr, ti*si)); di += double(fmaf(tr, si, -ti*sr));
+            }
+        } else
 #pragma unroll 8
         for (int i = q*16; i < q*16 + 16; ++i) {
             size_t const o = size_t(b)*kBlk + i*64 + j;
