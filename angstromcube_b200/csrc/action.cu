@@ -662,6 +662,56 @@ bool launch_action(DevicePlan &dp, T *y, T const *x, uint16_t const *colIndex, c
     return launch_dyadic<T>(dp, y, x, colIndex, st);
 }
 
+// ---------------------------------------------------------------- pieces of the dyadic part with
+// caller-given buffers and tables (FP64), for the vector-Jacobian products
+
+namespace {
+template <typename T, int L>
+void project_into_L(DevicePlan &dp, T *apc, T const *x, double const *table, cudaStream_t st) {
+    auto const &g = dp.prj_items[L];
+    if (0 == g.count) return;
+    sho_project_kernel<T, L><<<g.count, 128, 0, st>>>(
+        apc, x, dp.nCols, dptr<uint32_t>(g.items), dptr<uint32_t>(dp.prj_col), dptr<uint64_t>(dp.prj_coloff),
+        dptr<uint32_t>(dp.prj_slot), table, dptr<uint64_t>(dp.slot_mask), dp.table_stride, dptr<uint32_t>(dp.img_starts));
+    count_launch();
+}
+
+// generic projection (zeroes apc, then atomics per work item) into a caller-given buffer
+template <typename T>
+bool project_into(DevicePlan &dp, T *apc, T const *x, double const *table, cudaStream_t st) {
+    A43G_CUDA_TRY(cudaMemsetAsync(apc, 0, size_t(dp.ncoeffI)*dp.nCols*128*sizeof(T), st));
+    project_into_L<T, 0>(dp, apc, x, table, st); project_into_L<T, 1>(dp, apc, x, table, st);
+    project_into_L<T, 2>(dp, apc, x, table, st); project_into_L<T, 3>(dp, apc, x, table, st);
+    project_into_L<T, 4>(dp, apc, x, table, st); project_into_L<T, 5>(dp, apc, x, table, st);
+    project_into_L<T, 6>(dp, apc, x, table, st); project_into_L<T, 7>(dp, apc, x, table, st);
+    A43G_CUDA_TRY(cudaGetLastError());
+    return true;
+}
+} // namespace
+
+bool launch_project_with(DevicePlan &dp, double *apc, double const *x, double const *table, cudaStream_t st) {
+    return project_into<double>(dp, apc, x, table, st);
+}
+
+bool launch_collect_with(DevicePlan &dp, double *aac, double const *apc, double const *img_phase, cudaStream_t st) {
+    dim3 const ga(dp.nAtoms, dp.nCols);
+    sho_collect_kernel<double><<<ga, 64, 0, st>>>(aac, apc, dp.nCols, dptr<uint32_t>(dp.atom_starts),
+        dptr<int8_t>(dp.atom_lmax), dptr<uint32_t>(dp.sum_start), dptr<uint32_t>(dp.sum_col),
+        dptr<uint32_t>(dp.img_starts), img_phase);
+    count_launch();
+    A43G_CUDA_TRY(cudaGetLastError());
+    return true;
+}
+
+bool launch_mul_with(DevicePlan &dp, double *out, double const *in, cudaStream_t st) {
+    dim3 const ga(dp.nAtoms, dp.nCols);
+    sho_mul_kernel<double, double><<<ga, 64, 0, st>>>(out, in, dp.nCols, dptr<uint32_t>(dp.atom_starts),
+        dptr<int8_t>(dp.atom_lmax), dptr<double>(dp.atom_mat), dptr<uint32_t>(dp.atom_mat_off));
+    count_launch();
+    A43G_CUDA_TRY(cudaGetLastError());
+    return true;
+}
+
 template bool launch_local<double>(DevicePlan &, double *, double const *, cudaStream_t);
 template bool launch_local<float>(DevicePlan &, float *, float const *, cudaStream_t);
 template bool launch_dyadic<double>(DevicePlan &, double *, double const *, uint16_t const *, cudaStream_t);

@@ -2,6 +2,7 @@
 #include "../../include/a43g.h"
 #include "device.cuh"
 #include "solver.hpp"
+#include "vjp.hpp"
 
 #include <atomic>
 #include <cstring>
@@ -12,6 +13,7 @@ struct a43g_plan {
     a43g::GreenPlan host;
     a43g::DevicePlan dev;
     a43g::SolverWorkspace solver;
+    a43g::VjpWorkspace vjpws;
     bool energy_set = false;
     bool matrices_set = false;
     int device = -1;
@@ -211,6 +213,16 @@ int a43g_action_multiply(a43g_plan_t *plan, void *y, const void *x, const uint16
     if (!ok) return A43G_ERR_CUDA;
     if (flops) *flops = a43g::action_flops(plan->host, (A43G_F64 == dtype) ? 8 : 4);
     return A43G_OK;
+}
+
+int a43g_vjp(a43g_plan_t *plan, const void *L, const void *G, double *dV, double *dM, double *dR, void *stream) {
+    if (!plan || !L || !G) return fail(A43G_ERR_ARGUMENT, "null argument");
+    std::lock_guard<std::mutex> lock(plan->mtx);
+    if (!plan->energy_set) return fail(A43G_ERR_STATE, "energy parameter not set (a43g_plan_set_energy)");
+    int const rc = ensure_device(plan);
+    if (rc) return rc;
+    return a43g::vjp(plan->host, plan->dev, plan->vjpws, (double const*)L, (double const*)G, dV, dM, dR,
+                     (cudaStream_t)stream);
 }
 
 int a43g_action_part(a43g_plan_t *plan, int part, void *y, const void *x, void *stream, int dtype) {

@@ -92,6 +92,14 @@ bool launch_dyadic(DevicePlan &dp, T *y, T const *x, uint16_t const *colIndex, c
 
 double action_flops(GreenPlan const &hp, int real_bytes);
 
+
+// FP64 pieces of the dyadic part on caller-given buffers (vector-Jacobian products):
+// apc = P x with the given projector tables (zeroed first); aac = sum over images of
+// img_phase * apc; out = M in (atom matrices of the plan)
+bool launch_project_with(DevicePlan &dp, double *apc, double const *x, double const *table, cudaStream_t st);
+bool launch_collect_with(DevicePlan &dp, double *aac, double const *apc, double const *img_phase, cudaStream_t st);
+bool launch_mul_with(DevicePlan &dp, double *out, double const *in, cudaStream_t st);
+
 // tensor-core (tcgen05, 3xTF32) projection and addition of the FP32 action (projector_tc.cu)
 bool tc_projector_supported(DevicePlan const &dp);
 bool launch_project_tc(DevicePlan &dp, float const *x, cudaStream_t st);

@@ -123,6 +123,9 @@ struct GreenPlan {
     void set_energy(double Er, double Ei, double dVol, double scale_H = 1.0);
     // update_phases (src/green_function.cxx:218-251)
     std::string set_kpoint(double const k[3]);
+    // slot_H with the functions of direction dir replaced by their derivative with respect to
+    // the atom position (vector-Jacobian products; the reference has no derivatives)
+    std::vector<double> position_derivative_tables(int dir) const;
 };
 
 // set_phase (src/kinetic_plan.cxx:214-269): returns the deviation of the purified values

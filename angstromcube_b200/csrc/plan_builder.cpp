@@ -583,4 +583,31 @@ std::string GreenPlan::set_kpoint(double const k[3]) {
     return "";
 }
 
+// d/dR H_nu(xi) = -(1/sigma) (nu H_{nu-1}(xi) - xi H_nu(xi)) with xi = (r - R)/sigma, because the
+// unnormalized Hermite-Gauss functions H_nu = h_nu exp(-xi^2/2) have h_nu' = nu h_{nu-1}; the
+// points and the cut-off are those of slot_H (the 1D functions vanish outside the radius)
+std::vector<double> GreenPlan::position_derivative_tables(int dir) const {
+    std::vector<double> T(slot_H);
+    if (table_lmax < 0 || dir < 0 || dir > 2) return T;
+    int const nt = (table_lmax + 1)*12;
+    for (uint32_t a = 0; a < nAtomImages; ++a) {
+        int const lmax = AtomImageLmax[a];
+        double const isq = AtomImagePos[4*size_t(a) + 3], sinv = isq*isq;
+        for (uint32_t k = img_rows.start[a]; k < img_rows.start[a + 1]; ++k) {
+            float const *tc = &rowCubePos[4*size_t(img_rows.col[k])];
+            double const *H = &slot_H[size_t(k)*nt];
+            double *D = &T[size_t(k)*nt];
+            for (int i4 = 0; i4 < 4; ++i4) {
+                double const xi = sinv*((double(tc[dir])*4 + i4 + 0.5)*grid_spacing_dyadic[dir] - AtomImagePos[4*size_t(a) + dir]);
+                for (int nu = 0; nu <= lmax; ++nu) {
+                    double const hn = H[(nu*3 + dir)*4 + i4];
+                    double const hm = (nu > 0) ? H[((nu - 1)*3 + dir)*4 + i4] : 0.0;
+                    D[(nu*3 + dir)*4 + i4] = -sinv*(nu*hm - xi*hn);
+                }
+            }
+        }
+    }
+    return T;
+}
+
 } // namespace a43g

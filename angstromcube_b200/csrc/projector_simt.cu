@@ -14,7 +14,9 @@
 //     (16-byte copies, so x must be 16-byte aligned), and the partial coefficients of the item
 //     are added to the zeroed image coefficients with one atomic per coefficient;
 //   * addition: one CTA per block b, summing the contributions of all images near b in
-//     registers and updating y[b] once.
+//     registers and updating y[b] once; the coefficients of the next image are staged in shared
+//     memory with cp.async while the current one is applied (16-byte copies of rows that start
+//     on 512-byte boundaries of the plan's coefficient array).
 #include "device.cuh"
 
 namespace a43g {
@@ -153,7 +155,7 @@ __device__ __forceinline__ void add_image(float (&acc)[64], Tables<L> const &t, 
             float ax[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll
             for (int ix = 0; ix <= L - iz - iy; ++ix, ++sho) {
-                float const cv = __ldg(c + size_t(sho)*cstride);
+                float const cv = c[size_t(sho)*cstride];
 #pragma unroll
                 for (int xx = 0; xx < 4; ++xx) ax[xx] = fmaf(t.h[ix][0][xx], cv, ax[xx]);
             }
@@ -195,32 +197,54 @@ sho_add_f32_kernel(float *__restrict__ y, float const *__restrict__ cad, uint32_
                    float const *__restrict__ slot_H, uint64_t const *__restrict__ slot_mask, int stride,
                    int8_t const *__restrict__ img_lmax, uint32_t const *__restrict__ img_starts)
 {
+    constexpr int NCMAX = nsho_of(LMAX);
+    extern __shared__ __align__(16) float cbuf[];     // [2][NCMAX][128] coefficients of two images
     uint32_t const b = blockIdx.x;
     uint32_t const k0 = add_start[b], k1 = add_start[b + 1];
     if (k0 >= k1) return;
     int const tid = threadIdx.x, reim = tid >> 6, j = tid & 63;
     uint32_t const s = colIndex[b];
     size_t const cstride = size_t(nrhs)*128;
+    // the coefficients of image k (nSHO rows of 128 floats) go to shared memory ahead of use
+    auto stage = [&](uint32_t k, int buf) {
+        uint32_t const a = add_col[k];
+        int const L = img_lmax[a], nc = nsho_of(L);
+        float const *src = cad + (size_t(img_starts[a])*nrhs + s)*128;
+        float *dst = cbuf + buf*NCMAX*128;
+        for (int q = tid; q < nc*32; q += kThreads) {
+            int const row = q >> 5, part = (q & 31)*4;
+            cp_async16(dst + row*128 + part, src + size_t(row)*cstride + part);
+        }
+    };
     float acc[64];
 #pragma unroll
     for (int i = 0; i < 64; ++i) acc[i] = 0.f;
     uint64_t mask_all = 0;
-    for (uint32_t k = k0; k < k1; ++k) {
+    stage(k0, 0);
+    cp_async_commit();
+    int buf = 0;
+    for (uint32_t k = k0; k < k1; ++k, buf ^= 1) {
+        if (k + 1 < k1) stage(k + 1, buf ^ 1);
+        cp_async_commit();
+        cp_async_wait1();
+        __syncthreads();
         uint32_t const a = add_col[k], slot = add_slot[k];
         uint64_t const mask = slot_mask[slot];
-        if (!mask) continue;
-        mask_all |= mask;
-        float const *tab = slot_H + size_t(slot)*stride;
-        float const *c = cad + (size_t(img_starts[a])*nrhs + s)*128 + reim*64 + j;
-        int const L = img_lmax[a];                 // uniform over the CTA
-        if (L == LMAX) add_image_L<LMAX>(acc, tab, mask, c, cstride);
-        else if (LMAX > 0 && L == 0) add_image_L<0>(acc, tab, mask, c, cstride);
-        else if (LMAX > 1 && L == 1) add_image_L<(LMAX > 1 ? 1 : 0)>(acc, tab, mask, c, cstride);
-        else if (LMAX > 2 && L == 2) add_image_L<(LMAX > 2 ? 2 : 0)>(acc, tab, mask, c, cstride);
-        else if (LMAX > 3 && L == 3) add_image_L<(LMAX > 3 ? 3 : 0)>(acc, tab, mask, c, cstride);
-        else if (LMAX > 4 && L == 4) add_image_L<(LMAX > 4 ? 4 : 0)>(acc, tab, mask, c, cstride);
-        else if (LMAX > 5 && L == 5) add_image_L<(LMAX > 5 ? 5 : 0)>(acc, tab, mask, c, cstride);
-        else if (LMAX > 6 && L == 6) add_image_L<(LMAX > 6 ? 6 : 0)>(acc, tab, mask, c, cstride);
+        if (mask) {
+            mask_all |= mask;
+            float const *tab = slot_H + size_t(slot)*stride;
+            float const *c = cbuf + buf*NCMAX*128 + reim*64 + j;
+            int const L = img_lmax[a];                 // uniform over the CTA
+            if (L == LMAX) add_image_L<LMAX>(acc, tab, mask, c, 128);
+            else if (LMAX > 0 && L == 0) add_image_L<0>(acc, tab, mask, c, 128);
+            else if (LMAX > 1 && L == 1) add_image_L<(LMAX > 1 ? 1 : 0)>(acc, tab, mask, c, 128);
+            else if (LMAX > 2 && L == 2) add_image_L<(LMAX > 2 ? 2 : 0)>(acc, tab, mask, c, 128);
+            else if (LMAX > 3 && L == 3) add_image_L<(LMAX > 3 ? 3 : 0)>(acc, tab, mask, c, 128);
+            else if (LMAX > 4 && L == 4) add_image_L<(LMAX > 4 ? 4 : 0)>(acc, tab, mask, c, 128);
+            else if (LMAX > 5 && L == 5) add_image_L<(LMAX > 5 ? 5 : 0)>(acc, tab, mask, c, 128);
+            else if (LMAX > 6 && L == 6) add_image_L<(LMAX > 6 ? 6 : 0)>(acc, tab, mask, c, 128);
+        }
+        __syncthreads();                           // buffer buf is free for image k + 2
     }
     float *yb = y + size_t(b)*kBlk + reim*4096 + j;
 #pragma unroll
@@ -259,7 +283,9 @@ bool launch_project_f32(DevicePlan &dp, float const *x, cudaStream_t st) {
 
 template <int LMAX>
 void launch_add_f32_L(DevicePlan &dp, float *y, uint16_t const *colIndex, cudaStream_t st) {
-    sho_add_f32_kernel<LMAX><<<dp.nnzb, kThreads, 0, st>>>(y, dptr<float>(dp.cad), dp.nCols, colIndex,
+    constexpr int smem = 2*nsho_of(LMAX)*128*int(sizeof(float));
+    cudaFuncSetAttribute(sho_add_f32_kernel<LMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    sho_add_f32_kernel<LMAX><<<dp.nnzb, kThreads, smem, st>>>(y, dptr<float>(dp.cad), dp.nCols, colIndex,
         dptr<uint32_t>(dp.add_start), dptr<uint32_t>(dp.add_col), dptr<uint32_t>(dp.add_slot),
         dptr<float>(dp.slot_H32), dptr<uint64_t>(dp.slot_mask), dp.table_stride,
         dptr<int8_t>(dp.img_lmax), dptr<uint32_t>(dp.img_starts));

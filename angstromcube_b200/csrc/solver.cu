@@ -39,7 +39,9 @@ struct ColState {
     // combined coefficients of K_DX (X and D advanced over both half steps)
     double cu1x_re, cu1x_im, cu2x_re, cu2x_im, cdx_re, cdx_im;
     double cu1d_re, cu1d_im, cdd_re, cdd_im;
-    int32_t status;              // 0 active, 1 converged, 2 breakdown, 3 idle (zero column)
+    double tau_ref;              // stall detection: tau at the last halving, and its half step
+    int32_t m_ref;
+    int32_t status;              // 0 active, 1 converged, 2 breakdown, 3 idle (zero column), 4 stalled
     int32_t conv1;               // converged in the first half step of this iteration
 };
 
@@ -228,8 +230,7 @@ __global__ void __launch_bounds__(256) k_DX(TX *X, T *D, T *U1, T const *U2, T c
                 U1[o] = fmaf(g_r, u2r, fmaf(-g_i, u2i, W[o]));
                 U1[o + 4096] = fmaf(g_r, u2i, fmaf(g_i, u2r, W[o + 4096]));
             }
-            continue;
-        }
+        } else
 #pragma unroll 8
         for (int i = q*16; i < q*16 + 16; ++i) {
             size_t const o = size_t(b)*kBlk + i*64 + j;
@@ -306,6 +307,7 @@ __global__ void s_init(ColState *cs, Acc *accW, Acc *accV, uint32_t ncol, int32_
     ColState s{};
     double const bn = sqrt(accW[c].n2);
     s.bnorm = bn; s.tau = bn; s.theta = 0; s.eta_re = s.eta_im = 0;
+    s.tau_ref = bn; s.m_ref = 0;
     s.rho_re = accW[c].re; s.rho_im = accW[c].im;
     double const sr = accV[c].re, si = accV[c].im;
     if (!(bn > 0)) { s.status = 3; freeze(s); }
@@ -338,7 +340,12 @@ __global__ void s_half1(ColState *cs, Acc *acc, uint32_t ncol, int m, double tol
 }
 
 // second half step m = 2n: coefficients of K_DX, beta, rho; counts active columns
-__global__ void s_half2(ColState *cs, Acc *acc, uint32_t ncol, int m, double tol, int32_t *counters) {
+// stall_level > 0 (FP32 correction sweeps only): a column whose estimate is already below
+// stall_level and whose tau has not halved within stall_window half steps has reached the
+// rounding floor of the sweep; it is frozen like a converged one (the refinement step then
+// restarts from the true FP64 residual)
+__global__ void s_half2(ColState *cs, Acc *acc, uint32_t ncol, int m, double tol, int32_t *counters,
+                        double stall_level, int stall_window) {
     uint32_t const c = blockIdx.x*blockDim.x + threadIdx.x;
     if (c >= ncol) return;
     ColState s = cs[c];
@@ -377,8 +384,12 @@ __global__ void s_half2(ColState *cs, Acc *acc, uint32_t ncol, int m, double tol
     // beta = rho_n / rho_{n-1}
     double br, bi; cdiv(rnr, rni, s.rho_re, s.rho_im, br, bi);
     s.be_re = br; s.be_im = bi; s.rho_re = rnr; s.rho_im = rni;
-    if (tau*sqrt(double(m) + 1.0) <= tol*s.bnorm) {
+    double const est = tau*sqrt(double(m) + 1.0);
+    if (tau <= 0.5*s.tau_ref) { s.tau_ref = tau; s.m_ref = m; }
+    if (est <= tol*s.bnorm) {
         s.status = 1; s.be_re = s.be_im = 0; s.al_re = s.al_im = 0;
+    } else if (stall_level > 0 && est <= stall_level*s.bnorm && m - s.m_ref > stall_window) {
+        s.status = 4; s.be_re = s.be_im = 0; s.al_re = s.al_im = 0;
     } else if (rnr*rnr + rni*rni == 0.0) {
         s.status = 2; s.be_re = s.be_im = 0; s.al_re = s.al_im = 0; atomicAdd(&counters[1], 1);
     } else {
@@ -500,6 +511,9 @@ SolverWorkspace::~SolverWorkspace() {
 
 namespace {
 
+// half steps without a halving of tau after which a column of an FP32 sweep counts as stalled
+constexpr int kStallWindow = 60;
+
 struct InnerResult { int iterations = 0; int converged = 0; int breakdowns = 0; double estimate = 0; double applications = 0; };
 
 // tfQMR on the vectors of precision T whose W, U1 hold the right-hand side and D is zero;
@@ -507,7 +521,7 @@ struct InnerResult { int iterations = 0; int converged = 0; int breakdowns = 0; 
 // correction (zero for a plain solve)
 template <typename T, typename TX>
 bool tfqmr_inner(DevicePlan &dp, SolverWorkspace &ws, TfqmrVectors &v, TX *Xs, double tol, int maxit, int check_every,
-                 uint32_t seed, cudaStream_t st, InnerResult &res, int echo) {
+                 uint32_t seed, cudaStream_t st, InnerResult &res, int echo, double stall_level = 0) {
     uint32_t const nnzb = dp.nnzb, ncol = dp.nCols*64;
     uint16_t const *ci = dptr<uint16_t>(dp.colindx);
     auto *cs = dptr<ColState>(ws.colstate);
@@ -539,7 +553,7 @@ bool tfqmr_inner(DevicePlan &dp, SolverWorkspace &ws, TfqmrVectors &v, TX *Xs, d
         if (!launch_action<T>(dp, AU2, U2, ci, st)) return false;
         k_C<T><<<g, 256, 0, st>>>(W, AU1, AU2, nnzb, ci, cs, accA, seed);
         count_launch();
-        s_half2<<<gs, 256, 0, st>>>(cs, accA, ncol, 2*it, tol, cnt);
+        s_half2<<<gs, 256, 0, st>>>(cs, accA, ncol, 2*it, tol, cnt, stall_level, kStallWindow);
         count_launch();
         k_DX<T, TX><<<g, 256, 0, st>>>(X, D, U1, U2, W, nnzb, ci, cs);
         count_launch();
@@ -675,7 +689,9 @@ int solve(GreenPlan &hp, DevicePlan &dp, SolverWorkspace &ws, a43g_solve_options
             double const itol = std::max(inner_tol, 0.5*opt.tolerance/rmax);
             // FP32 correction sweep (keeping its solution in FP64 does not lower the FP32 residual
             // floor, measured, so the correction is accumulated once per sweep)
-            if (!tfqmr_inner<float, float>(dp, ws, v, dptr<float>(v.X), itol, left, check, seed + 7919u*uint32_t(ref + 1), st, res, opt.echo)) return A43G_ERR_CUDA;
+            // columns stalled below 10x the sweep tolerance end the sweep (FP32 rounding floor)
+            if (!tfqmr_inner<float, float>(dp, ws, v, dptr<float>(v.X), itol, left, check, seed + 7919u*uint32_t(ref + 1), st, res,
+                                           opt.echo, 10*itol)) return A43G_ERR_CUDA;
             k_accumulate<float><<<g*8, 256, 0, st>>>(X64, dptr<float>(v.X), n);
             count_launch();
             if (!residual64(dp, ws, X64, R64, AX64, st, rmax, res.applications)) return A43G_ERR_CUDA;

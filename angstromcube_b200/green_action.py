@@ -86,3 +86,31 @@ def solve_batched(plan, energies, kpoints, dVol, want_rho=False, stream=0, **kw)
                                         stats, st), "a43g_solve_batched")
     out = [stats[i].as_dict() for i in range(n)]
     return out, (rho[..., 0] + 1j * rho[..., 1] if want_rho else None)
+
+
+def vjp(plan, L, G, potential=True, matrices=True, positions=True, stream=0):
+    """Derivatives of F = sum over blocks and columns of L^T (H - E S) G (complex, no
+    conjugation) for CUDA float64 tensors L, G [nnzb, 2, 64, 64].  Returns a dict with
+      "V": complex [ncells, 64]        dF/dV in cell-cube layout,
+      "M": list of complex [nc, nc]    dF/dM_A per plan atom (order of export()["global_atom_ids"]),
+      "R": complex [nAtoms, 3]         dF/dR_A (atom positions)."""
+    e = plan.export()
+    nat = len(e["AtomLmax"])
+    ncs = [((int(l) + 1) * (int(l) + 2) * (int(l) + 3)) // 6 for l in e["AtomLmax"]]   # int8 in the export
+    dV = np.zeros((plan.sizes["ncells"], 64, 2)) if potential else None
+    dM = np.zeros(max(1, sum(2 * n * n for n in ncs))) if matrices else None
+    dR = np.zeros((max(nat, 1), 3, 2)) if positions else None
+    st = ctypes.c_void_p(stream if isinstance(stream, int) else stream.cuda_stream)
+    check(_lib.lib().a43g_vjp(plan.handle, ptr(L), ptr(G), ptr(dV), ptr(dM), ptr(dR), st), "a43g_vjp")
+    out = {}
+    if potential:
+        out["V"] = dV[..., 0] + 1j * dV[..., 1]
+    if matrices:
+        mats, o = [], 0
+        for n in ncs:
+            mats.append(dM[o:o + n * n].reshape(n, n) + 1j * dM[o + n * n:o + 2 * n * n].reshape(n, n))
+            o += 2 * n * n
+        out["M"] = mats
+    if positions:
+        out["R"] = (dR[..., 0] + 1j * dR[..., 1])[:nat]
+    return out

@@ -133,6 +133,20 @@ int a43g_action_multiply(a43g_plan_t *plan, void *y, const void *x, const uint16
  *         include/green_dyadic.hxx:856-922). */
 int a43g_action_part(a43g_plan_t *plan, int part, void *y, const void *x, void *stream, int dtype);
 
+/* ---- vector-Jacobian products of the action (no reference counterpart: the reference has no
+ * derivatives, forces or adjoint).  For device FP64 block vectors L and G [nnzb][2][64][64]
+ * the bilinear form  F = sum over blocks and columns of L^T (H - E S) G  (complex, without
+ * conjugation) is differentiated with respect to
+ *   dV: the local potential, host complex [ncells][64][2]  (cell-cube layout of a43g_plan_set_potential);
+ *   dM: the atom matrices M_A = dVol (dH - E dS) of the plan's atoms (export AtomStarts and
+ *       global_atom_ids give their order), host complex, per atom [2][nc][nc] (real plane, then
+ *       imaginary plane), concatenated;
+ *   dR: the atom positions, host complex [nAtoms][3][2] (x, y, z).
+ * Any output may be NULL.  With G = (H - E S)^-1 B and L the adjoint Green function (the solve at
+ * conj(E), conjugated, times the weights of a functional) -dF gives the gradient of that functional.
+ * Synchronizes the stream. */
+int a43g_vjp(a43g_plan_t *plan, const void *L, const void *G, double *dV, double *dM, double *dR, void *stream);
+
 /* synchronizes the device and reports an error a kernel of this plan recorded (for example a
  * bounded wait of the tensor-core projector that timed out); clears the record */
 int a43g_plan_device_status(a43g_plan_t *plan);
