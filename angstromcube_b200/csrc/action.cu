@@ -712,6 +712,44 @@ bool launch_mul_with(DevicePlan &dp, double *out, double const *in, cudaStream_t
     return true;
 }
 
+// the whole action with the dyadic coefficients in caller-given scratch (generic kernels only)
+template <typename T>
+bool launch_action_scratch(DevicePlan &dp, T *y, T const *x, uint16_t const *colIndex, cudaStream_t st,
+                           DyadicScratch const &sc) {
+    if (!launch_local<T>(dp, y, x, st)) return false;
+    if (dp.nAI < 1 || dp.nCols < 1) return true;
+    T *apc = static_cast<T*>(sc.apc), *cad = static_cast<T*>(sc.cad);
+    if (!project_into<T>(dp, apc, x, dptr<double>(dp.slot_H), st)) return false;
+    dim3 const ga(dp.nAtoms, dp.nCols);
+    if (dp.nAI > dp.nAtoms) {
+        sho_collect_kernel<T><<<ga, 64, 0, st>>>(sc.aac, apc, dp.nCols,
+            dptr<uint32_t>(dp.atom_starts), dptr<int8_t>(dp.atom_lmax), dptr<uint32_t>(dp.sum_start),
+            dptr<uint32_t>(dp.sum_col), dptr<uint32_t>(dp.img_starts), dptr<double>(dp.img_phase));
+        count_launch();
+        sho_mul_kernel<double, double><<<ga, 64, 0, st>>>(sc.cadd, sc.aac, dp.nCols,
+            dptr<uint32_t>(dp.atom_starts), dptr<int8_t>(dp.atom_lmax), dptr<double>(dp.atom_mat), dptr<uint32_t>(dp.atom_mat_off));
+        count_launch();
+        sho_broadcast_kernel<T><<<ga, 64, 0, st>>>(cad, sc.cadd, dp.nCols,
+            dptr<uint32_t>(dp.atom_starts), dptr<int8_t>(dp.atom_lmax), dptr<uint32_t>(dp.sum_start),
+            dptr<uint32_t>(dp.sum_col), dptr<uint32_t>(dp.img_starts), dptr<double>(dp.img_phase));
+        count_launch();
+    } else {
+        sho_mul_kernel<T, T><<<ga, 64, 0, st>>>(cad, apc, dp.nCols,
+            dptr<uint32_t>(dp.atom_starts), dptr<int8_t>(dp.atom_lmax), dptr<double>(dp.atom_mat), dptr<uint32_t>(dp.atom_mat_off));
+        count_launch();
+    }
+    sho_add_kernel<T><<<dp.nnzb, 128, 0, st>>>(y, cad, dp.nCols, dp.nnzb, colIndex,
+        dptr<uint32_t>(dp.add_start), dptr<uint32_t>(dp.add_col), dptr<uint32_t>(dp.add_slot),
+        dptr<double>(dp.slot_H), dptr<uint64_t>(dp.slot_mask), dp.table_stride,
+        dptr<int8_t>(dp.img_lmax), dptr<uint32_t>(dp.img_starts));
+    count_launch();
+    A43G_CUDA_TRY(cudaGetLastError());
+    return true;
+}
+
+template bool launch_action_scratch<double>(DevicePlan &, double *, double const *, uint16_t const *, cudaStream_t, DyadicScratch const &);
+template bool launch_action_scratch<float>(DevicePlan &, float *, float const *, uint16_t const *, cudaStream_t, DyadicScratch const &);
+
 template bool launch_local<double>(DevicePlan &, double *, double const *, cudaStream_t);
 template bool launch_local<float>(DevicePlan &, float *, float const *, cudaStream_t);
 template bool launch_dyadic<double>(DevicePlan &, double *, double const *, uint16_t const *, cudaStream_t);

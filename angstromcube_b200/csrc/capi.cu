@@ -3,6 +3,7 @@
 #include "device.cuh"
 #include "solver.hpp"
 #include "vjp.hpp"
+#include "noalloc.hpp"
 
 #include <atomic>
 #include <cstring>
@@ -210,6 +211,35 @@ int a43g_action_multiply(a43g_plan_t *plan, void *y, const void *x, const uint16
     if (A43G_F64 == dtype) ok = a43g::launch_action<double>(plan->dev, (double*)y, (double const*)x, colIndex, st);
     else if (A43G_F32 == dtype) ok = a43g::launch_action<float>(plan->dev, (float*)y, (float const*)x, colIndex, st);
     else return fail(A43G_ERR_ARGUMENT, "dtype must be A43G_F64 or A43G_F32");
+    if (!ok) return A43G_ERR_CUDA;
+    if (flops) *flops = a43g::action_flops(plan->host, (A43G_F64 == dtype) ? 8 : 4);
+    return A43G_OK;
+}
+
+int a43g_action_multiply_noalloc(a43g_plan_t *plan, void *y, const void *x, const uint16_t *colIndex,
+                                 uint32_t nnzb, uint32_t nCols, void *stream, int dtype, double *flops) {
+    if (!plan || (!y && nnzb) || (!x && nnzb) || (!colIndex && nnzb)) return fail(A43G_ERR_ARGUMENT, "null argument");
+    std::lock_guard<std::mutex> lock(plan->mtx);
+    if (nnzb != plan->host.nnzb()) return fail(A43G_ERR_ARGUMENT, "nnzb does not match the plan");
+    if (nCols != plan->host.nCols) return fail(A43G_ERR_ARGUMENT, "nCols does not match the plan");
+    if (!plan->energy_set) return fail(A43G_ERR_STATE, "energy parameter not set (a43g_plan_set_energy)");
+    if (y == x) return fail(A43G_ERR_ARGUMENT, "y and x must not alias");
+    if (A43G_F64 != dtype && A43G_F32 != dtype) return fail(A43G_ERR_ARGUMENT, "dtype must be A43G_F64 or A43G_F32");
+    // this entry point never uploads (uploading allocates): the plan must be current on this device
+    int dev = -1;
+    if (cudaSuccess != cudaGetDevice(&dev)) return fail(A43G_ERR_CUDA, "no CUDA device available");
+    if (!plan->dev.uploaded || plan->device != dev || plan->dev.values_dirty)
+        return fail(A43G_ERR_STATE, "the plan is not current on this device: call a43g_plan_upload after the last "
+                                    "change of potential, matrices, energy or k-point");
+    size_t const need = a43g::noalloc_required(plan->dev, (A43G_F64 == dtype) ? 8 : 4);
+    if (need > a43g::noalloc_capacity())
+        return fail(A43G_ERR_UNSUPPORTED, "the projector coefficients of this plan need " + std::to_string(need) +
+                    " bytes of scratch, more than the " + std::to_string(a43g::noalloc_capacity()) +
+                    " bytes of the allocation-free entry point; use a43g_action_multiply");
+    auto const st = (cudaStream_t)stream;
+    bool const ok = (A43G_F64 == dtype)
+        ? a43g::action_noalloc<double>(plan->dev, (double*)y, (double const*)x, colIndex, st)
+        : a43g::action_noalloc<float>(plan->dev, (float*)y, (float const*)x, colIndex, st);
     if (!ok) return A43G_ERR_CUDA;
     if (flops) *flops = a43g::action_flops(plan->host, (A43G_F64 == dtype) ? 8 : 4);
     return A43G_OK;

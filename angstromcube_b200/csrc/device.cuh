@@ -92,6 +92,13 @@ bool launch_dyadic(DevicePlan &dp, T *y, T const *x, uint16_t const *colIndex, c
 
 double action_flops(GreenPlan const &hp, int real_bytes);
 
+// the action with the dyadic coefficients in caller-given scratch instead of the plan's
+// buffers: apc, cad hold ncoeffI*nCols*128 reals of the action's precision, aac, cadd
+// ncoeffA*nCols*128 doubles (apc is zeroed by the call; the others are overwritten)
+struct DyadicScratch { void *apc, *cad; double *aac, *cadd; };
+template <typename T>
+bool launch_action_scratch(DevicePlan &dp, T *y, T const *x, uint16_t const *colIndex, cudaStream_t st,
+                           DyadicScratch const &sc);
 
 // FP64 pieces of the dyadic part on caller-given buffers (vector-Jacobian products):
 // apc = P x with the given projector tables (zeroed first); aac = sum over images of

@@ -126,6 +126,20 @@ int a43g_action_multiply(a43g_plan_t *plan, void *y, const void *x, const uint16
                          uint32_t nnzb, uint32_t nCols, unsigned l2nX, void *stream, int dtype,
                          double *flops);
 
+/* ---- the same action without any device allocation.  No counterpart in the reference (its
+ * action allocates its projector scratch on every call).  For callers that must not let a
+ * library allocate device memory: work recorded into a CUDA graph, hosts whose memory pool owns
+ * all device memory, loops that cannot afford the device-wide synchronization of cudaMalloc.
+ * The projector coefficients live in one fixed 16 MiB array compiled into the library (present
+ * on every GPU that loads it until the process exits); plans that need more are rejected with
+ * A43G_ERR_UNSUPPORTED.  The plan must already be current on the calling device
+ * (a43g_plan_upload after the last change of potential, matrices, energy or k-point), else
+ * A43G_ERR_STATE.  The first call on each device looks up the array's device address; make it
+ * before any stream capture.  All calls on a device share the array: calls whose GPU work
+ * overlaps race on it and must be serialized by the caller.  Arguments as a43g_action_multiply. */
+int a43g_action_multiply_noalloc(a43g_plan_t *plan, void *y, const void *x, const uint16_t *colIndex,
+                                 uint32_t nnzb, uint32_t nCols, void *stream, int dtype, double *flops);
+
 /* ---- one part of the operator, for profiling and for the adjoint kernels (no reference
  * counterpart; the reference applies the parts only together inside action_t::multiply):
  * part 0: y = (V - E) x + T x  (local potential and kinetic energy, include/green_potential.hxx
