@@ -425,17 +425,28 @@ sho_mul_kernel(Tout *__restrict__ out, Tin const *__restrict__ in, uint32_t nrhs
     int const nc = nsho_c(atom_lmax[A]);
     size_t const a0 = atom_starts[A];
     double const *Mr = mats + mat_off[A], *Mi = Mr + nc*nc;
-    for (int i = 0; i < nc; ++i) {
-        double re = 0, im = 0;
+    constexpr int R = 8;                       // output rows per pass: each input value is loaded once per R rows
+    for (int i0 = 0; i0 < nc; i0 += R) {
+        double re[R], im[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) { re[r] = 0; im[r] = 0; }
         for (int k = 0; k < nc; ++k) {
             Tin const *src = in + ((a0 + k)*nrhs + s)*128;
             double const xr = double(src[j]), xi = double(src[64 + j]);
-            double const mr = Mr[i*nc + k], mi = Mi[i*nc + k];
-            re += mr*xr - mi*xi;
-            im += mr*xi + mi*xr;
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                int const i = (i0 + r < nc) ? i0 + r : nc - 1;   // clamped rows are not stored
+                double const mr = __ldg(Mr + i*nc + k), mi = __ldg(Mi + i*nc + k);
+                re[r] += mr*xr - mi*xi;
+                im[r] += mr*xi + mi*xr;
+            }
         }
-        Tout *dst = out + ((a0 + i)*nrhs + s)*128;
-        dst[j] = Tout(re); dst[64 + j] = Tout(im);
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            if (i0 + r >= nc) break;
+            Tout *dst = out + ((a0 + i0 + r)*nrhs + s)*128;
+            dst[j] = Tout(re[r]); dst[64 + j] = Tout(im[r]);
+        }
     }
 }
 
@@ -610,7 +621,8 @@ bool launch_dyadic(DevicePlan &dp, T *y, T const *x, uint16_t const *colIndex, c
     // both FP32 projector paths stage x with 16-byte loads; other x take the generic kernels
     bool const aligned16 = 0 == (reinterpret_cast<uintptr_t>(x) & 15u);
     bool const tc = (sizeof(T) == 4) && dp.use_tc && aligned16 && tc_projector_supported(dp);
-    bool const simt32 = (sizeof(T) == 4) && !tc && simt_f32_projector_supported(dp, x);
+    bool const simt32 = (sizeof(T) == 4) && !tc && simt_f32_projector_supported(dp, x) &&
+                        0 == (reinterpret_cast<uintptr_t>(y) & 15u);
     if (tc) {
         if (!launch_project_tc(dp, (float const*)x, st)) return false;
     } else if (simt32) {

@@ -62,6 +62,7 @@ struct DevicePlan {
     DeviceBuffer subset_dev;     // uint32 [nCols] diagonal block of each source column
     DeviceBuffer slot_H, slot_mask, prj_slot, add_slot;   // projector tables per (image, row)
     DeviceBuffer slot_H32;       // float copy of slot_H for the FP32 kernels
+    DeviceBuffer add_info;       // uint4 per SHOadd entry: slot, first coefficient of the image, basis size, 0
     int table_stride = 0;        // doubles per slot in slot_H
     DeviceBuffer dev_error;      // int: first error code recorded by a kernel (0: none)
     bool use_tc = true;          // FP32 projector on the tensor cores (else SIMT)
@@ -112,8 +113,8 @@ bool tc_projector_supported(DevicePlan const &dp);
 bool launch_project_tc(DevicePlan &dp, float const *x, cudaStream_t st);
 bool launch_add_tc(DevicePlan &dp, float *y, uint16_t const *colIndex, cudaStream_t st);
 
-// sum-factorized FP32 projection and addition on the CUDA cores (projector_simt.cu); the
-// projection stages blocks with 16-byte copies and needs a 16-byte aligned x
+// sum-factorized FP32 projection and addition on the CUDA cores (projector_simt.cu); both
+// stage blocks with 16-byte copies and need 16-byte aligned x and y
 bool simt_f32_projector_supported(DevicePlan const &dp, void const *x);
 bool launch_project_f32(DevicePlan &dp, float const *x, cudaStream_t st);
 bool launch_add_f32(DevicePlan &dp, float *y, uint16_t const *colIndex, cudaStream_t st);

@@ -139,6 +139,16 @@ bool upload_plan(GreenPlan const &hp, DevicePlan &dp) {
     if (!put(dp.slot_H, hp.slot_H) || !put(dp.slot_mask, hp.slot_mask)) return false;
     if (!put(dp.slot_H32, std::vector<float>(hp.slot_H.begin(), hp.slot_H.end()))) return false;
     if (!put(dp.prj_slot, hp.prj_slot) || !put(dp.add_slot, hp.add_slot)) return false;
+    {   // one 16-byte record per addition pair, so the kernel needs no dependent index loads
+        std::vector<uint32_t> info(4*size_t(hp.SHOadd.nnz()), 0u);
+        for (size_t k = 0; k < hp.SHOadd.nnz(); ++k) {
+            uint32_t const a = hp.SHOadd.col[k];
+            info[4*k + 0] = hp.add_slot[k];
+            info[4*k + 1] = hp.AtomImageStarts[a];
+            info[4*k + 2] = uint32_t(hp.AtomImageLmax[a]);
+        }
+        if (!put(dp.add_info, info)) return false;
+    }
     if (!put(dp.subset_dev, hp.subset)) return false;
     if (!put(dp.dev_error, std::vector<int32_t>(4, 0))) return false;
     {

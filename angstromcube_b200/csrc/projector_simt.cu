@@ -36,6 +36,7 @@ __device__ __forceinline__ void cp_async16(void *dst, void const *src) {
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
 // the 1D tables of one slot: T[nu][dir][i] at tab[(nu*3 + dir)*4 + i], dir 0/1/2 = x/y/z
 template <int L>
@@ -50,6 +51,22 @@ __device__ __forceinline__ void load_tables(Tables<L> &t, float const *__restric
             float4 const v = __ldg(reinterpret_cast<float4 const*>(tab + (nu*3 + d)*4));
             t.h[nu][d][0] = v.x; t.h[nu][d][1] = v.y; t.h[nu][d][2] = v.z; t.h[nu][d][3] = v.w;
         }
+}
+
+// the same from a table staged in shared memory
+template <int L>
+__device__ __forceinline__ void load_tables_shared(Tables<L> &t, float const *tab) {
+#pragma unroll
+    for (int nu = 0; nu <= L; ++nu)
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            float4 const v = *reinterpret_cast<float4 const*>(tab + (nu*3 + d)*4);
+            t.h[nu][d][0] = v.x; t.h[nu][d][1] = v.y; t.h[nu][d][2] = v.z; t.h[nu][d][3] = v.w;
+        }
+}
+
+__device__ __forceinline__ void cp_async8(void *dst, void const *src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" :: "r"(smem_addr(dst)), "l"(src) : "memory");
 }
 
 // ---------------------------------------------------------------- projection
@@ -69,32 +86,40 @@ sho_project_f32_kernel(float *__restrict__ apc, float const *__restrict__ x, uin
     int const tid = threadIdx.x, reim = tid >> 6, j = tid & 63;
     uint64_t const off = prj_coloff[s];
 
-    auto stage = [&](uint32_t k, int buf) {
-        char const *src = reinterpret_cast<char const*>(x + size_t(prj_col[off + k])*kBlk);
+    __shared__ __align__(16) float tbuf[2][(L + 1)*12];   // 1D tables of the staged blocks' slots
+    __shared__ uint64_t mbuf[2];                           // and their masks
+    // block, table and mask of list position k go to shared memory ahead of use; the block and
+    // slot indices are loaded one position earlier still
+    auto stage = [&](uint32_t b, uint32_t slot, int buf) {
+        char const *src = reinterpret_cast<char const*>(x + size_t(b)*kBlk);
         char *dst = reinterpret_cast<char*>(xs + buf*kBlk);
 #pragma unroll
         for (int r = 0; r < kBlk*4/(16*kThreads); ++r) {
             int const o = (r*kThreads + tid)*16;
             cp_async16(dst + o, src + o);
         }
+        if (tid < (L + 1)*3) cp_async16(&tbuf[buf][tid*4], slot_H + size_t(slot)*stride + tid*4);
+        if (tid == kThreads - 1) cp_async8(&mbuf[buf], slot_mask + slot);
     };
 
     float acc[NS];
 #pragma unroll
     for (int i = 0; i < NS; ++i) acc[i] = 0.f;
 
-    stage(k0, 0);
+    stage(prj_col[off + k0], prj_slot[off + k0], 0);
     cp_async_commit();
+    uint32_t nb = 0, ns = 0;
+    if (k0 + 1 < k1) { nb = prj_col[off + k0 + 1]; ns = prj_slot[off + k0 + 1]; }
     int buf = 0;
     for (uint32_t k = k0; k < k1; ++k, buf ^= 1) {
-        if (k + 1 < k1) stage(k + 1, buf ^ 1);
+        if (k + 1 < k1) stage(nb, ns, buf ^ 1);
         cp_async_commit();
+        if (k + 2 < k1) { nb = prj_col[off + k + 2]; ns = prj_slot[off + k + 2]; }   // for the next iteration
         cp_async_wait1();                            // block k has landed (this thread's copies)
         __syncthreads();                             // ... and everybody else's
-        uint32_t const slot = prj_slot[off + k];
         Tables<L> t;
-        load_tables<L>(t, slot_H + size_t(slot)*stride);
-        uint64_t const mask = slot_mask[slot];
+        load_tables_shared<L>(t, tbuf[buf]);
+        uint64_t const mask = mbuf[buf];
         float const *xb = xs + buf*kBlk + reim*4096 + j;
 #pragma unroll
         for (int z = 0; z < 4; ++z) {
@@ -183,58 +208,91 @@ template <int L>
 __device__ __forceinline__ void add_image_L(float (&acc)[64], float const *__restrict__ tab, uint64_t mask,
                                             float const *__restrict__ c, size_t cstride) {
     Tables<L> t;
-    load_tables<L>(t, tab);
+    load_tables_shared<L>(t, tab);
     if (~0ull == mask) add_image<L, true>(acc, t, mask, c, cstride);
     else add_image<L, false>(acc, t, mask, c, cstride);
 }
 
-// LMAX: largest basis size of the plan (the switch below instantiates no larger one)
+// LMAX: largest basis size of the plan (the instantiation has no larger one).  One CTA walks the
+// blocks [b0, b1) (consecutive, same order as y) and treats their (block, image) pairs as one
+// stream: the coefficients, table and mask of the next pair are staged while the current pair is
+// applied, and the y values of the next block with atoms are staged during the whole of the
+// current block, so neither the start of a block nor its final y update waits for memory.
 template <int LMAX>
-__global__ void __launch_bounds__(kThreads, 3)
-sho_add_f32_kernel(float *__restrict__ y, float const *__restrict__ cad, uint32_t nrhs,
-                   uint16_t const *__restrict__ colIndex, uint32_t const *__restrict__ add_start,
-                   uint32_t const *__restrict__ add_col, uint32_t const *__restrict__ add_slot,
-                   float const *__restrict__ slot_H, uint64_t const *__restrict__ slot_mask, int stride,
-                   int8_t const *__restrict__ img_lmax, uint32_t const *__restrict__ img_starts)
+__global__ void __launch_bounds__(kThreads, 2)
+sho_add_f32_kernel(float *__restrict__ y, float const *__restrict__ cad, uint32_t nrhs, uint32_t nnzb,
+                   uint32_t blocks_per_cta, uint16_t const *__restrict__ colIndex,
+                   uint32_t const *__restrict__ add_start, uint4 const *__restrict__ info,
+                   float const *__restrict__ slot_H, uint64_t const *__restrict__ slot_mask, int stride)
 {
     constexpr int NCMAX = nsho_of(LMAX);
-    extern __shared__ __align__(16) float cbuf[];     // [2][NCMAX][128] coefficients of two images
-    uint32_t const b = blockIdx.x;
-    uint32_t const k0 = add_start[b], k1 = add_start[b + 1];
-    if (k0 >= k1) return;
+    extern __shared__ __align__(16) float smem_f[];
+    float *cbuf = smem_f;                                  // [2][NCMAX][128] coefficients of two pairs
+    float *ybuf = smem_f + 2*NCMAX*128;                    // [8192] y of the current block
+    __shared__ __align__(16) float tbuf[2][(LMAX + 1)*12];
+    __shared__ uint64_t mbuf[2];
+    uint32_t const b0 = blockIdx.x*blocks_per_cta, b1 = min(b0 + blocks_per_cta, nnzb);
+    if (b0 >= b1) return;
+    uint32_t const T0 = add_start[b0], T1 = add_start[b1];
+    if (T0 >= T1) return;                                  // no atoms near any of these blocks
     int const tid = threadIdx.x, reim = tid >> 6, j = tid & 63;
-    uint32_t const s = colIndex[b];
     size_t const cstride = size_t(nrhs)*128;
-    // the coefficients of image k (nSHO rows of 128 floats) go to shared memory ahead of use
-    auto stage = [&](uint32_t k, int buf) {
-        uint32_t const a = add_col[k];
-        int const L = img_lmax[a], nc = nsho_of(L);
-        float const *src = cad + (size_t(img_starts[a])*nrhs + s)*128;
+
+    // the block owning pair t: blocks are visited in order, skipping blocks without pairs
+    uint32_t bb = b0;
+    while (add_start[bb + 1] <= T0) ++bb;
+    uint32_t s = colIndex[bb];
+    uint32_t bend = add_start[bb + 1];                     // first pair of the next block
+
+    auto stage_pair = [&](uint4 const inf, uint32_t src_col, int buf) {
+        int const L = int(inf.z), nc = nsho_of(L);
+        float const *src = cad + (size_t(inf.y)*nrhs + src_col)*128;
         float *dst = cbuf + buf*NCMAX*128;
         for (int q = tid; q < nc*32; q += kThreads) {
             int const row = q >> 5, part = (q & 31)*4;
             cp_async16(dst + row*128 + part, src + size_t(row)*cstride + part);
         }
+        if (tid < (L + 1)*3) cp_async16(&tbuf[buf][tid*4], slot_H + size_t(inf.x)*stride + tid*4);
+        if (tid == kThreads - 1) cp_async8(&mbuf[buf], slot_mask + inf.x);
     };
+    auto stage_y = [&](uint32_t blk) {
+        float const *src = y + size_t(blk)*kBlk;
+#pragma unroll
+        for (int r = 0; r < kBlk/(4*kThreads); ++r) {
+            int const o = (r*kThreads + tid)*4;
+            cp_async16(ybuf + o, src + o);
+        }
+    };
+    // the source column of the pair after t (it may belong to a later block)
+    auto column_of = [&](uint32_t t) -> uint32_t {
+        uint32_t c = bb;
+        while (add_start[c + 1] <= t) ++c;
+        return colIndex[c];
+    };
+
     float acc[64];
 #pragma unroll
     for (int i = 0; i < 64; ++i) acc[i] = 0.f;
     uint64_t mask_all = 0;
-    stage(k0, 0);
+    uint4 const zero4 = make_uint4(0u, 0u, 0u, 0u);
+    uint4 cur = info[T0];
+    stage_y(bb);
+    stage_pair(cur, s, 0);
     cp_async_commit();
+    uint4 nxt = (T0 + 1 < T1) ? info[T0 + 1] : zero4;
     int buf = 0;
-    for (uint32_t k = k0; k < k1; ++k, buf ^= 1) {
-        if (k + 1 < k1) stage(k + 1, buf ^ 1);
+    for (uint32_t t = T0; t < T1; ++t, buf ^= 1) {
+        if (t + 1 < T1) stage_pair(nxt, (t + 1 < bend) ? s : column_of(t + 1), buf ^ 1);
         cp_async_commit();
+        uint4 const after = (t + 2 < T1) ? info[t + 2] : zero4;
         cp_async_wait1();
         __syncthreads();
-        uint32_t const a = add_col[k], slot = add_slot[k];
-        uint64_t const mask = slot_mask[slot];
+        uint64_t const mask = mbuf[buf];
         if (mask) {
             mask_all |= mask;
-            float const *tab = slot_H + size_t(slot)*stride;
+            float const *tab = tbuf[buf];
             float const *c = cbuf + buf*NCMAX*128 + reim*64 + j;
-            int const L = img_lmax[a];                 // uniform over the CTA
+            int const L = int(cur.z);                      // uniform over the CTA
             if (L == LMAX) add_image_L<LMAX>(acc, tab, mask, c, 128);
             else if (LMAX > 0 && L == 0) add_image_L<0>(acc, tab, mask, c, 128);
             else if (LMAX > 1 && L == 1) add_image_L<(LMAX > 1 ? 1 : 0)>(acc, tab, mask, c, 128);
@@ -244,11 +302,30 @@ sho_add_f32_kernel(float *__restrict__ y, float const *__restrict__ cad, uint32_
             else if (LMAX > 5 && L == 5) add_image_L<(LMAX > 5 ? 5 : 0)>(acc, tab, mask, c, 128);
             else if (LMAX > 6 && L == 6) add_image_L<(LMAX > 6 ? 6 : 0)>(acc, tab, mask, c, 128);
         }
-        __syncthreads();                           // buffer buf is free for image k + 2
-    }
-    float *yb = y + size_t(b)*kBlk + reim*4096 + j;
+        cur = nxt; nxt = after;
+        if (t + 1 == bend) {
+            // last pair of block bb: y[bb] = staged y + sums on the points inside the spheres
+            cp_async_wait0();
+            __syncthreads();
+            float const *yb_s = ybuf + reim*4096 + j;
+            float *yb = y + size_t(bb)*kBlk + reim*4096 + j;
 #pragma unroll
-    for (int p = 0; p < 64; ++p) if ((mask_all >> p) & 1u) yb[p*64] += acc[p];
+            for (int p = 0; p < 64; ++p) {
+                if ((mask_all >> p) & 1u) yb[p*64] = yb_s[p*64] + acc[p];
+                acc[p] = 0.f;
+            }
+            mask_all = 0;
+            __syncthreads();                               // ybuf free
+            if (t + 1 < T1) {
+                ++bb;
+                while (add_start[bb + 1] <= t + 1) ++bb;
+                s = colIndex[bb];
+                bend = add_start[bb + 1];
+                stage_y(bb);                               // lands during the pairs of block bb
+            }
+        }
+        __syncthreads();                                   // buffers buf are free for pair t + 2
+    }
 }
 
 template <int L>
@@ -283,12 +360,13 @@ bool launch_project_f32(DevicePlan &dp, float const *x, cudaStream_t st) {
 
 template <int LMAX>
 void launch_add_f32_L(DevicePlan &dp, float *y, uint16_t const *colIndex, cudaStream_t st) {
-    constexpr int smem = 2*nsho_of(LMAX)*128*int(sizeof(float));
+    constexpr int smem = (2*nsho_of(LMAX)*128 + kBlk)*int(sizeof(float));
+    constexpr uint32_t kBlocksPerCta = 16;
     cudaFuncSetAttribute(sho_add_f32_kernel<LMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    sho_add_f32_kernel<LMAX><<<dp.nnzb, kThreads, smem, st>>>(y, dptr<float>(dp.cad), dp.nCols, colIndex,
-        dptr<uint32_t>(dp.add_start), dptr<uint32_t>(dp.add_col), dptr<uint32_t>(dp.add_slot),
-        dptr<float>(dp.slot_H32), dptr<uint64_t>(dp.slot_mask), dp.table_stride,
-        dptr<int8_t>(dp.img_lmax), dptr<uint32_t>(dp.img_starts));
+    unsigned const grid = (dp.nnzb + kBlocksPerCta - 1)/kBlocksPerCta;
+    sho_add_f32_kernel<LMAX><<<grid, kThreads, smem, st>>>(y, dptr<float>(dp.cad), dp.nCols, dp.nnzb, kBlocksPerCta,
+        colIndex, dptr<uint32_t>(dp.add_start), dptr<uint4>(dp.add_info), dptr<float>(dp.slot_H32),
+        dptr<uint64_t>(dp.slot_mask), dp.table_stride);
 }
 
 bool launch_add_f32(DevicePlan &dp, float *y, uint16_t const *colIndex, cudaStream_t st) {

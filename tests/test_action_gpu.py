@@ -152,7 +152,13 @@ def test_action_fp32_unaligned_input():
     y_off = torch.empty((p.nnzb, 2, 64, 64), dtype=torch.float32, device="cuda")
     op.multiply(y_off, x_off, ci, p.nnzb, p.nCols)
     torch.cuda.synchronize()
+    # and a y that is only 4-byte aligned
+    ybuf = torch.zeros(n + 1, dtype=torch.float32, device="cuda")
+    y_off2 = ybuf[1:].view(p.nnzb, 2, 64, 64)
+    op.multiply(y_off2, x_off.contiguous().clone(), ci, p.nnzb, p.nCols)
+    torch.cuda.synchronize()
     y_al = apply(p, xn, np.float32)
+    assert rel_err(y_off2.cpu().numpy(), y_al) < FP32_TOL
     y_ref = oracle.RestatedOracle(p.export(), Vc, E).action(xn.astype(np.float64))
     assert rel_err(y_off.cpu().numpy(), y_ref) < FP32_TOL
     assert rel_err(y_al, y_ref) < FP32_TOL
