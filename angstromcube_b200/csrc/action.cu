@@ -210,6 +210,159 @@ local_fused_kernel(T *__restrict__ y, T const *__restrict__ x,
     }
 }
 
+// The same fused local operator with the global loads of every step issued one step ahead:
+// the neighbour codes of the whole z-line are read into shared memory once, so the rows of cube
+// k+1 (its z-successor, its y and x neighbours and its potential row) are requested before cube
+// k is computed and arrive while it is.  Bloch phases are applied when the rows are consumed.
+// Lines of at most kMaxLine cubes (the host checks).
+constexpr int kMaxLine = 128;
+
+template <typename T> struct Rows { T re[4], im[4]; };
+
+template <typename T>
+__device__ __forceinline__ void row_raw(T const *__restrict__ x, int32_t e, int r, int col, Rows<T> &o) {
+    if (-1 == e) {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) { o.re[i] = T(0); o.im[i] = T(0); }
+        return;
+    }
+    T const *b = x + size_t(nbr_block(e))*kBlockReals + (r*4)*64 + col;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) { o.re[i] = __ldg(b + i*64); o.im[i] = __ldg(b + 4096 + i*64); }
+}
+
+template <typename T>
+__device__ __forceinline__ void row_phase(int32_t e, T pr, T pi, Rows<T> &o) {
+    if (e < -1) {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            T const a = pr*o.re[i] - pi*o.im[i], c = pr*o.im[i] + pi*o.re[i];
+            o.re[i] = a; o.im[i] = c;
+        }
+    }
+}
+
+template <typename T, int S>
+__global__ void __launch_bounds__(S*16, 2)
+local_fused_pf_kernel(T *__restrict__ y, T const *__restrict__ x,
+                      uint32_t const *__restrict__ zstart, int32_t const *__restrict__ zlist,
+                      int32_t const *__restrict__ nbr, int32_t const *__restrict__ veff,
+                      T const *__restrict__ Vcell, LocalArgs<T> const a)
+{
+    constexpr int NSL = 64/S, PAD = 68;
+    __shared__ __align__(16) T sm[5][2][S][PAD];   // slots: 3 rotating z-slots, y-, y+
+    __shared__ int32_t code[kMaxLine][8];           // per step: block, x-, x+, y-, y+, veff, z-next
+    __shared__ int32_t zleft, nline;
+    int const line = blockIdx.x/NSL, slice = blockIdx.x % NSL;
+    int const tid = threadIdx.x, j = tid % S, r = tid/S;       // r = z*4 + y
+    int const zq = r >> 2, yq = r & 3, col = slice*S + j;
+    int32_t const *L = zlist + zstart[line];
+    if (0 == tid) {
+        int n = 0;
+        while (L[4 + n] > 0) ++n;                   // lists end with 4 non-positive entries
+        nline = n; zleft = list_code(L[3]);
+    }
+    __syncthreads();
+    int const n = nline;
+    if (0 == n) return;                             // uniform: nothing on this line
+    for (int k = tid; k < n; k += S*16) {
+        int32_t const b = L[4 + k] - 1;
+        int32_t const *nb = nbr + 6*size_t(b);
+        code[k][0] = b; code[k][1] = nb[0]; code[k][2] = nb[1]; code[k][3] = nb[2]; code[k][4] = nb[3];
+        code[k][5] = veff[b]; code[k][6] = list_code(L[5 + k]);
+    }
+    __syncthreads();
+    T const (&cx)[5] = a.st.c[0];
+    T const (&cy)[5] = a.st.c[1];
+    T const (&cz)[5] = a.st.c[2];
+    T const c0 = cx[0] + cy[0] + cz[0];
+
+    Rows<T> cur;                                     // own row of the current cube
+    {
+        Rows<T> h;
+        row_raw(x, zleft, r, col, h);
+        row_phase(zleft, a.ph[2][0][0], a.ph[2][0][1], h);
+        sts_row(&sm[0][0][j][r*4], h.re); sts_row(&sm[0][1][j][r*4], h.im);
+    }
+    row_raw(x, code[0][0], r, col, cur);
+    sts_row(&sm[1][0][j][r*4], cur.re); sts_row(&sm[1][1][j][r*4], cur.im);
+    // rows of step 0 requested before the loop
+    Rows<T> pz, pym, pyp, pxm, pxp;
+    Row4<T> pV;
+    auto request = [&](int k) {
+        row_raw(x, code[k][6], r, col, pz);
+        row_raw(x, code[k][3], r, col, pym);
+        row_raw(x, code[k][4], r, col, pyp);
+        row_raw(x, code[k][1], r, col, pxm);
+        row_raw(x, code[k][2], r, col, pxp);
+        int32_t const iloc = code[k][5];
+        if (iloc < 0) { pV.v[0] = pV.v[1] = pV.v[2] = pV.v[3] = T(0); }
+        else pV = lds_row_global(Vcell + size_t(iloc)*64 + r*4);
+    };
+    request(0);
+    int sp = 0, sc = 1, sn = 2;
+    for (int k = 0; k < n; ++k) {
+        int32_t const b = code[k][0];
+        row_phase(code[k][6], a.ph[2][1][0], a.ph[2][1][1], pz);
+        row_phase(code[k][3], a.ph[1][0][0], a.ph[1][0][1], pym);
+        row_phase(code[k][4], a.ph[1][1][0], a.ph[1][1][1], pyp);
+        row_phase(code[k][1], a.ph[0][0][0], a.ph[0][0][1], pxm);
+        row_phase(code[k][2], a.ph[0][1][0], a.ph[0][1][1], pxp);
+        __syncthreads();                             // previous step finished reading the slots
+        sts_row(&sm[sn][0][j][r*4], pz.re);  sts_row(&sm[sn][1][j][r*4], pz.im);
+        sts_row(&sm[3][0][j][r*4], pym.re);  sts_row(&sm[3][1][j][r*4], pym.im);
+        sts_row(&sm[4][0][j][r*4], pyp.re);  sts_row(&sm[4][1][j][r*4], pyp.im);
+        __syncthreads();
+        T lr[12], li[12];                            // x-line: left row | own row | right row
+        T V[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            lr[i] = pxm.re[i]; li[i] = pxm.im[i];
+            lr[4 + i] = cur.re[i]; li[4 + i] = cur.im[i];
+            lr[8 + i] = pxp.re[i]; li[8 + i] = pxp.im[i];
+            V[i] = pV.v[i];
+        }
+        Rows<T> const nextc = pz;
+        if (k + 1 < n) request(k + 1);               // arrives while this cube is computed
+        T accr[4], acci[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            T const Vt = V[i] - a.E_re;
+            accr[i] = Vt*cur.re[i] + a.E_im*cur.im[i] + c0*cur.re[i];
+            acci[i] = Vt*cur.im[i] - a.E_im*cur.re[i] + c0*cur.im[i];
+        }
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int d = 1; d <= 4; ++d) {
+                accr[i] += cx[d]*(lr[4 + i - d] + lr[4 + i + d]);
+                acci[i] += cx[d]*(li[4 + i - d] + li[4 + i + d]);
+            }
+#pragma unroll
+        for (int d = 1; d <= 4; ++d) {
+            int const ym = yq - d, yp = yq + d, zm = zq - d, zp = zq + d;
+            int const s_ym = (ym < 0) ? 3 : sc, s_yp = (yp > 3) ? 4 : sc;
+            int const s_zm = (zm < 0) ? sp : sc, s_zp = (zp > 3) ? sn : sc;
+            int const o_ym = (zq*4 + (ym & 3))*4, o_yp = (zq*4 + (yp & 3))*4;
+            int const o_zm = ((zm & 3)*4 + yq)*4, o_zp = ((zp & 3)*4 + yq)*4;
+            Row4<T> const r1 = lds_row(&sm[s_ym][0][j][o_ym]), r2 = lds_row(&sm[s_yp][0][j][o_yp]);
+            Row4<T> const r3 = lds_row(&sm[s_zm][0][j][o_zm]), r4 = lds_row(&sm[s_zp][0][j][o_zp]);
+            Row4<T> const i1 = lds_row(&sm[s_ym][1][j][o_ym]), i2 = lds_row(&sm[s_yp][1][j][o_yp]);
+            Row4<T> const i3 = lds_row(&sm[s_zm][1][j][o_zm]), i4 = lds_row(&sm[s_zp][1][j][o_zp]);
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                accr[i] += cy[d]*(r1.v[i] + r2.v[i]) + cz[d]*(r3.v[i] + r4.v[i]);
+                acci[i] += cy[d]*(i1.v[i] + i2.v[i]) + cz[d]*(i3.v[i] + i4.v[i]);
+            }
+        }
+        T *yb = y + size_t(b)*kBlockReals + (r*4)*64 + col;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) { yb[i*64] = accr[i]; yb[4096 + i*64] = acci[i]; }
+        int const t = sp; sp = sc; sc = sn; sn = t;  // rotate the z-slots
+        cur = nextc;
+    }
+}
+
 // ---------------------------------------------------------------- generic local path
 
 // y = (V - E) x for every block (include/green_potential.hxx:15-139, collinear)
@@ -574,7 +727,11 @@ bool launch_local(DevicePlan &dp, T *y, T const *x, cudaStream_t st) {
         for (int d = 0; d < 3; ++d) for (int s = 0; s < 2; ++s) for (int c = 0; c < 2; ++c) a.ph[d][s][c] = T(dp.phase[d][s][c]);
         constexpr int S = (sizeof(T) == 8) ? 8 : 16;
         unsigned const nblk = dp.nlists[2]*(64/S);
-        if (nblk) {
+        if (nblk && sizeof(T) == 4 && dp.max_zline <= kMaxLine) {
+            local_fused_pf_kernel<T, S><<<nblk, S*16, 0, st>>>(y, x, dptr<uint32_t>(dp.lists_start[2]),
+                dptr<int32_t>(dp.lists[2]), dptr<int32_t>(dp.nbr), dptr<int32_t>(dp.veff_index), vcell<T>(dp), a);
+            count_launch();
+        } else if (nblk) {
             local_fused_kernel<T, S><<<nblk, S*16, 0, st>>>(y, x, dptr<uint32_t>(dp.lists_start[2]),
                 dptr<int32_t>(dp.lists[2]), dptr<int32_t>(dp.nbr), dptr<int32_t>(dp.veff_index), vcell<T>(dp), a);
             count_launch();

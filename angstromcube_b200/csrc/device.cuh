@@ -43,6 +43,7 @@ struct DevicePlan {
     double grid[4] = {0, 0, 0, 0};
     double E_re = 0, E_im = 0;
     bool fused_local = false;    // all directions use the 9-point stencil: fused kernel
+    uint32_t max_zline = 0;      // cubes in the longest z-line
     uint32_t nlists[3] = {0, 0, 0};
 
     DeviceBuffer veff_index;     // int32 [nnzb]

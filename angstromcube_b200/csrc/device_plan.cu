@@ -82,6 +82,14 @@ bool upload_plan(GreenPlan const &hp, DevicePlan &dp) {
     }
     dp.grid[3] = hp.grid_spacing_dyadic[3];
     dp.fused_local = all4;
+    dp.max_zline = 0;
+    {
+        auto const &K = hp.kinetic[2];
+        for (uint32_t il = 0; il < K.nlists(); ++il) {
+            uint32_t const len = K.start[il + 1] - K.start[il];
+            dp.max_zline = std::max(dp.max_zline, len > 2*kNhalo ? len - 2*kNhalo : 0u);
+        }
+    }
 
     if (!put(dp.veff_index, hp.veff_index)) return false;
     if (!put(dp.nbr, neighbour_table(hp))) return false;

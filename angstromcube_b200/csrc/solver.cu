@@ -123,16 +123,17 @@ __global__ void __launch_bounds__(256) k_init_dots(T const *W, T const *V, uint3
 // K_A: U2 = U1 - alpha V ; acc |W - alpha AU1|^2
 template <typename T>
 __global__ void __launch_bounds__(256) k_A(T *U2, T const *U1, T const *V, T const *W, T const *AU1, uint32_t nnzb,
-                                           uint16_t const *colindx, ColState const *cs, Acc *acc) {
+                                           uint16_t const *colindx, ColState const *cs, Acc *acc,
+                                           float const *cf, uint32_t ncol) {
     __shared__ double red[4][64][3];
     int const j = threadIdx.x & 63, q = threadIdx.x >> 6;
     for (uint32_t b = blockIdx.x; b < nnzb; b += gridDim.x) {
         uint32_t const col = colindx[b]*64 + j;
-        double const ar = cs[col].al_re, ai = cs[col].al_im;
         double n2 = 0;
         if constexpr (sizeof(T) == 4) {
-            // FP32 sweep: vector arithmetic in FP32, the norm accumulated in FP64
-            float const fr = float(ar), fi = float(ai);
+            // FP32 sweep: vector arithmetic in FP32, 32-term partial sums in FP32, the rest in FP64
+            float const fr = cf[col], fi = cf[ncol + col];
+            float n2f = 0.f;
 #pragma unroll 8
             for (int i = q*16; i < q*16 + 16; ++i) {
                 size_t const o = size_t(b)*kBlk + i*64 + j;
@@ -141,9 +142,11 @@ __global__ void __launch_bounds__(256) k_A(T *U2, T const *U1, T const *V, T con
                 U2[o + 4096] = fmaf(-fi, vr, fmaf(-fr, vi, U1[o + 4096]));
                 float const ur = AU1[o], ui = AU1[o + 4096];
                 float const wr = fmaf(fi, ui, fmaf(-fr, ur, W[o])), wi = fmaf(-fi, ur, fmaf(-fr, ui, W[o + 4096]));
-                n2 += double(fmaf(wr, wr, wi*wi));
+                n2f = fmaf(wr, wr, fmaf(wi, wi, n2f));
             }
+            n2 = double(n2f);
         } else {
+        double const ar = cs[col].al_re, ai = cs[col].al_im;
 #pragma unroll 8
         for (int i = q*16; i < q*16 + 16; ++i) {
             size_t const o = size_t(b)*kBlk + i*64 + j;
@@ -162,15 +165,17 @@ __global__ void __launch_bounds__(256) k_A(T *U2, T const *U1, T const *V, T con
 // K_C: W = W - alpha (AU1 + AU2) ; acc |W|^2 and rt^H W
 template <typename T>
 __global__ void __launch_bounds__(256) k_C(T *W, T const *AU1, T const *AU2, uint32_t nnzb,
-                                           uint16_t const *colindx, ColState const *cs, Acc *acc, uint32_t seed) {
+                                           uint16_t const *colindx, ColState const *cs, Acc *acc, uint32_t seed,
+                                           float const *cf, uint32_t ncol) {
     __shared__ double red[4][64][3];
     int const j = threadIdx.x & 63, q = threadIdx.x >> 6;
     for (uint32_t b = blockIdx.x; b < nnzb; b += gridDim.x) {
         uint32_t const col = colindx[b]*64 + j;
-        double const ar = cs[col].al_re, ai = cs[col].al_im;
+        double const ar = (sizeof(T) == 8) ? cs[col].al_re : 0.0, ai = (sizeof(T) == 8) ? cs[col].al_im : 0.0;
         double n2 = 0, dr = 0, di = 0;
         if constexpr (sizeof(T) == 4) {
-            float const fr = float(ar), fi = float(ai);
+            float const fr = cf[col], fi = cf[ncol + col];
+            float n2f = 0.f, drf = 0.f, dif = 0.f;
 #pragma unroll 8
             for (int i = q*16; i < q*16 + 16; ++i) {
                 size_t const o = size_t(b)*kBlk + i*64 + j;
@@ -179,9 +184,10 @@ __global__ void __launch_bounds__(256) k_C(T *W, T const *AU1, T const *AU2, uin
                 W[o] = wr; W[o + 4096] = wi;
                 uint32_t const idx = uint32_t(o);
                 float const tr = shadow32(seed, idx), ti = shadow32(seed, idx + 4096u);
-                n2 += double(fmaf(wr, wr, wi*wi));
-                dr += double(fmaf(tr, wr, ti*wi)); di += double(fmaf(tr, wi, -ti*wr));
+                n2f = fmaf(wr, wr, fmaf(wi, wi, n2f));
+                drf = fmaf(tr, wr, fmaf(ti, wi, drf)); dif = fmaf(tr, wi, fmaf(-ti, wr, dif));
             }
+            n2 = double(n2f); dr = double(drf); di = double(dif);
         } else
 #pragma unroll 8
         for (int i = q*16; i < q*16 + 16; ++i) {
@@ -205,16 +211,17 @@ __global__ void __launch_bounds__(256) k_C(T *W, T const *AU1, T const *AU2, uin
 // FP32 rounding, which lowers the residual floor of an FP32 sweep)
 template <typename T, typename TX>
 __global__ void __launch_bounds__(256) k_DX(TX *X, T *D, T *U1, T const *U2, T const *W, uint32_t nnzb,
-                                            uint16_t const *colindx, ColState const *cs) {
+                                            uint16_t const *colindx, ColState const *cs, float const *cf, uint32_t ncol) {
     int const j = threadIdx.x & 63, q = threadIdx.x >> 6;
     for (uint32_t b = blockIdx.x; b < nnzb; b += gridDim.x) {
-        ColState const &s = cs[colindx[b]*64 + j];
-        double const ax_r = s.cu1x_re, ax_i = s.cu1x_im, bx_r = s.cu2x_re, bx_i = s.cu2x_im, cx_r = s.cdx_re, cx_i = s.cdx_im;
-        double const ad_r = s.cu1d_re, ad_i = s.cu1d_im, cd_r = s.cdd_re, cd_i = s.cdd_im;
-        double const be_r = s.be_re, be_i = s.be_im;
+        uint32_t const col = colindx[b]*64 + j;
         if constexpr (sizeof(T) == 4 && sizeof(TX) == 4) {
-            float const a_r = ax_r, a_i = ax_i, b_r = bx_r, b_i = bx_i, c_r = cx_r, c_i = cx_i;
-            float const d_r = ad_r, d_i = ad_i, e_r = cd_r, e_i = cd_i, g_r = be_r, g_i = be_i;
+            float const g_r = cf[2*size_t(ncol) + col], g_i = cf[3*size_t(ncol) + col];
+            float const a_r = cf[4*size_t(ncol) + col], a_i = cf[5*size_t(ncol) + col];
+            float const b_r = cf[6*size_t(ncol) + col], b_i = cf[7*size_t(ncol) + col];
+            float const c_r = cf[8*size_t(ncol) + col], c_i = cf[9*size_t(ncol) + col];
+            float const d_r = cf[10*size_t(ncol) + col], d_i = cf[11*size_t(ncol) + col];
+            float const e_r = cf[12*size_t(ncol) + col], e_i = cf[13*size_t(ncol) + col];
 #pragma unroll 8
             for (int i = q*16; i < q*16 + 16; ++i) {
                 size_t const o = size_t(b)*kBlk + i*64 + j;
@@ -230,7 +237,11 @@ __global__ void __launch_bounds__(256) k_DX(TX *X, T *D, T *U1, T const *U2, T c
                 U1[o] = fmaf(g_r, u2r, fmaf(-g_i, u2i, W[o]));
                 U1[o + 4096] = fmaf(g_r, u2i, fmaf(g_i, u2r, W[o + 4096]));
             }
-        } else
+        } else {
+        ColState const &s = cs[col];
+        double const ax_r = s.cu1x_re, ax_i = s.cu1x_im, bx_r = s.cu2x_re, bx_i = s.cu2x_im, cx_r = s.cdx_re, cx_i = s.cdx_im;
+        double const ad_r = s.cu1d_re, ad_i = s.cu1d_im, cd_r = s.cdd_re, cd_i = s.cdd_im;
+        double const be_r = s.be_re, be_i = s.be_im;
 #pragma unroll 8
         for (int i = q*16; i < q*16 + 16; ++i) {
             size_t const o = size_t(b)*kBlk + i*64 + j;
@@ -245,21 +256,24 @@ __global__ void __launch_bounds__(256) k_DX(TX *X, T *D, T *U1, T const *U2, T c
             U1[o] = T(wr + (be_r*u2r - be_i*u2i));
             U1[o + 4096] = T(wi + (be_r*u2i + be_i*u2r));
         }
+        }
     }
 }
 
 // K_E: V = AU1 + beta (AU2 + beta V) ; acc rt^H V
 template <typename T>
 __global__ void __launch_bounds__(256) k_E(T *V, T const *AU1, T const *AU2, uint32_t nnzb,
-                                           uint16_t const *colindx, ColState const *cs, Acc *acc, uint32_t seed) {
+                                           uint16_t const *colindx, ColState const *cs, Acc *acc, uint32_t seed,
+                                           float const *cf, uint32_t ncol) {
     __shared__ double red[4][64][3];
     int const j = threadIdx.x & 63, q = threadIdx.x >> 6;
     for (uint32_t b = blockIdx.x; b < nnzb; b += gridDim.x) {
         uint32_t const col = colindx[b]*64 + j;
-        double const br = cs[col].be_re, bi = cs[col].be_im;
+        double const br = (sizeof(T) == 8) ? cs[col].be_re : 0.0, bi = (sizeof(T) == 8) ? cs[col].be_im : 0.0;
         double dr = 0, di = 0;
         if constexpr (sizeof(T) == 4) {
-            float const fr = float(br), fi = float(bi);
+            float const fr = cf[2*size_t(ncol) + col], fi = cf[3*size_t(ncol) + col];
+            float drf = 0.f, dif = 0.f;
 #pragma unroll 8
             for (int i = q*16; i < q*16 + 16; ++i) {
                 size_t const o = size_t(b)*kBlk + i*64 + j;
@@ -269,8 +283,9 @@ __global__ void __launch_bounds__(256) k_E(T *V, T const *AU1, T const *AU2, uin
                 V[o] = sr; V[o + 4096] = si;
                 uint32_t const idx = uint32_t(o);
                 float const tr = shadow32(seed, idx), ti = shadow32(seed, idx + 4096u);
-                dr += double(fmaf(tr, sr, ti*si)); di += double(fmaf(tr, si, -ti*sr));
+                drf = fmaf(tr, sr, fmaf(ti, si, drf)); dif = fmaf(tr, si, fmaf(-ti, sr, dif));
             }
+            dr = double(drf); di = double(dif);
         } else
 #pragma unroll 8
         for (int i = q*16; i < q*16 + 16; ++i) {
@@ -301,7 +316,17 @@ __device__ __forceinline__ void freeze(ColState &s) {
     s.cu1d_re = s.cu1d_im = s.cdd_re = s.cdd_im = 0;
 }
 
-__global__ void s_init(ColState *cs, Acc *accW, Acc *accV, uint32_t ncol, int32_t *counters) {
+// the coefficients the FP32 vector kernels use, as float columns cf[i][ncol] (coalesced loads):
+// alpha, beta, and the five complex K_DX coefficients
+constexpr int kCoef = 14;
+__device__ __forceinline__ void store_coef(float *cf, uint32_t ncol, uint32_t c, ColState const &s) {
+    double const v[kCoef] = {s.al_re, s.al_im, s.be_re, s.be_im, s.cu1x_re, s.cu1x_im, s.cu2x_re, s.cu2x_im,
+                             s.cdx_re, s.cdx_im, s.cu1d_re, s.cu1d_im, s.cdd_re, s.cdd_im};
+#pragma unroll
+    for (int i = 0; i < kCoef; ++i) cf[size_t(i)*ncol + c] = float(v[i]);
+}
+
+__global__ void s_init(ColState *cs, Acc *accW, Acc *accV, uint32_t ncol, int32_t *counters, float *cf) {
     uint32_t const c = blockIdx.x*blockDim.x + threadIdx.x;
     if (c >= ncol) return;
     ColState s{};
@@ -314,6 +339,7 @@ __global__ void s_init(ColState *cs, Acc *accW, Acc *accV, uint32_t ncol, int32_
     else if (sr*sr + si*si == 0.0 || s.rho_re*s.rho_re + s.rho_im*s.rho_im == 0.0) { s.status = 2; freeze(s); atomicAdd(&counters[1], 1); }
     else { cdiv(s.rho_re, s.rho_im, sr, si, s.al_re, s.al_im); s.status = 0; }
     cs[c] = s;
+    store_coef(cf, ncol, c, s);
     accW[c] = Acc{0, 0, 0, 0}; accV[c] = Acc{0, 0, 0, 0};
 }
 
@@ -345,13 +371,13 @@ __global__ void s_half1(ColState *cs, Acc *acc, uint32_t ncol, int m, double tol
 // rounding floor of the sweep; it is frozen like a converged one (the refinement step then
 // restarts from the true FP64 residual)
 __global__ void s_half2(ColState *cs, Acc *acc, uint32_t ncol, int m, double tol, int32_t *counters,
-                        double stall_level, int stall_window) {
+                        double stall_level, int stall_window, float *cf) {
     uint32_t const c = blockIdx.x*blockDim.x + threadIdx.x;
     if (c >= ncol) return;
     ColState s = cs[c];
     double const wn = sqrt(acc[c].n2), rnr = acc[c].re, rni = acc[c].im;
     acc[c] = Acc{0, 0, 0, 0};
-    if (0 != s.status) { freeze(s); cs[c] = s; return; }
+    if (0 != s.status) { freeze(s); cs[c] = s; store_coef(cf, ncol, c, s); return; }
     // first-half coefficients: D1 = U1 + kd1 D0 ; X1 = X0 + et1 D1
     double const k1r = s.kd1_re, k1i = s.kd1_im, e1r = s.et1_re, e1i = s.et1_im;
     if (s.conv1) {
@@ -362,6 +388,7 @@ __global__ void s_half2(ColState *cs, Acc *acc, uint32_t ncol, int m, double tol
         s.be_re = s.be_im = 0; s.al_re = s.al_im = 0;
         s.status = 1;
         cs[c] = s;
+        store_coef(cf, ncol, c, s);
         return;
     }
     double const th = wn/s.tau;
@@ -396,20 +423,22 @@ __global__ void s_half2(ColState *cs, Acc *acc, uint32_t ncol, int m, double tol
         atomicAdd(&counters[0], 1);
     }
     cs[c] = s;
+    store_coef(cf, ncol, c, s);
 }
 
 // alpha = rho / (rt^H V)
-__global__ void s_alpha(ColState *cs, Acc *acc, uint32_t ncol, int32_t *counters) {
+__global__ void s_alpha(ColState *cs, Acc *acc, uint32_t ncol, int32_t *counters, float *cf) {
     uint32_t const c = blockIdx.x*blockDim.x + threadIdx.x;
     if (c >= ncol) return;
     ColState s = cs[c];
     double const sr = acc[c].re, si = acc[c].im;
     acc[c] = Acc{0, 0, 0, 0};
     // the K_DX coefficients have been applied: finished columns keep all-zero coefficients
-    if (0 != s.status) { freeze(s); cs[c] = s; return; }
-    if (sr*sr + si*si == 0.0) { s.status = 2; freeze(s); atomicAdd(&counters[1], 1); cs[c] = s; return; }
+    if (0 != s.status) { freeze(s); cs[c] = s; store_coef(cf, ncol, c, s); return; }
+    if (sr*sr + si*si == 0.0) { s.status = 2; freeze(s); atomicAdd(&counters[1], 1); cs[c] = s; store_coef(cf, ncol, c, s); return; }
     cdiv(s.rho_re, s.rho_im, sr, si, s.al_re, s.al_im);
     cs[c] = s;
+    store_coef(cf, ncol, c, s);
 }
 
 __global__ void s_estimate(ColState const *cs, uint32_t ncol, int m, double *out) {
@@ -527,6 +556,7 @@ bool tfqmr_inner(DevicePlan &dp, SolverWorkspace &ws, TfqmrVectors &v, TX *Xs, d
     auto *cs = dptr<ColState>(ws.colstate);
     Acc *accA = (Acc*)(cs + ncol);     // two accumulator banks after the states
     auto *accB = accA + ncol;
+    float *cf = reinterpret_cast<float*>(accB + ncol);   // kCoef float columns for the FP32 kernels
     int32_t *cnt = dptr<int32_t>(ws.counters);
     unsigned const g = grid_for(nnzb), gs = (ncol + 255)/256;
     TX *X = Xs;
@@ -540,27 +570,27 @@ bool tfqmr_inner(DevicePlan &dp, SolverWorkspace &ws, TfqmrVectors &v, TX *Xs, d
     res.applications += 1;
     k_init_dots<T><<<g, 256, 0, st>>>(W, V, nnzb, ci, accA, accB, seed);
     count_launch();
-    s_init<<<gs, 256, 0, st>>>(cs, accA, accB, ncol, cnt);
+    s_init<<<gs, 256, 0, st>>>(cs, accA, accB, ncol, cnt, cf);
     count_launch();
     int it = 0;
     for (it = 1; it <= maxit; ++it) {
         bool const check = (0 == it % check_every) || (it == maxit);
         if (check) A43G_CUDA_TRY(cudaMemsetAsync(cnt, 0, sizeof(int32_t), st));
-        k_A<T><<<g, 256, 0, st>>>(U2, U1, V, W, AU1, nnzb, ci, cs, accA);
+        k_A<T><<<g, 256, 0, st>>>(U2, U1, V, W, AU1, nnzb, ci, cs, accA, cf, ncol);
         count_launch();
         s_half1<<<gs, 256, 0, st>>>(cs, accA, ncol, 2*it - 1, tol);
         count_launch();
         if (!launch_action<T>(dp, AU2, U2, ci, st)) return false;
-        k_C<T><<<g, 256, 0, st>>>(W, AU1, AU2, nnzb, ci, cs, accA, seed);
+        k_C<T><<<g, 256, 0, st>>>(W, AU1, AU2, nnzb, ci, cs, accA, seed, cf, ncol);
         count_launch();
-        s_half2<<<gs, 256, 0, st>>>(cs, accA, ncol, 2*it, tol, cnt, stall_level, kStallWindow);
+        s_half2<<<gs, 256, 0, st>>>(cs, accA, ncol, 2*it, tol, cnt, stall_level, kStallWindow, cf);
         count_launch();
-        k_DX<T, TX><<<g, 256, 0, st>>>(X, D, U1, U2, W, nnzb, ci, cs);
+        k_DX<T, TX><<<g, 256, 0, st>>>(X, D, U1, U2, W, nnzb, ci, cs, cf, ncol);
         count_launch();
         if (!launch_action<T>(dp, AU1, U1, ci, st)) return false;
-        k_E<T><<<g, 256, 0, st>>>(V, AU1, AU2, nnzb, ci, cs, accA, seed);
+        k_E<T><<<g, 256, 0, st>>>(V, AU1, AU2, nnzb, ci, cs, accA, seed, cf, ncol);
         count_launch();
-        s_alpha<<<gs, 256, 0, st>>>(cs, accA, ncol, cnt);
+        s_alpha<<<gs, 256, 0, st>>>(cs, accA, ncol, cnt, cf);
         count_launch();
         res.applications += 2;
         if (check) {
@@ -599,7 +629,7 @@ bool tfqmr_inner(DevicePlan &dp, SolverWorkspace &ws, TfqmrVectors &v, TX *Xs, d
 
 bool workspace_common(DevicePlan &dp, SolverWorkspace &ws) {
     size_t const ncol = size_t(dp.nCols)*64;
-    if (!ws.colstate.alloc(ncol*(sizeof(ColState) + 2*sizeof(Acc)))) return false;
+    if (!ws.colstate.alloc(ncol*(sizeof(ColState) + 2*sizeof(Acc) + kCoef*sizeof(float)))) return false;
     if (!ws.counters.alloc(64)) return false;
     if (!ws.colnorm.alloc((ncol + 8)*sizeof(double))) return false;
     if (!ws.host_counters) A43G_CUDA_TRY(cudaMallocHost(&ws.host_counters, 64));
@@ -678,13 +708,17 @@ int solve(GreenPlan &hp, DevicePlan &dp, SolverWorkspace &ws, a43g_solve_options
         if (!residual64(dp, ws, X64, R64, AX64, st, rmax, res.applications)) return A43G_ERR_CUDA;
         int const maxref = std::max(1, opt.max_refinements);
         double const inner_tol = (opt.inner_tolerance > 0) ? opt.inner_tolerance : 1e-4;
-        int ref = 0;
+        int ref = 0, first_sweep = 0;
         for (ref = 0; ref < maxref && rmax > opt.tolerance; ++ref) {
             k_set_from<float><<<g*8, 256, 0, st>>>(dptr<float>(v.W), dptr<float>(v.U1), dptr<float>(v.D), R64, n);
             count_launch();
             if (cudaSuccess != cudaMemsetAsync(v.X.ptr, 0, n*4, st)) { set_error("memset"); return A43G_ERR_CUDA; }
-            int const left = opt.max_iterations - res.iterations;
+            int left = opt.max_iterations - res.iterations;
             if (left < 1) break;
+            // a correction sweep that needs far more iterations than the first one has stagnated
+            // at the FP32 rounding floor: end it, recompute the true residual and restart (with a
+            // new shadow vector), which is cheaper than letting it run
+            if (ref > 0) left = std::min(left, std::max(2*first_sweep, 100));
             // relative inner tolerance, not tighter than needed for the outer target
             double const itol = std::max(inner_tol, 0.5*opt.tolerance/rmax);
             // FP32 correction sweep (keeping its solution in FP64 does not lower the FP32 residual
@@ -692,6 +726,7 @@ int solve(GreenPlan &hp, DevicePlan &dp, SolverWorkspace &ws, a43g_solve_options
             // columns stalled below 10x the sweep tolerance end the sweep (FP32 rounding floor)
             if (!tfqmr_inner<float, float>(dp, ws, v, dptr<float>(v.X), itol, left, check, seed + 7919u*uint32_t(ref + 1), st, res,
                                            opt.echo, 10*itol)) return A43G_ERR_CUDA;
+            if (0 == ref) first_sweep = res.iterations;
             k_accumulate<float><<<g*8, 256, 0, st>>>(X64, dptr<float>(v.X), n);
             count_launch();
             if (!residual64(dp, ws, X64, R64, AX64, st, rmax, res.applications)) return A43G_ERR_CUDA;
