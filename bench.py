@@ -34,7 +34,7 @@ TOLERANCE = 1e-8
 # tfQMR iterations of the plain FP64 solver at this workload, energy and tolerance (measured
 # with this code on a B200); the reference arm, which runs without a GPU, extrapolates its
 # action time to a solve with it.  The main arm uses the count of its own FP64 solve.
-FP64_ITERATIONS = 480
+FP64_ITERATIONS = 240
 METRIC = "Solves/s at 1e-8 resid (mixed+batched vs plain FP64); action % HBM peak"
 
 
