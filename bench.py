@@ -217,7 +217,8 @@ def time_part(lib_mod, plan, part, dtype_code, x, y, reps, stream):
 
 
 def read_traffic(kernel):
-    """DRAM bytes per launch of a kernel from the committed ncu summary (profiles/traffic.txt)."""
+    """DRAM bytes per block of a kernel from the committed ncu summary (profiles/traffic.txt: one
+    line per kernel, name and bytes per block, measured on a smaller case and scaled by blocks)."""
     try:
         with open(os.path.join(ROOT, "profiles", "traffic.txt")) as f:
             for line in f:
@@ -340,8 +341,8 @@ def measure_kernels(a, plan, w, stream, out, hbm, bf16, peak_kind):
     t_local = time_part(_lib, plan, 0, _lib.A43G_F32, x, y, 20, stream)
     bytes_local = 2*nnzb*8192*4 + plan.sizes["ncells"]*64*4 + nnzb*(7*4) + plan.sizes["lists_nnz2"]*4
     ach = bytes_local/t_local/1e9
-    traffic = read_traffic("local_fused_kernel_f32")
-    out["roofline"] = {"kernel": "local_fused_kernel<float> (potential + 8th-order kinetic, one pass)",
+    traffic = read_traffic("local_fused_pf_kernel_f32")
+    out["roofline"] = {"kernel": "local_fused_pf_kernel<float,16> (potential + 8th-order kinetic, one pass)",
                        "bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach/hbm,
                        "peak_kind": peak_kind, "algorithmic_bytes_per_launch": bytes_local,
                        "ms_per_launch": t_local*1e3,
