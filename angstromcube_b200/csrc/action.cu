@@ -778,12 +778,11 @@ bool launch_dyadic(DevicePlan &dp, T *y, T const *x, uint16_t const *colIndex, c
     // both FP32 projector paths stage x with 16-byte loads; other x take the generic kernels
     bool const aligned16 = 0 == (reinterpret_cast<uintptr_t>(x) & 15u);
     bool const tc = (sizeof(T) == 4) && dp.use_tc && aligned16 && tc_projector_supported(dp);
-    bool const simt32 = (sizeof(T) == 4) && !tc && simt_f32_projector_supported(dp, x) &&
-                        0 == (reinterpret_cast<uintptr_t>(y) & 15u);
+    bool const simt = !tc && simt_projector_supported(dp, x, y, sizeof(T));
     if (tc) {
         if (!launch_project_tc(dp, (float const*)x, st)) return false;
-    } else if (simt32) {
-        if (!launch_project_f32(dp, (float const*)x, st)) return false;
+    } else if (simt) {
+        if (!launch_project_simt<T>(dp, x, st)) return false;
     } else {
         // coefficients of images without any block stay zero
         A43G_CUDA_TRY(cudaMemsetAsync(dp.apc.ptr, 0, size_t(dp.ncoeffI)*dp.nCols*128*sizeof(T), st));
@@ -812,8 +811,8 @@ bool launch_dyadic(DevicePlan &dp, T *y, T const *x, uint16_t const *colIndex, c
     }
     if (tc) {
         if (!launch_add_tc(dp, (float*)y, colIndex, st)) return false;
-    } else if (simt32) {
-        if (!launch_add_f32(dp, (float*)y, colIndex, st)) return false;
+    } else if (simt && sizeof(T) == 4) {
+        if (!launch_add_simt<float>(dp, (float*)y, colIndex, st)) return false;
     } else {
         sho_add_kernel<T><<<dp.nnzb, 128, 0, st>>>(y, dptr<T>(dp.cad), dp.nCols, dp.nnzb, colIndex,
             dptr<uint32_t>(dp.add_start), dptr<uint32_t>(dp.add_col), dptr<uint32_t>(dp.add_slot),

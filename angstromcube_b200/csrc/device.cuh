@@ -114,10 +114,10 @@ bool tc_projector_supported(DevicePlan const &dp);
 bool launch_project_tc(DevicePlan &dp, float const *x, cudaStream_t st);
 bool launch_add_tc(DevicePlan &dp, float *y, uint16_t const *colIndex, cudaStream_t st);
 
-// sum-factorized FP32 projection and addition on the CUDA cores (projector_simt.cu); both
-// stage blocks with 16-byte copies and need 16-byte aligned x and y
-bool simt_f32_projector_supported(DevicePlan const &dp, void const *x);
-bool launch_project_f32(DevicePlan &dp, float const *x, cudaStream_t st);
-bool launch_add_f32(DevicePlan &dp, float *y, uint16_t const *colIndex, cudaStream_t st);
+// sum-factorized projection and addition on the CUDA cores (projector_simt.cu, FP32 and FP64);
+// both stage blocks with 16-byte copies and need 16-byte aligned x and y
+bool simt_projector_supported(DevicePlan const &dp, void const *x, void const *y, size_t real_bytes);
+template <typename T> bool launch_project_simt(DevicePlan &dp, T const *x, cudaStream_t st);
+template <typename T> bool launch_add_simt(DevicePlan &dp, T *y, uint16_t const *colIndex, cudaStream_t st);  // FP32
 
 } // namespace a43g

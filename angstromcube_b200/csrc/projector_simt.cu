@@ -1,4 +1,4 @@
-// FP32 projector contraction of the action on the CUDA cores, sum-factorized
+// Projector contraction of the action on the CUDA cores (FP32 and FP64), sum-factorized
 // (include/green_dyadic.hxx:112-288 projection, :325-518 addition).
 //
 // The projector functions are separable on the spherical mask,
@@ -38,32 +38,34 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 __device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
-// the 1D tables of one slot: T[nu][dir][i] at tab[(nu*3 + dir)*4 + i], dir 0/1/2 = x/y/z
-template <int L>
-struct Tables { float h[L + 1][3][4]; };
+// the 1D tables of one slot, H[nu][dir][i] at tab[(nu*3 + dir)*4 + i], dir 0/1/2 = x/y/z, staged in
+// shared memory: FP32 copies them into registers, FP64 (twice the registers) reads them in place
+template <typename T, int L> struct Tables;
+template <int L> struct Tables<float, L> {
+    float h[L + 1][3][4];
+    __device__ __forceinline__ void load(float const *tab) {
+#pragma unroll
+        for (int nu = 0; nu <= L; ++nu)
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                float4 const v = *reinterpret_cast<float4 const*>(tab + (nu*3 + d)*4);
+                h[nu][d][0] = v.x; h[nu][d][1] = v.y; h[nu][d][2] = v.z; h[nu][d][3] = v.w;
+            }
+    }
+    __device__ __forceinline__ float operator()(int nu, int d, int i) const { return h[nu][d][i]; }
+};
+template <int L> struct Tables<double, L> {
+    double const *p;
+    __device__ __forceinline__ void load(double const *tab) { p = tab; }
+    __device__ __forceinline__ double operator()(int nu, int d, int i) const { return p[(nu*3 + d)*4 + i]; }
+};
 
-template <int L>
-__device__ __forceinline__ void load_tables(Tables<L> &t, float const *__restrict__ tab) {
-#pragma unroll
-    for (int nu = 0; nu <= L; ++nu)
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-            float4 const v = __ldg(reinterpret_cast<float4 const*>(tab + (nu*3 + d)*4));
-            t.h[nu][d][0] = v.x; t.h[nu][d][1] = v.y; t.h[nu][d][2] = v.z; t.h[nu][d][3] = v.w;
-        }
-}
+__device__ __forceinline__ float fmat(float a, float b, float c) { return fmaf(a, b, c); }
+__device__ __forceinline__ double fmat(double a, double b, double c) { return fma(a, b, c); }
 
-// the same from a table staged in shared memory
-template <int L>
-__device__ __forceinline__ void load_tables_shared(Tables<L> &t, float const *tab) {
-#pragma unroll
-    for (int nu = 0; nu <= L; ++nu)
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-            float4 const v = *reinterpret_cast<float4 const*>(tab + (nu*3 + d)*4);
-            t.h[nu][d][0] = v.x; t.h[nu][d][1] = v.y; t.h[nu][d][2] = v.z; t.h[nu][d][3] = v.w;
-        }
-}
+// CTAs per SM the kernels are compiled for (FP64 needs twice the registers and shared memory)
+template <typename T> struct Occ { static constexpr int project = 3, add = 2; };
+template <> struct Occ<double> { static constexpr int project = 1; };   // the addition is FP32 only
 
 __device__ __forceinline__ void cp_async8(void *dst, void const *src) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" :: "r"(smem_addr(dst)), "l"(src) : "memory");
@@ -71,22 +73,23 @@ __device__ __forceinline__ void cp_async8(void *dst, void const *src) {
 
 // ---------------------------------------------------------------- projection
 
-template <int L>
-__global__ void __launch_bounds__(kThreads, 3)
-sho_project_f32_kernel(float *__restrict__ apc, float const *__restrict__ x, uint32_t nrhs,
+template <typename T, int L>
+__global__ void __launch_bounds__(kThreads, Occ<T>::project)
+sho_project_simt_kernel(T *__restrict__ apc, T const *__restrict__ x, uint32_t nrhs,
                        uint32_t const *__restrict__ items, uint32_t const *__restrict__ prj_col,
                        uint64_t const *__restrict__ prj_coloff, uint32_t const *__restrict__ prj_slot,
-                       float const *__restrict__ slot_H, uint64_t const *__restrict__ slot_mask, int stride,
+                       T const *__restrict__ slot_H, uint64_t const *__restrict__ slot_mask, int stride,
                        uint32_t const *__restrict__ img_starts)
 {
     constexpr int NS = nsho_of(L), N2 = n2_of(L);
-    extern __shared__ __align__(16) float xs[];       // [2][kBlk]
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T *xs = reinterpret_cast<T*>(smem_raw);           // [2][kBlk]
     uint32_t const *item = items + 4*size_t(blockIdx.x);
     uint32_t const a = item[0], s = item[1], k0 = item[2], k1 = item[3];
     int const tid = threadIdx.x, reim = tid >> 6, j = tid & 63;
     uint64_t const off = prj_coloff[s];
 
-    __shared__ __align__(16) float tbuf[2][(L + 1)*12];   // 1D tables of the staged blocks' slots
+    __shared__ __align__(16) T tbuf[2][(L + 1)*12];       // 1D tables of the staged blocks' slots
     __shared__ uint64_t mbuf[2];                           // and their masks
     // block, table and mask of list position k go to shared memory ahead of use; the block and
     // slot indices are loaded one position earlier still
@@ -94,17 +97,18 @@ sho_project_f32_kernel(float *__restrict__ apc, float const *__restrict__ x, uin
         char const *src = reinterpret_cast<char const*>(x + size_t(b)*kBlk);
         char *dst = reinterpret_cast<char*>(xs + buf*kBlk);
 #pragma unroll
-        for (int r = 0; r < kBlk*4/(16*kThreads); ++r) {
+        for (int r = 0; r < kBlk*int(sizeof(T))/(16*kThreads); ++r) {
             int const o = (r*kThreads + tid)*16;
             cp_async16(dst + o, src + o);
         }
-        if (tid < (L + 1)*3) cp_async16(&tbuf[buf][tid*4], slot_H + size_t(slot)*stride + tid*4);
+        constexpr int TE = 16/int(sizeof(T));          // table elements per 16-byte copy
+        if (tid < (L + 1)*12/TE) cp_async16(&tbuf[buf][tid*TE], slot_H + size_t(slot)*stride + tid*TE);
         if (tid == kThreads - 1) cp_async8(&mbuf[buf], slot_mask + slot);
     };
 
-    float acc[NS];
+    T acc[NS];
 #pragma unroll
-    for (int i = 0; i < NS; ++i) acc[i] = 0.f;
+    for (int i = 0; i < NS; ++i) acc[i] = T(0);
 
     stage(prj_col[off + k0], prj_slot[off + k0], 0);
     cp_async_commit();
@@ -117,49 +121,49 @@ sho_project_f32_kernel(float *__restrict__ apc, float const *__restrict__ x, uin
         if (k + 2 < k1) { nb = prj_col[off + k + 2]; ns = prj_slot[off + k + 2]; }   // for the next iteration
         cp_async_wait1();                            // block k has landed (this thread's copies)
         __syncthreads();                             // ... and everybody else's
-        Tables<L> t;
-        load_tables_shared<L>(t, tbuf[buf]);
+        Tables<T, L> t;
+        t.load(tbuf[buf]);
         uint64_t const mask = mbuf[buf];
-        float const *xb = xs + buf*kBlk + reim*4096 + j;
+        T const *xb = xs + buf*kBlk + reim*4096 + j;
 #pragma unroll
         for (int z = 0; z < 4; ++z) {
             if (0 == ((mask >> (16*z)) & 0xffffu)) continue;     // uniform: plane outside the sphere
-            float byx[N2];
+            T byx[N2];
 #pragma unroll
-            for (int i = 0; i < N2; ++i) byx[i] = 0.f;
+            for (int i = 0; i < N2; ++i) byx[i] = T(0);
 #pragma unroll
             for (int yy = 0; yy < 4; ++yy) {
-                float ax[L + 1];
+                T ax[L + 1];
 #pragma unroll
-                for (int i = 0; i <= L; ++i) ax[i] = 0.f;
+                for (int i = 0; i <= L; ++i) ax[i] = T(0);
 #pragma unroll
                 for (int xx = 0; xx < 4; ++xx) {
                     int const p = (z*4 + yy)*4 + xx;
-                    float const v = ((mask >> p) & 1u) ? xb[p*64] : 0.f;
+                    T const v = ((mask >> p) & 1u) ? xb[p*64] : T(0);
 #pragma unroll
-                    for (int ix = 0; ix <= L; ++ix) ax[ix] = fmaf(v, t.h[ix][0][xx], ax[ix]);
+                    for (int ix = 0; ix <= L; ++ix) ax[ix] = fmat(v, t(ix, 0, xx), ax[ix]);
                 }
 #pragma unroll
                 for (int iy = 0, iyx = 0; iy <= L; ++iy) {
-                    float const hy = t.h[iy][1][yy];
+                    T const hy = t(iy, 1, yy);
 #pragma unroll
-                    for (int ix = 0; ix <= L - iy; ++ix, ++iyx) byx[iyx] = fmaf(ax[ix], hy, byx[iyx]);
+                    for (int ix = 0; ix <= L - iy; ++ix, ++iyx) byx[iyx] = fmat(ax[ix], hy, byx[iyx]);
                 }
             }
 #pragma unroll
             for (int iz = 0, sho = 0; iz <= L; ++iz) {
-                float const hz = t.h[iz][2][z];
+                T const hz = t(iz, 2, z);
 #pragma unroll
                 for (int iy = 0; iy <= L - iz; ++iy) {
                     int const iyx = iy*(2*L + 3 - iy)/2;
 #pragma unroll
-                    for (int ix = 0; ix <= L - iz - iy; ++ix, ++sho) acc[sho] = fmaf(byx[iyx + ix], hz, acc[sho]);
+                    for (int ix = 0; ix <= L - iz - iy; ++ix, ++sho) acc[sho] = fmat(byx[iyx + ix], hz, acc[sho]);
                 }
             }
         }
         __syncthreads();                             // buffer buf is free for block k + 2
     }
-    float *out = apc + (size_t(img_starts[a])*nrhs + s)*128 + reim*64 + j;
+    T *out = apc + (size_t(img_starts[a])*nrhs + s)*128 + reim*64 + j;
 #pragma unroll
     for (int sho = 0; sho < NS; ++sho) atomicAdd(out + size_t(sho)*nrhs*128, acc[sho]);
 }
@@ -167,50 +171,50 @@ sho_project_f32_kernel(float *__restrict__ apc, float const *__restrict__ x, uin
 // ---------------------------------------------------------------- addition
 
 // contribution of one image with basis size L to the 64 point sums of this thread
-template <int L, bool FULL>
-__device__ __forceinline__ void add_image(float (&acc)[64], Tables<L> const &t, uint64_t mask,
-                                          float const *__restrict__ c, size_t cstride) {
+template <typename T, int L, bool FULL>
+__device__ __forceinline__ void add_image(T (&acc)[64], Tables<T, L> const &t, uint64_t mask,
+                                          T const *__restrict__ c, size_t cstride) {
 #pragma unroll
     for (int iz = 0, sho = 0; iz <= L; ++iz) {
-        float byx[16];
+        T byx[16];
 #pragma unroll
-        for (int i = 0; i < 16; ++i) byx[i] = 0.f;
+        for (int i = 0; i < 16; ++i) byx[i] = T(0);
 #pragma unroll
         for (int iy = 0; iy <= L - iz; ++iy) {
-            float ax[4] = {0.f, 0.f, 0.f, 0.f};
+            T ax[4] = {T(0), T(0), T(0), T(0)};
 #pragma unroll
             for (int ix = 0; ix <= L - iz - iy; ++ix, ++sho) {
-                float const cv = c[size_t(sho)*cstride];
+                T const cv = c[size_t(sho)*cstride];
 #pragma unroll
-                for (int xx = 0; xx < 4; ++xx) ax[xx] = fmaf(t.h[ix][0][xx], cv, ax[xx]);
+                for (int xx = 0; xx < 4; ++xx) ax[xx] = fmat(t(ix, 0, xx), cv, ax[xx]);
             }
 #pragma unroll
             for (int yy = 0; yy < 4; ++yy) {
-                float const hy = t.h[iy][1][yy];
+                T const hy = t(iy, 1, yy);
 #pragma unroll
-                for (int xx = 0; xx < 4; ++xx) byx[yy*4 + xx] = fmaf(hy, ax[xx], byx[yy*4 + xx]);
+                for (int xx = 0; xx < 4; ++xx) byx[yy*4 + xx] = fmat(hy, ax[xx], byx[yy*4 + xx]);
             }
         }
 #pragma unroll
         for (int z = 0; z < 4; ++z) {
-            float const hz = t.h[iz][2][z];
+            T const hz = t(iz, 2, z);
 #pragma unroll
             for (int q = 0; q < 16; ++q) {
                 int const p = z*16 + q;
-                if (FULL) acc[p] = fmaf(hz, byx[q], acc[p]);
-                else acc[p] = ((mask >> p) & 1u) ? fmaf(hz, byx[q], acc[p]) : acc[p];
+                if (FULL) acc[p] = fmat(hz, byx[q], acc[p]);
+                else acc[p] = ((mask >> p) & 1u) ? fmat(hz, byx[q], acc[p]) : acc[p];
             }
         }
     }
 }
 
-template <int L>
-__device__ __forceinline__ void add_image_L(float (&acc)[64], float const *__restrict__ tab, uint64_t mask,
-                                            float const *__restrict__ c, size_t cstride) {
-    Tables<L> t;
-    load_tables_shared<L>(t, tab);
-    if (~0ull == mask) add_image<L, true>(acc, t, mask, c, cstride);
-    else add_image<L, false>(acc, t, mask, c, cstride);
+template <typename T, int L>
+__device__ __forceinline__ void add_image_L(T (&acc)[64], T const *__restrict__ tab, uint64_t mask,
+                                            T const *__restrict__ c, size_t cstride) {
+    Tables<T, L> t;
+    t.load(tab);
+    if (~0ull == mask) add_image<T, L, true>(acc, t, mask, c, cstride);
+    else add_image<T, L, false>(acc, t, mask, c, cstride);
 }
 
 // LMAX: largest basis size of the plan (the instantiation has no larger one).  One CTA walks the
@@ -218,18 +222,19 @@ __device__ __forceinline__ void add_image_L(float (&acc)[64], float const *__res
 // stream: the coefficients, table and mask of the next pair are staged while the current pair is
 // applied, and the y values of the next block with atoms are staged during the whole of the
 // current block, so neither the start of a block nor its final y update waits for memory.
-template <int LMAX>
-__global__ void __launch_bounds__(kThreads, 2)
-sho_add_f32_kernel(float *__restrict__ y, float const *__restrict__ cad, uint32_t nrhs, uint32_t nnzb,
-                   uint32_t blocks_per_cta, uint16_t const *__restrict__ colIndex,
-                   uint32_t const *__restrict__ add_start, uint4 const *__restrict__ info,
-                   float const *__restrict__ slot_H, uint64_t const *__restrict__ slot_mask, int stride)
+template <typename T, int LMAX>
+__global__ void __launch_bounds__(kThreads, Occ<T>::add)
+sho_add_simt_kernel(T *__restrict__ y, T const *__restrict__ cad, uint32_t nrhs, uint32_t nnzb,
+                    uint32_t blocks_per_cta, uint16_t const *__restrict__ colIndex,
+                    uint32_t const *__restrict__ add_start, uint4 const *__restrict__ info,
+                    T const *__restrict__ slot_H, uint64_t const *__restrict__ slot_mask, int stride)
 {
     constexpr int NCMAX = nsho_of(LMAX);
-    extern __shared__ __align__(16) float smem_f[];
-    float *cbuf = smem_f;                                  // [2][NCMAX][128] coefficients of two pairs
-    float *ybuf = smem_f + 2*NCMAX*128;                    // [8192] y of the current block
-    __shared__ __align__(16) float tbuf[2][(LMAX + 1)*12];
+    constexpr int TE = 16/int(sizeof(T));                  // elements per 16-byte copy
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T *cbuf = reinterpret_cast<T*>(smem_raw);              // [2][NCMAX][128] coefficients of two pairs
+    T *ybuf = cbuf + 2*NCMAX*128;                          // [8192] y of the current block
+    __shared__ __align__(16) T tbuf[2][(LMAX + 1)*12];
     __shared__ uint64_t mbuf[2];
     uint32_t const b0 = blockIdx.x*blocks_per_cta, b1 = min(b0 + blocks_per_cta, nnzb);
     if (b0 >= b1) return;
@@ -246,20 +251,21 @@ sho_add_f32_kernel(float *__restrict__ y, float const *__restrict__ cad, uint32_
 
     auto stage_pair = [&](uint4 const inf, uint32_t src_col, int buf) {
         int const L = int(inf.z), nc = nsho_of(L);
-        float const *src = cad + (size_t(inf.y)*nrhs + src_col)*128;
-        float *dst = cbuf + buf*NCMAX*128;
-        for (int q = tid; q < nc*32; q += kThreads) {
-            int const row = q >> 5, part = (q & 31)*4;
+        T const *src = cad + (size_t(inf.y)*nrhs + src_col)*128;
+        T *dst = cbuf + buf*NCMAX*128;
+        constexpr int CPR = 128/TE;                        // 16-byte copies per coefficient row
+        for (int q = tid; q < nc*CPR; q += kThreads) {
+            int const row = q/CPR, part = (q % CPR)*TE;
             cp_async16(dst + row*128 + part, src + size_t(row)*cstride + part);
         }
-        if (tid < (L + 1)*3) cp_async16(&tbuf[buf][tid*4], slot_H + size_t(inf.x)*stride + tid*4);
+        if (tid < (L + 1)*12/TE) cp_async16(&tbuf[buf][tid*TE], slot_H + size_t(inf.x)*stride + tid*TE);
         if (tid == kThreads - 1) cp_async8(&mbuf[buf], slot_mask + inf.x);
     };
     auto stage_y = [&](uint32_t blk) {
-        float const *src = y + size_t(blk)*kBlk;
+        T const *src = y + size_t(blk)*kBlk;
 #pragma unroll
-        for (int r = 0; r < kBlk/(4*kThreads); ++r) {
-            int const o = (r*kThreads + tid)*4;
+        for (int r = 0; r < kBlk/(TE*kThreads); ++r) {
+            int const o = (r*kThreads + tid)*TE;
             cp_async16(ybuf + o, src + o);
         }
     };
@@ -270,9 +276,9 @@ sho_add_f32_kernel(float *__restrict__ y, float const *__restrict__ cad, uint32_
         return colIndex[c];
     };
 
-    float acc[64];
+    T acc[64];
 #pragma unroll
-    for (int i = 0; i < 64; ++i) acc[i] = 0.f;
+    for (int i = 0; i < 64; ++i) acc[i] = T(0);
     uint64_t mask_all = 0;
     uint4 const zero4 = make_uint4(0u, 0u, 0u, 0u);
     uint4 cur = info[T0];
@@ -290,29 +296,29 @@ sho_add_f32_kernel(float *__restrict__ y, float const *__restrict__ cad, uint32_
         uint64_t const mask = mbuf[buf];
         if (mask) {
             mask_all |= mask;
-            float const *tab = tbuf[buf];
-            float const *c = cbuf + buf*NCMAX*128 + reim*64 + j;
+            T const *tab = tbuf[buf];
+            T const *c = cbuf + buf*NCMAX*128 + reim*64 + j;
             int const L = int(cur.z);                      // uniform over the CTA
-            if (L == LMAX) add_image_L<LMAX>(acc, tab, mask, c, 128);
-            else if (LMAX > 0 && L == 0) add_image_L<0>(acc, tab, mask, c, 128);
-            else if (LMAX > 1 && L == 1) add_image_L<(LMAX > 1 ? 1 : 0)>(acc, tab, mask, c, 128);
-            else if (LMAX > 2 && L == 2) add_image_L<(LMAX > 2 ? 2 : 0)>(acc, tab, mask, c, 128);
-            else if (LMAX > 3 && L == 3) add_image_L<(LMAX > 3 ? 3 : 0)>(acc, tab, mask, c, 128);
-            else if (LMAX > 4 && L == 4) add_image_L<(LMAX > 4 ? 4 : 0)>(acc, tab, mask, c, 128);
-            else if (LMAX > 5 && L == 5) add_image_L<(LMAX > 5 ? 5 : 0)>(acc, tab, mask, c, 128);
-            else if (LMAX > 6 && L == 6) add_image_L<(LMAX > 6 ? 6 : 0)>(acc, tab, mask, c, 128);
+            if (L == LMAX) add_image_L<T, LMAX>(acc, tab, mask, c, 128);
+            else if (LMAX > 0 && L == 0) add_image_L<T, 0>(acc, tab, mask, c, 128);
+            else if (LMAX > 1 && L == 1) add_image_L<T, (LMAX > 1 ? 1 : 0)>(acc, tab, mask, c, 128);
+            else if (LMAX > 2 && L == 2) add_image_L<T, (LMAX > 2 ? 2 : 0)>(acc, tab, mask, c, 128);
+            else if (LMAX > 3 && L == 3) add_image_L<T, (LMAX > 3 ? 3 : 0)>(acc, tab, mask, c, 128);
+            else if (LMAX > 4 && L == 4) add_image_L<T, (LMAX > 4 ? 4 : 0)>(acc, tab, mask, c, 128);
+            else if (LMAX > 5 && L == 5) add_image_L<T, (LMAX > 5 ? 5 : 0)>(acc, tab, mask, c, 128);
+            else if (LMAX > 6 && L == 6) add_image_L<T, (LMAX > 6 ? 6 : 0)>(acc, tab, mask, c, 128);
         }
         cur = nxt; nxt = after;
         if (t + 1 == bend) {
             // last pair of block bb: y[bb] = staged y + sums on the points inside the spheres
             cp_async_wait0();
             __syncthreads();
-            float const *yb_s = ybuf + reim*4096 + j;
-            float *yb = y + size_t(bb)*kBlk + reim*4096 + j;
+            T const *yb_s = ybuf + reim*4096 + j;
+            T *yb = y + size_t(bb)*kBlk + reim*4096 + j;
 #pragma unroll
             for (int p = 0; p < 64; ++p) {
                 if ((mask_all >> p) & 1u) yb[p*64] = yb_s[p*64] + acc[p];
-                acc[p] = 0.f;
+                acc[p] = T(0);
             }
             mask_all = 0;
             __syncthreads();                               // ybuf free
@@ -328,61 +334,82 @@ sho_add_f32_kernel(float *__restrict__ y, float const *__restrict__ cad, uint32_
     }
 }
 
-template <int L>
-void launch_project_f32_L(DevicePlan &dp, float const *x, cudaStream_t st) {
+template <typename T> T const *simt_table(DevicePlan const &dp);
+template <> float const *simt_table<float>(DevicePlan const &dp) { return dptr<float>(dp.slot_H32); }
+template <> double const *simt_table<double>(DevicePlan const &dp) { return dptr<double>(dp.slot_H); }
+
+template <typename T, int L>
+void launch_project_L(DevicePlan &dp, T const *x, cudaStream_t st) {
     auto const &g = dp.prj_items[L];
     if (0 == g.count) return;
-    constexpr int smem = 2*kBlk*int(sizeof(float));
-    // 64 KB of dynamic shared memory (a per-device attribute, so set on every launch)
-    cudaFuncSetAttribute(sho_project_f32_kernel<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    sho_project_f32_kernel<L><<<g.count, kThreads, smem, st>>>(
-        dptr<float>(dp.apc), x, dp.nCols, dptr<uint32_t>(g.items), dptr<uint32_t>(dp.prj_col),
-        dptr<uint64_t>(dp.prj_coloff), dptr<uint32_t>(dp.prj_slot), dptr<float>(dp.slot_H32),
+    constexpr int smem = 2*kBlk*int(sizeof(T));
+    // double-buffered block stage (a per-device attribute, so set on every launch)
+    cudaFuncSetAttribute(sho_project_simt_kernel<T, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    sho_project_simt_kernel<T, L><<<g.count, kThreads, smem, st>>>(
+        dptr<T>(dp.apc), x, dp.nCols, dptr<uint32_t>(g.items), dptr<uint32_t>(dp.prj_col),
+        dptr<uint64_t>(dp.prj_coloff), dptr<uint32_t>(dp.prj_slot), simt_table<T>(dp),
         dptr<uint64_t>(dp.slot_mask), dp.table_stride, dptr<uint32_t>(dp.img_starts));
     count_launch();
 }
 
-} // namespace
-
-bool simt_f32_projector_supported(DevicePlan const &dp, void const *x) {
-    return dp.slot_H32.ptr && dp.lmax_max <= 7 && 0 == (reinterpret_cast<uintptr_t>(x) & 15u);
+template <typename T, int LMAX>
+void launch_add_L(DevicePlan &dp, T *y, uint16_t const *colIndex, cudaStream_t st) {
+    constexpr int smem = (2*nsho_of(LMAX)*128 + kBlk)*int(sizeof(T));
+    constexpr uint32_t kBlocksPerCta = 16;
+    cudaFuncSetAttribute(sho_add_simt_kernel<T, LMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    unsigned const grid = (dp.nnzb + kBlocksPerCta - 1)/kBlocksPerCta;
+    sho_add_simt_kernel<T, LMAX><<<grid, kThreads, smem, st>>>(y, dptr<T>(dp.cad), dp.nCols, dp.nnzb, kBlocksPerCta,
+        colIndex, dptr<uint32_t>(dp.add_start), dptr<uint4>(dp.add_info), simt_table<T>(dp),
+        dptr<uint64_t>(dp.slot_mask), dp.table_stride);
 }
 
-bool launch_project_f32(DevicePlan &dp, float const *x, cudaStream_t st) {
-    A43G_CUDA_TRY(cudaMemsetAsync(dp.apc.ptr, 0, size_t(dp.ncoeffI)*dp.nCols*128*sizeof(float), st));
-    launch_project_f32_L<0>(dp, x, st); launch_project_f32_L<1>(dp, x, st);
-    launch_project_f32_L<2>(dp, x, st); launch_project_f32_L<3>(dp, x, st);
-    launch_project_f32_L<4>(dp, x, st); launch_project_f32_L<5>(dp, x, st);
-    launch_project_f32_L<6>(dp, x, st); launch_project_f32_L<7>(dp, x, st);
+} // namespace
+
+bool simt_projector_supported(DevicePlan const &dp, void const *x, void const *y, size_t real_bytes) {
+    // 16-byte staging copies; the FP64 addition stages up to numax 5 (shared memory)
+    int const lmax_limit = (8 == real_bytes) ? 5 : 7;
+    return dp.slot_H32.ptr && dp.lmax_max <= lmax_limit && 0 == (reinterpret_cast<uintptr_t>(x) & 15u) &&
+           0 == (reinterpret_cast<uintptr_t>(y) & 15u);
+}
+
+template <typename T>
+bool launch_project_simt(DevicePlan &dp, T const *x, cudaStream_t st) {
+    A43G_CUDA_TRY(cudaMemsetAsync(dp.apc.ptr, 0, size_t(dp.ncoeffI)*dp.nCols*128*sizeof(T), st));
+    launch_project_L<T, 0>(dp, x, st); launch_project_L<T, 1>(dp, x, st);
+    launch_project_L<T, 2>(dp, x, st); launch_project_L<T, 3>(dp, x, st);
+    launch_project_L<T, 4>(dp, x, st); launch_project_L<T, 5>(dp, x, st);
+    if constexpr (sizeof(T) == 4) {
+        launch_project_L<T, 6>(dp, x, st); launch_project_L<T, 7>(dp, x, st);
+    }
     A43G_CUDA_TRY(cudaGetLastError());
     return true;
 }
 
-template <int LMAX>
-void launch_add_f32_L(DevicePlan &dp, float *y, uint16_t const *colIndex, cudaStream_t st) {
-    constexpr int smem = (2*nsho_of(LMAX)*128 + kBlk)*int(sizeof(float));
-    constexpr uint32_t kBlocksPerCta = 16;
-    cudaFuncSetAttribute(sho_add_f32_kernel<LMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    unsigned const grid = (dp.nnzb + kBlocksPerCta - 1)/kBlocksPerCta;
-    sho_add_f32_kernel<LMAX><<<grid, kThreads, smem, st>>>(y, dptr<float>(dp.cad), dp.nCols, dp.nnzb, kBlocksPerCta,
-        colIndex, dptr<uint32_t>(dp.add_start), dptr<uint4>(dp.add_info), dptr<float>(dp.slot_H32),
-        dptr<uint64_t>(dp.slot_mask), dp.table_stride);
-}
-
-bool launch_add_f32(DevicePlan &dp, float *y, uint16_t const *colIndex, cudaStream_t st) {
+// (FP32 only: in FP64 the 64 point sums per thread do not fit the registers; the FP64 action
+// keeps the generic addition kernel)
+template <typename T>
+bool launch_add_simt(DevicePlan &dp, T *y, uint16_t const *colIndex, cudaStream_t st) {
     switch (dp.lmax_max) {
-        case 0: launch_add_f32_L<0>(dp, y, colIndex, st); break;
-        case 1: launch_add_f32_L<1>(dp, y, colIndex, st); break;
-        case 2: launch_add_f32_L<2>(dp, y, colIndex, st); break;
-        case 3: launch_add_f32_L<3>(dp, y, colIndex, st); break;
-        case 4: launch_add_f32_L<4>(dp, y, colIndex, st); break;
-        case 5: launch_add_f32_L<5>(dp, y, colIndex, st); break;
-        case 6: launch_add_f32_L<6>(dp, y, colIndex, st); break;
-        default: launch_add_f32_L<7>(dp, y, colIndex, st); break;
+        case 0: launch_add_L<T, 0>(dp, y, colIndex, st); break;
+        case 1: launch_add_L<T, 1>(dp, y, colIndex, st); break;
+        case 2: launch_add_L<T, 2>(dp, y, colIndex, st); break;
+        case 3: launch_add_L<T, 3>(dp, y, colIndex, st); break;
+        case 4: launch_add_L<T, 4>(dp, y, colIndex, st); break;
+        case 5: launch_add_L<T, 5>(dp, y, colIndex, st); break;
+        default:
+            if constexpr (sizeof(T) == 4) {
+                if (6 == dp.lmax_max) launch_add_L<T, 6>(dp, y, colIndex, st);
+                else launch_add_L<T, 7>(dp, y, colIndex, st);
+            }
+            break;
     }
     count_launch();
     A43G_CUDA_TRY(cudaGetLastError());
     return true;
 }
+
+template bool launch_project_simt<float>(DevicePlan &, float const *, cudaStream_t);
+template bool launch_project_simt<double>(DevicePlan &, double const *, cudaStream_t);
+template bool launch_add_simt<float>(DevicePlan &, float *, uint16_t const *, cudaStream_t);
 
 } // namespace a43g

@@ -157,3 +157,44 @@ def test_vjp_solve_gradient_vs_finite_differences():
         J.append(_functional(_solve(product_plan(g2, Vc, mats, offs, E, k, dVol))[1], W, w))
     fd = (J[0] - J[1]) / 2e-4
     assert abs(fd - gR[2]) <= 1e-6 * max(abs(gR[2]), 1e-3 * np.abs(gR).max()), (fd, gR)
+
+
+def test_vjp_potential_matches_reference_cpu_solves():
+    """dJ/dV assembled on the CPU from solves with the reference's own action (oracle/_ref, its
+    CPU build, driven by the numpy tfQMR restatement) agrees with the GPU adjoint gradient."""
+    import oracle
+    from oracle import tfqmr
+    from helpers import reference_plan
+    if not oracle.ref_available():
+        pytest.skip("oracle/_ref not built")
+    g = geometry((4, 4, 4), (1, 1, 1), 3.0, (1, 1, 1), 4, 2, seed=11, sigma=0.5, numax=3)
+    Vc, mats, offs, E, k, dVol, na = inputs_for(g, seed=21)
+    E = complex(-0.3, 0.5)                            # broad enough for short CPU solves
+    rng = np.random.default_rng(13)
+    W = rng.uniform(0.5, 1.5, size=64)
+    w = complex(0.3, -0.2)
+    # reference CPU solves at E and at conj(E)
+    sol = []
+    for e in (E, E.conjugate()):
+        r = reference_plan(g, Vc, mats, offs, e, k, dVol)
+        ex = r.export()
+        X, info = tfqmr.solve_blocks(r.action, ex["subset"], ex["colindx"], r.sizes["nnzb"], r.sizes["nCols"],
+                                     tol=1e-11, maxiter=1500)
+        assert info["converged"], info
+        sol.append(X[:, 0] + 1j * X[:, 1])
+        veff = ex["veff_index"]
+    Gc, Gac = sol
+    Lam = np.conj(Gac) * W[None, None, :]
+    dV_cpu = np.zeros((len(Vc), 64), complex)
+    prod = (Lam * Gc).sum(axis=2)                     # [nnzb, 64 points]
+    for b, cell in enumerate(veff):
+        if cell >= 0:
+            dV_cpu[cell] += prod[b]
+    gV_cpu = np.imag(-w * dV_cpu)
+    # the same on the GPU: solves, adjoint, vector-Jacobian product
+    p = product_plan(g, Vc, mats, offs, E, k, dVol)
+    G, _ = _solve(p)
+    Ga, _ = _solve(product_plan(g, Vc, mats, offs, E.conjugate(), k, dVol))
+    Lt = torch.stack([Ga[:, 0], -Ga[:, 1]], dim=1) * torch.from_numpy(W).cuda()
+    gV_gpu = np.imag(-w * green_action.vjp(p, Lt, G, matrices=False, positions=False)["V"])
+    assert np.abs(gV_gpu - gV_cpu).max() <= 1e-7 * np.abs(gV_cpu).max()
