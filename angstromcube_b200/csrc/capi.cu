@@ -28,6 +28,8 @@ std::atomic<uint64_t> g_launches{0};
 }
 void set_error(std::string const &msg) { g_error = msg; }
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+void count_launches(uint64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+uint64_t launches_so_far() { return g_launches.load(std::memory_order_relaxed); }
 } // namespace a43g
 
 using a43g::set_error;

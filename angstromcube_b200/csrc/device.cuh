@@ -79,6 +79,12 @@ struct DevicePlan {
 };
 
 bool upload_plan(GreenPlan const &hp, DevicePlan &dp);
+// kernel attributes (dynamic shared memory above 48 KB) of the current device
+bool prepare_simt_kernels();
+bool prepare_tc_kernels();
+// kernel launch counter: n launches at once (replays of a captured graph)
+void count_launches(uint64_t n);
+uint64_t launches_so_far();
 bool upload_values(GreenPlan const &hp, DevicePlan &dp);
 bool ensure_dyadic_scratch(DevicePlan &dp, size_t elem_bytes);
 

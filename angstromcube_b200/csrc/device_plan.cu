@@ -67,6 +67,7 @@ std::vector<int32_t> neighbour_table(GreenPlan const &hp) {
 } // namespace
 
 bool upload_plan(GreenPlan const &hp, DevicePlan &dp) {
+    if (!prepare_simt_kernels() || !prepare_tc_kernels()) return false;
     dp.nnzb = uint32_t(hp.nnzb()); dp.nRows = hp.nRows; dp.nCols = hp.nCols;
     dp.nAtoms = hp.nAtoms; dp.nAI = hp.nAtomImages;
     dp.ncoeffI = uint32_t(hp.ncoeff_images()); dp.ncoeffA = uint32_t(hp.ncoeff_atoms());

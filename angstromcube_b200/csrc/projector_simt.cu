@@ -342,9 +342,7 @@ template <typename T, int L>
 void launch_project_L(DevicePlan &dp, T const *x, cudaStream_t st) {
     auto const &g = dp.prj_items[L];
     if (0 == g.count) return;
-    constexpr int smem = 2*kBlk*int(sizeof(T));
-    // double-buffered block stage (a per-device attribute, so set on every launch)
-    cudaFuncSetAttribute(sho_project_simt_kernel<T, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    constexpr int smem = 2*kBlk*int(sizeof(T));         // double-buffered block stage
     sho_project_simt_kernel<T, L><<<g.count, kThreads, smem, st>>>(
         dptr<T>(dp.apc), x, dp.nCols, dptr<uint32_t>(g.items), dptr<uint32_t>(dp.prj_col),
         dptr<uint64_t>(dp.prj_coloff), dptr<uint32_t>(dp.prj_slot), simt_table<T>(dp),
@@ -356,14 +354,34 @@ template <typename T, int LMAX>
 void launch_add_L(DevicePlan &dp, T *y, uint16_t const *colIndex, cudaStream_t st) {
     constexpr int smem = (2*nsho_of(LMAX)*128 + kBlk)*int(sizeof(T));
     constexpr uint32_t kBlocksPerCta = 16;
-    cudaFuncSetAttribute(sho_add_simt_kernel<T, LMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     unsigned const grid = (dp.nnzb + kBlocksPerCta - 1)/kBlocksPerCta;
     sho_add_simt_kernel<T, LMAX><<<grid, kThreads, smem, st>>>(y, dptr<T>(dp.cad), dp.nCols, dp.nnzb, kBlocksPerCta,
         colIndex, dptr<uint32_t>(dp.add_start), dptr<uint4>(dp.add_info), simt_table<T>(dp),
         dptr<uint64_t>(dp.slot_mask), dp.table_stride);
 }
 
+template <typename T, int L>
+void set_smem_attributes() {
+    cudaFuncSetAttribute(sho_project_simt_kernel<T, L>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         2*kBlk*int(sizeof(T)));
+    if constexpr (sizeof(T) == 4)
+        cudaFuncSetAttribute(sho_add_simt_kernel<T, L>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (2*nsho_of(L)*128 + kBlk)*int(sizeof(T)));
+}
+
 } // namespace
+
+bool prepare_simt_kernels() {
+    // the dynamic shared memory the kernels need beyond 48 KB (per device: called with the
+    // device current, before any launch and outside stream capture)
+    set_smem_attributes<float, 0>(); set_smem_attributes<float, 1>(); set_smem_attributes<float, 2>();
+    set_smem_attributes<float, 3>(); set_smem_attributes<float, 4>(); set_smem_attributes<float, 5>();
+    set_smem_attributes<float, 6>(); set_smem_attributes<float, 7>();
+    set_smem_attributes<double, 0>(); set_smem_attributes<double, 1>(); set_smem_attributes<double, 2>();
+    set_smem_attributes<double, 3>(); set_smem_attributes<double, 4>(); set_smem_attributes<double, 5>();
+    A43G_CUDA_TRY(cudaGetLastError());
+    return true;
+}
 
 bool simt_projector_supported(DevicePlan const &dp, void const *x, void const *y, size_t real_bytes) {
     // 16-byte staging copies; the FP64 addition stages up to numax 5 (shared memory)

@@ -302,13 +302,13 @@ sho_add_tc_kernel(float *__restrict__ y, float const *__restrict__ cad, uint32_t
 
 bool tc_projector_supported(DevicePlan const &dp) { return dp.lmax_max >= 0 && dp.lmax_max <= 5; }
 
+bool prepare_tc_kernels() {
+    A43G_CUDA_TRY(cudaFuncSetAttribute(sho_project_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmem));
+    A43G_CUDA_TRY(cudaFuncSetAttribute(sho_add_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmem));
+    return true;
+}
+
 bool launch_project_tc(DevicePlan &dp, float const *x, cudaStream_t st) {
-    static bool attr = false;
-    if (!attr) {
-        A43G_CUDA_TRY(cudaFuncSetAttribute(sho_project_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmem));
-        A43G_CUDA_TRY(cudaFuncSetAttribute(sho_add_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmem));
-        attr = true;
-    }
     for (int L = 0; L < 8; ++L) {
         auto const &g = dp.img_group[L];
         if (0 == g.count) continue;

@@ -17,6 +17,7 @@
 #include "solver.hpp"
 
 #include <algorithm>
+#include <cstdlib>
 #include <cmath>
 #include <cstdio>
 #include <vector>
@@ -344,9 +345,12 @@ __global__ void s_init(ColState *cs, Acc *accW, Acc *accV, uint32_t ncol, int32_
 }
 
 // first half step m = 2n-1
-__global__ void s_half1(ColState *cs, Acc *acc, uint32_t ncol, int m, double tol) {
+// the iteration number n (1-based) is counters[2] + 1: s_alpha advances it at the end of each
+// iteration, so a captured iteration replays unchanged
+__global__ void s_half1(ColState *cs, Acc *acc, uint32_t ncol, int32_t const *counters, double tol) {
     uint32_t const c = blockIdx.x*blockDim.x + threadIdx.x;
     if (c >= ncol) return;
+    int const m = 2*(counters[2] + 1) - 1;
     ColState s = cs[c];
     double const wn = sqrt(acc[c].n2);
     acc[c].n2 = 0;
@@ -370,10 +374,11 @@ __global__ void s_half1(ColState *cs, Acc *acc, uint32_t ncol, int m, double tol
 // stall_level and whose tau has not halved within stall_window half steps has reached the
 // rounding floor of the sweep; it is frozen like a converged one (the refinement step then
 // restarts from the true FP64 residual)
-__global__ void s_half2(ColState *cs, Acc *acc, uint32_t ncol, int m, double tol, int32_t *counters,
+__global__ void s_half2(ColState *cs, Acc *acc, uint32_t ncol, double tol, int32_t *counters,
                         double stall_level, int stall_window, float *cf) {
     uint32_t const c = blockIdx.x*blockDim.x + threadIdx.x;
     if (c >= ncol) return;
+    int const m = 2*(counters[2] + 1);
     ColState s = cs[c];
     double const wn = sqrt(acc[c].n2), rnr = acc[c].re, rni = acc[c].im;
     acc[c] = Acc{0, 0, 0, 0};
@@ -429,6 +434,7 @@ __global__ void s_half2(ColState *cs, Acc *acc, uint32_t ncol, int m, double tol
 // alpha = rho / (rt^H V)
 __global__ void s_alpha(ColState *cs, Acc *acc, uint32_t ncol, int32_t *counters, float *cf) {
     uint32_t const c = blockIdx.x*blockDim.x + threadIdx.x;
+    if (0 == c) counters[2] += 1;                   // next iteration (read only by later kernels)
     if (c >= ncol) return;
     ColState s = cs[c];
     double const sr = acc[c].re, si = acc[c].im;
@@ -572,18 +578,17 @@ bool tfqmr_inner(DevicePlan &dp, SolverWorkspace &ws, TfqmrVectors &v, TX *Xs, d
     count_launch();
     s_init<<<gs, 256, 0, st>>>(cs, accA, accB, ncol, cnt, cf);
     count_launch();
-    int it = 0;
-    for (it = 1; it <= maxit; ++it) {
-        bool const check = (0 == it % check_every) || (it == maxit);
-        if (check) A43G_CUDA_TRY(cudaMemsetAsync(cnt, 0, sizeof(int32_t), st));
+    // one iteration; counters[0] counts the columns still active after it
+    auto iteration = [&]() -> bool {
+        A43G_CUDA_TRY(cudaMemsetAsync(cnt, 0, sizeof(int32_t), st));
         k_A<T><<<g, 256, 0, st>>>(U2, U1, V, W, AU1, nnzb, ci, cs, accA, cf, ncol);
         count_launch();
-        s_half1<<<gs, 256, 0, st>>>(cs, accA, ncol, 2*it - 1, tol);
+        s_half1<<<gs, 256, 0, st>>>(cs, accA, ncol, cnt, tol);
         count_launch();
         if (!launch_action<T>(dp, AU2, U2, ci, st)) return false;
         k_C<T><<<g, 256, 0, st>>>(W, AU1, AU2, nnzb, ci, cs, accA, seed, cf, ncol);
         count_launch();
-        s_half2<<<gs, 256, 0, st>>>(cs, accA, ncol, 2*it, tol, cnt, stall_level, kStallWindow, cf);
+        s_half2<<<gs, 256, 0, st>>>(cs, accA, ncol, tol, cnt, stall_level, kStallWindow, cf);
         count_launch();
         k_DX<T, TX><<<g, 256, 0, st>>>(X, D, U1, U2, W, nnzb, ci, cs, cf, ncol);
         count_launch();
@@ -592,6 +597,40 @@ bool tfqmr_inner(DevicePlan &dp, SolverWorkspace &ws, TfqmrVectors &v, TX *Xs, d
         count_launch();
         s_alpha<<<gs, 256, 0, st>>>(cs, accA, ncol, cnt, cf);
         count_launch();
+        return true;
+    };
+    // the iteration is captured once into a CUDA graph and replayed (one launch instead of
+    // about 25 per iteration); not on the legacy default stream, which cannot be captured
+    cudaGraphExec_t exec = nullptr;
+    uint64_t per_iteration = 0;
+    if (st != nullptr && !std::getenv("A43G_NO_GRAPH")) {
+        uint64_t const l0 = launches_so_far();
+        cudaGraph_t graph = nullptr;
+        A43G_CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        bool const ok = iteration();
+        cudaError_t const e = cudaStreamEndCapture(st, &graph);
+        if (!ok || cudaSuccess != e || !graph) {
+            if (graph) cudaGraphDestroy(graph);
+            set_error(std::string("capture of the tfQMR iteration: ") + cudaGetErrorString(e));
+            return false;
+        }
+        cudaError_t const ei = cudaGraphInstantiate(&exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (cudaSuccess != ei) { set_error(std::string("cudaGraphInstantiate: ") + cudaGetErrorString(ei)); return false; }
+        per_iteration = launches_so_far() - l0;
+        count_launches(uint64_t(0) - per_iteration);   // captured, not launched: counted per replay
+    }
+    struct GraphGuard { cudaGraphExec_t &e; ~GraphGuard() { if (e) cudaGraphExecDestroy(e); } } guard{exec};
+    uint64_t const captured = per_iteration;
+    int it = 0;
+    for (it = 1; it <= maxit; ++it) {
+        bool const check = (0 == it % check_every) || (it == maxit);
+        if (exec) {
+            A43G_CUDA_TRY(cudaGraphLaunch(exec, st));
+            count_launches(captured);
+        } else if (!iteration()) {
+            return false;
+        }
         res.applications += 2;
         if (check) {
             A43G_CUDA_TRY(cudaMemcpyAsync(ws.host_counters, cnt, 4*sizeof(int32_t), cudaMemcpyDeviceToHost, st));

@@ -75,3 +75,24 @@ def test_solve_matches_numpy_tfqmr():
     assert info["converged"]
     Xg = X.cpu().numpy()
     assert np.abs(Xg - Xo).max() / np.abs(Xo).max() < 1e-6
+
+
+@pytest.mark.parametrize("precision", ["float64", "float32"])
+def test_graph_replay_matches_direct_launches(precision):
+    """On a non-default stream every tfQMR iteration is one replay of a captured CUDA graph; on
+    the default stream the kernels are launched one by one.  Both converge to the same solution
+    (the per-column reductions use atomics, so agreement is to the solve tolerance, not bits)."""
+    from angstromcube_b200 import _lib
+    w, p = setup("periodic4_1atom")
+    X0 = torch.zeros((p.nnzb, 2, 64, 64), device="cuda", dtype=torch.float64)
+    X1 = torch.zeros_like(X0)
+    maxit = 800 if precision == "float64" else 2400
+    s0, _ = green_action.solve(p, X=X0, tolerance=1e-10, max_iterations=maxit, precision=precision)
+    stream = torch.cuda.Stream()
+    n0 = _lib.lib().a43g_kernel_launches()
+    s1, _ = green_action.solve(p, X=X1, tolerance=1e-10, max_iterations=maxit, precision=precision, stream=stream)
+    torch.cuda.synchronize()
+    assert _lib.lib().a43g_kernel_launches() - n0 > 10 * s1["iterations"]   # replays are counted
+    assert s0["converged"] and s1["converged"], (s0, s1)
+    err = ((X0 - X1).abs().max() / X0.abs().max()).item()
+    assert err < 1e-8
