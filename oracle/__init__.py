@@ -201,6 +201,27 @@ def ref_sho_prefactors(numax, sigma):
     return out
 
 
+def ref_quadrature(kind, n):
+    """The reference's quadrature tables (src/energy_contour.cxx:456, :2156): kind "legendre"
+    or "fermi_dirac"; nodes ascending and weights."""
+    lib = _load_ref()
+    x = np.zeros(256); w = np.zeros(256)
+    f = lib.ref_gauss_legendre if kind == "legendre" else lib.ref_gauss_fermi_dirac
+    m = f(_ptr(x), _ptr(w), ctypes.c_uint(int(n)))
+    o = np.argsort(x[:m])
+    return x[:m][o], w[:m][o]
+
+
+def ref_energy_mesh(kBT, eBot, nBot, nPar, nFer, nPol):
+    """energy_contour::get_energy_mesh (src/energy_contour.cxx:139-240): points and weights."""
+    lib = _load_ref()
+    E = np.zeros(2 * 512); W = np.zeros(2 * 512)
+    lib.ref_energy_mesh.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                    ctypes.c_uint, ctypes.c_uint, ctypes.c_uint, ctypes.c_int]
+    n = lib.ref_energy_mesh(_ptr(E), _ptr(W), 512, kBT, eBot, nBot, nPar, nFer, nPol)
+    return E[:2 * n:2] + 1j * E[1:2 * n:2], W[:2 * n:2] + 1j * W[1:2 * n:2]
+
+
 # ---------------------------------------------------------------- restated oracle (plain C)
 
 class _OraclePlan(ctypes.Structure):

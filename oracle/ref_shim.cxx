@@ -23,6 +23,14 @@
 #include "control.hxx"          // control::set
 #include "sho_tools.hxx"        // sho_tools::nSHO
 #include "sho_projection.hxx"   // sho_projection::get_sho_prefactors
+#include "energy_contour.hxx"   // energy_contour::get_energy_mesh and its quadratures
+#include "green_solver.hxx"     // green_solver_t (link stubs below)
+
+// defined in src/energy_contour.cxx without a declaration in its header
+namespace energy_contour {
+std::vector<std::complex<double>> get_energy_mesh(std::vector<std::complex<double>> &w8, double kBT, double eBot,
+                                                  unsigned nBot, unsigned nPar, unsigned nFer, int nPol, int echo);
+}
 
 namespace {
 
@@ -275,4 +283,29 @@ void ref_sho_prefactors(double *out, int numax, double sigma) {
     for (size_t i = 0; i < f.size(); ++i) out[i] = f[i];
 }
 
+// energy_contour::get_energy_mesh (src/energy_contour.cxx:139-240): up to cap points E and
+// weights w8 as interleaved (re, im) pairs; returns the number of points
+int ref_energy_mesh(double *E, double *w8, int cap, double kBT, double eBot, unsigned nBot, unsigned nPar,
+                    unsigned nFer, int nPol) {
+    std::vector<std::complex<double>> w;
+    auto const Ep = energy_contour::get_energy_mesh(w, kBT, eBot, nBot, nPar, nFer, nPol, 0);
+    int const n = int(Ep.size());
+    for (int i = 0; i < n && i < cap; ++i) {
+        E[2*i] = Ep[i].real(); E[2*i + 1] = Ep[i].imag();
+        w8[2*i] = w[i].real(); w8[2*i + 1] = w[i].imag();
+    }
+    return n;
+}
+
+// the quadratures of the contour (src/energy_contour.cxx:456, :2156); x, w hold 128 entries
+int ref_gauss_legendre(double *x, double *w, unsigned n) { return energy_contour::Gauss_Legendre_quadrature(x, w, n, 0); }
+int ref_gauss_fermi_dirac(double *x, double *w, unsigned n) { return energy_contour::Gauss_Fermi_Dirac_quadrature(x, w, n, 0); }
+
 } // extern "C"
+
+// The contour source also holds the integrator, which calls the solver; the solver needs the
+// external tfQMRgpu headers and is not built here.  These definitions only satisfy the linker:
+// the oracle never constructs a green_solver_t.
+green_solver_t::green_solver_t(action_plan_t *, int, int) { std::fprintf(stderr, "oracle: no solver\n"); }
+green_solver_t::~green_solver_t() {}
+status_t green_solver_t::solve(std::complex<double> *, uint32_t, int, int, int) { return 1; }
