@@ -17,7 +17,7 @@ A43G_F64, A43G_F32 = 0, 1
 EXPORTED = [
     "a43g_last_error", "a43g_version", "a43g_plan_build", "a43g_plan_destroy", "a43g_plan_get_sizes",
     "a43g_plan_export", "a43g_plan_set_potential", "a43g_plan_set_atom_matrices", "a43g_plan_set_energy",
-    "a43g_plan_set_kpoint", "a43g_plan_upload", "a43g_action_multiply", "a43g_action_part", "a43g_vjp", "a43g_action_multiply_noalloc",
+    "a43g_plan_set_kpoint", "a43g_plan_upload", "a43g_action_multiply", "a43g_action_part", "a43g_vjp", "a43g_plan_autotune", "a43g_action_multiply_noalloc",
     "a43g_kernel_launches", "a43g_plan_device_status", "a43g_solve", "a43g_solve_batched",
 ]
 
@@ -91,6 +91,7 @@ def lib():
         L.a43g_action_multiply.argtypes = [vp, vp, vp, vp, u32, u32, ctypes.c_uint, vp, i32, ctypes.POINTER(f64)]
         L.a43g_action_part.argtypes = [vp, i32, vp, vp, vp, i32]
         L.a43g_vjp.argtypes = [vp, vp, vp, vp, vp, vp, vp]
+        L.a43g_plan_autotune.argtypes = [vp, i32, vp, ctypes.c_char_p, ctypes.c_size_t]
         L.a43g_action_multiply_noalloc.argtypes = [vp, vp, vp, vp, u32, u32, vp, i32, ctypes.POINTER(f64)]
         L.a43g_kernel_launches.restype = ctypes.c_uint64
         L.a43g_plan_device_status.argtypes = [vp]

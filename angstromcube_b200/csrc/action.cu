@@ -727,7 +727,7 @@ bool launch_local(DevicePlan &dp, T *y, T const *x, cudaStream_t st) {
         for (int d = 0; d < 3; ++d) for (int s = 0; s < 2; ++s) for (int c = 0; c < 2; ++c) a.ph[d][s][c] = T(dp.phase[d][s][c]);
         constexpr int S = (sizeof(T) == 8) ? 8 : 16;
         unsigned const nblk = dp.nlists[2]*(64/S);
-        if (nblk && sizeof(T) == 4 && dp.max_zline <= kMaxLine) {
+        if (nblk && sizeof(T) == 4 && dp.max_zline <= kMaxLine && 0 == dp.local_variant) {
             local_fused_pf_kernel<T, S><<<nblk, S*16, 0, st>>>(y, x, dptr<uint32_t>(dp.lists_start[2]),
                 dptr<int32_t>(dp.lists[2]), dptr<int32_t>(dp.nbr), dptr<int32_t>(dp.veff_index), vcell<T>(dp), a);
             count_launch();

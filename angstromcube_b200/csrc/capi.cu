@@ -5,6 +5,7 @@
 #include "vjp.hpp"
 #include "noalloc.hpp"
 
+#include <algorithm>
 #include <atomic>
 #include <cstring>
 #include <mutex>
@@ -245,6 +246,25 @@ int a43g_action_multiply_noalloc(a43g_plan_t *plan, void *y, const void *x, cons
     if (!ok) return A43G_ERR_CUDA;
     if (flops) *flops = a43g::action_flops(plan->host, (A43G_F64 == dtype) ? 8 : 4);
     return A43G_OK;
+}
+
+int a43g_plan_autotune(a43g_plan_t *plan, int dtype, void *stream, char *report, size_t report_size) {
+    if (!plan) return fail(A43G_ERR_ARGUMENT, "null argument");
+    std::lock_guard<std::mutex> lock(plan->mtx);
+    if (!plan->energy_set) return fail(A43G_ERR_STATE, "energy parameter not set (a43g_plan_set_energy)");
+    int const rc = ensure_device(plan);
+    if (rc) return rc;
+    std::string text;
+    bool ok;
+    if (A43G_F64 == dtype) ok = a43g::autotune<double>(plan->host, plan->dev, (cudaStream_t)stream, text);
+    else if (A43G_F32 == dtype) ok = a43g::autotune<float>(plan->host, plan->dev, (cudaStream_t)stream, text);
+    else return fail(A43G_ERR_ARGUMENT, "dtype must be A43G_F64 or A43G_F32");
+    if (report && report_size) {
+        size_t const m = std::min(report_size - 1, text.size());
+        std::memcpy(report, text.data(), m);
+        report[m] = 0;
+    }
+    return ok ? A43G_OK : A43G_ERR_CUDA;
 }
 
 int a43g_vjp(a43g_plan_t *plan, const void *L, const void *G, double *dV, double *dM, double *dR, void *stream) {

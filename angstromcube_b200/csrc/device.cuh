@@ -44,6 +44,10 @@ struct DevicePlan {
     double E_re = 0, E_im = 0;
     bool fused_local = false;    // all directions use the 9-point stencil: fused kernel
     uint32_t max_zline = 0;      // cubes in the longest z-line
+    // schedule parameters, set by the autotuner (autotune.cu) or left at these defaults
+    uint32_t prj_chunk = 16;         // blocks per projection work item
+    uint32_t add_blocks = 16;        // blocks per CTA of the FP32 addition
+    int local_variant = 0;           // 0: local kernel with one-step-ahead loads, 1: plain
     uint32_t nlists[3] = {0, 0, 0};
 
     DeviceBuffer veff_index;     // int32 [nnzb]
@@ -86,6 +90,11 @@ bool prepare_tc_kernels();
 void count_launches(uint64_t n);
 uint64_t launches_so_far();
 bool upload_values(GreenPlan const &hp, DevicePlan &dp);
+// projection work items (image, source, up to dp.prj_chunk consecutive blocks of its list)
+bool build_prj_items(GreenPlan const &hp, DevicePlan &dp);
+// chooses the schedule parameters of the action for this plan by timing them (autotune.cu)
+template <typename T>
+bool autotune(GreenPlan const &hp, DevicePlan &dp, cudaStream_t st, std::string &report);
 bool ensure_dyadic_scratch(DevicePlan &dp, size_t elem_bytes);
 
 // the action y = (H - E S) x on real_t = double or float

@@ -125,25 +125,7 @@ bool upload_plan(GreenPlan const &hp, DevicePlan &dp) {
         if (!put(dp.img_group[L].images, imgs)) return false;
     }
     if (dp.lmax_max > 7) { set_error("projector basis sizes above numax 7 are not supported"); return false; }
-    {
-        constexpr uint32_t kPrjChunk = 16;
-        std::vector<uint32_t> items[8];
-        for (uint32_t s = 0; s < hp.nCols; ++s) {
-            auto const &c = hp.SHOprj[s];
-            if (c.start.empty()) continue;
-            for (uint32_t a = 0; a < hp.nAtomImages; ++a) {
-                int const L = hp.AtomImageLmax[a];
-                for (uint32_t k = c.start[a]; k < c.start[a + 1]; k += kPrjChunk) {
-                    uint32_t const it[4] = {a, s, k, std::min(k + kPrjChunk, c.start[a + 1])};
-                    items[L].insert(items[L].end(), it, it + 4);
-                }
-            }
-        }
-        for (int L = 0; L < 8; ++L) {
-            dp.prj_items[L].count = uint32_t(items[L].size()/4);
-            if (!put(dp.prj_items[L].items, items[L])) return false;
-        }
-    }
+    if (!build_prj_items(hp, dp)) return false;
     dp.table_stride = (hp.table_lmax + 1)*12;
     if (!put(dp.slot_H, hp.slot_H) || !put(dp.slot_mask, hp.slot_mask)) return false;
     if (!put(dp.slot_H32, std::vector<float>(hp.slot_H.begin(), hp.slot_H.end()))) return false;
@@ -170,6 +152,27 @@ bool upload_plan(GreenPlan const &hp, DevicePlan &dp) {
     dp.uploaded = true;
     dp.values_dirty = true;
     return upload_values(hp, dp);
+}
+
+bool build_prj_items(GreenPlan const &hp, DevicePlan &dp) {
+    uint32_t const chunk = std::max<uint32_t>(1, dp.prj_chunk);
+    std::vector<uint32_t> items[8];
+    for (uint32_t s = 0; s < hp.nCols; ++s) {
+        auto const &c = hp.SHOprj[s];
+        if (c.start.empty()) continue;
+        for (uint32_t a = 0; a < hp.nAtomImages; ++a) {
+            int const L = hp.AtomImageLmax[a];
+            for (uint32_t k = c.start[a]; k < c.start[a + 1]; k += chunk) {
+                uint32_t const it[4] = {a, s, k, std::min(k + chunk, c.start[a + 1])};
+                items[L].insert(items[L].end(), it, it + 4);
+            }
+        }
+    }
+    for (int L = 0; L < 8; ++L) {
+        dp.prj_items[L].count = uint32_t(items[L].size()/4);
+        if (!put(dp.prj_items[L].items, items[L])) return false;
+    }
+    return true;
 }
 
 bool upload_values(GreenPlan const &hp, DevicePlan &dp) {

@@ -19,6 +19,8 @@
 //     on 512-byte boundaries of the plan's coefficient array).
 #include "device.cuh"
 
+#include <algorithm>
+
 namespace a43g {
 
 namespace {
@@ -353,9 +355,9 @@ void launch_project_L(DevicePlan &dp, T const *x, cudaStream_t st) {
 template <typename T, int LMAX>
 void launch_add_L(DevicePlan &dp, T *y, uint16_t const *colIndex, cudaStream_t st) {
     constexpr int smem = (2*nsho_of(LMAX)*128 + kBlk)*int(sizeof(T));
-    constexpr uint32_t kBlocksPerCta = 16;
-    unsigned const grid = (dp.nnzb + kBlocksPerCta - 1)/kBlocksPerCta;
-    sho_add_simt_kernel<T, LMAX><<<grid, kThreads, smem, st>>>(y, dptr<T>(dp.cad), dp.nCols, dp.nnzb, kBlocksPerCta,
+    uint32_t const per_cta = std::max<uint32_t>(1, dp.add_blocks);
+    unsigned const grid = (dp.nnzb + per_cta - 1)/per_cta;
+    sho_add_simt_kernel<T, LMAX><<<grid, kThreads, smem, st>>>(y, dptr<T>(dp.cad), dp.nCols, dp.nnzb, per_cta,
         colIndex, dptr<uint32_t>(dp.add_start), dptr<uint4>(dp.add_info), simt_table<T>(dp),
         dptr<uint64_t>(dp.slot_mask), dp.table_stride);
 }

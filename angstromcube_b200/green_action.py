@@ -114,3 +114,12 @@ def vjp(plan, L, G, potential=True, matrices=True, positions=True, stream=0):
     if positions:
         out["R"] = (dR[..., 0] + 1j * dR[..., 1])[:nat]
     return out
+
+
+def autotune(plan, precision="float32", stream=0):
+    """Chooses the action's schedule for this plan by timing (a43g_plan_autotune); returns the
+    report text."""
+    buf = ctypes.create_string_buffer(4096)
+    st = ctypes.c_void_p(stream if isinstance(stream, int) else stream.cuda_stream)
+    check(_lib.lib().a43g_plan_autotune(plan.handle, _dtype_code(precision), st, buf, len(buf)), "a43g_plan_autotune")
+    return buf.value.decode()

@@ -161,6 +161,13 @@ int a43g_action_part(a43g_plan_t *plan, int part, void *y, const void *x, void *
  * Synchronizes the stream. */
 int a43g_vjp(a43g_plan_t *plan, const void *L, const void *G, double *dV, double *dM, double *dR, void *stream);
 
+/* ---- autotuner (no reference counterpart): times the schedule parameters of the action for
+ * this plan in the given precision on the current device (blocks per projection CTA, blocks per
+ * addition CTA, local-kernel variant, CUDA-core or tensor-core FP32 projector) and keeps the
+ * fastest for the plan's later calls; allocates two scratch block vectors for its duration.
+ * report (optional) receives a text summary of the timings. */
+int a43g_plan_autotune(a43g_plan_t *plan, int dtype, void *stream, char *report, size_t report_size);
+
 /* synchronizes the device and reports an error a kernel of this plan recorded (for example a
  * bounded wait of the tensor-core projector that timed out); clears the record */
 int a43g_plan_device_status(a43g_plan_t *plan);

@@ -175,3 +175,19 @@ def test_action_rejects_bad_sizes():
         op.multiply(torch.empty_like(x), x, ci, p.nnzb + 1, p.nCols)
     with pytest.raises(RuntimeError, match="alias"):
         op.multiply(x, x, ci, p.nnzb, p.nCols)
+
+
+@pytest.mark.parametrize("name", ["wrap8", "peri_xy_wrap_z"])
+def test_autotune_keeps_parity(name):
+    """The autotuner only changes the schedule: after it the FP32 and FP64 actions still match
+    the oracle."""
+    g = GEOMETRIES[name]()
+    Vc, mats, offs, E, k, dVol, na = inputs_for(g)
+    p = product_plan(g, Vc, mats, offs, E, k, dVol)
+    report = green_action.autotune(p, "float32")
+    assert "chosen" in report, report
+    x = np.random.default_rng(12).standard_normal((p.nnzb, 2, 64, 64))
+    y_ref = oracle.RestatedOracle(p.export(), Vc, E).action(x)
+    assert rel_err(apply(p, x, np.float32), y_ref) < FP32_TOL
+    assert "chosen" in green_action.autotune(p, "float64")
+    assert rel_err(apply(p, x, np.float64), y_ref) < FP64_TOL
