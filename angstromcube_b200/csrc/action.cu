@@ -811,8 +811,8 @@ bool launch_dyadic(DevicePlan &dp, T *y, T const *x, uint16_t const *colIndex, c
     }
     if (tc) {
         if (!launch_add_tc(dp, (float*)y, colIndex, st)) return false;
-    } else if (simt && sizeof(T) == 4) {
-        if (!launch_add_simt<float>(dp, (float*)y, colIndex, st)) return false;
+    } else if (simt) {
+        if (!launch_add_simt<T>(dp, y, colIndex, st)) return false;
     } else {
         sho_add_kernel<T><<<dp.nnzb, 128, 0, st>>>(y, dptr<T>(dp.cad), dp.nCols, dp.nnzb, colIndex,
             dptr<uint32_t>(dp.add_start), dptr<uint32_t>(dp.add_col), dptr<uint32_t>(dp.add_slot),

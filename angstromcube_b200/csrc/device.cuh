@@ -133,6 +133,6 @@ bool launch_add_tc(DevicePlan &dp, float *y, uint16_t const *colIndex, cudaStrea
 // both stage blocks with 16-byte copies and need 16-byte aligned x and y
 bool simt_projector_supported(DevicePlan const &dp, void const *x, void const *y, size_t real_bytes);
 template <typename T> bool launch_project_simt(DevicePlan &dp, T const *x, cudaStream_t st);
-template <typename T> bool launch_add_simt(DevicePlan &dp, T *y, uint16_t const *colIndex, cudaStream_t st);  // FP32
+template <typename T> bool launch_add_simt(DevicePlan &dp, T *y, uint16_t const *colIndex, cudaStream_t st);
 
 } // namespace a43g

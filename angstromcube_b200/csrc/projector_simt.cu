@@ -67,7 +67,7 @@ __device__ __forceinline__ double fmat(double a, double b, double c) { return fm
 
 // CTAs per SM the kernels are compiled for (FP64 needs twice the registers and shared memory)
 template <typename T> struct Occ { static constexpr int project = 3, add = 2; };
-template <> struct Occ<double> { static constexpr int project = 1; };   // the addition is FP32 only
+template <> struct Occ<double> { static constexpr int project = 1, add = 1; };
 
 __device__ __forceinline__ void cp_async8(void *dst, void const *src) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" :: "r"(smem_addr(dst)), "l"(src) : "memory");
@@ -173,11 +173,15 @@ sho_project_simt_kernel(T *__restrict__ apc, T const *__restrict__ x, uint32_t n
 // ---------------------------------------------------------------- addition
 
 // contribution of one image with basis size L to the 64 point sums of this thread
-template <typename T, int L, bool FULL>
-__device__ __forceinline__ void add_image(T (&acc)[64], Tables<T, L> const &t, uint64_t mask,
-                                          T const *__restrict__ c, size_t cstride) {
-#pragma unroll
-    for (int iz = 0, sho = 0; iz <= L; ++iz) {
+// ZS threads share a column and split its z-planes (FP64: the 64 sums of one thread would not
+// fit the registers); each computes the x and y stages in full and its planes zh*(4/ZS) ...
+template <typename T, int L, bool FULL, int ZS>
+__device__ __forceinline__ void add_image(T (&acc)[64/ZS], Tables<T, L> const &t, uint64_t mask,
+                                          T const *__restrict__ c, size_t cstride, int zh) {
+    constexpr int kUnrollZ = (8 == sizeof(T)) ? 1 : L + 1;     // FP64: one z-order at a time (registers)
+    int sho = 0;
+#pragma unroll kUnrollZ
+    for (int iz = 0; iz <= L; ++iz) {
         T byx[16];
 #pragma unroll
         for (int i = 0; i < 16; ++i) byx[i] = T(0);
@@ -198,25 +202,26 @@ __device__ __forceinline__ void add_image(T (&acc)[64], Tables<T, L> const &t, u
             }
         }
 #pragma unroll
-        for (int z = 0; z < 4; ++z) {
+        for (int zz = 0; zz < 4/ZS; ++zz) {
+            int const z = zh*(4/ZS) + zz;
             T const hz = t(iz, 2, z);
 #pragma unroll
             for (int q = 0; q < 16; ++q) {
-                int const p = z*16 + q;
-                if (FULL) acc[p] = fmat(hz, byx[q], acc[p]);
-                else acc[p] = ((mask >> p) & 1u) ? fmat(hz, byx[q], acc[p]) : acc[p];
+                int const p = z*16 + q, pl = zz*16 + q;
+                if (FULL) acc[pl] = fmat(hz, byx[q], acc[pl]);
+                else acc[pl] = ((mask >> p) & 1u) ? fmat(hz, byx[q], acc[pl]) : acc[pl];
             }
         }
     }
 }
 
-template <typename T, int L>
-__device__ __forceinline__ void add_image_L(T (&acc)[64], T const *__restrict__ tab, uint64_t mask,
-                                            T const *__restrict__ c, size_t cstride) {
+template <typename T, int L, int ZS>
+__device__ __forceinline__ void add_image_L(T (&acc)[64/ZS], T const *__restrict__ tab, uint64_t mask,
+                                            T const *__restrict__ c, size_t cstride, int zh) {
     Tables<T, L> t;
     t.load(tab);
-    if (~0ull == mask) add_image<T, L, true>(acc, t, mask, c, cstride);
-    else add_image<T, L, false>(acc, t, mask, c, cstride);
+    if (~0ull == mask) add_image<T, L, true, ZS>(acc, t, mask, c, cstride, zh);
+    else add_image<T, L, false, ZS>(acc, t, mask, c, cstride, zh);
 }
 
 // LMAX: largest basis size of the plan (the instantiation has no larger one).  One CTA walks the
@@ -224,8 +229,8 @@ __device__ __forceinline__ void add_image_L(T (&acc)[64], T const *__restrict__ 
 // stream: the coefficients, table and mask of the next pair are staged while the current pair is
 // applied, and the y values of the next block with atoms are staged during the whole of the
 // current block, so neither the start of a block nor its final y update waits for memory.
-template <typename T, int LMAX>
-__global__ void __launch_bounds__(kThreads, Occ<T>::add)
+template <typename T, int LMAX, int ZS = int(sizeof(T))/4>
+__global__ void __launch_bounds__(kThreads*ZS, Occ<T>::add)
 sho_add_simt_kernel(T *__restrict__ y, T const *__restrict__ cad, uint32_t nrhs, uint32_t nnzb,
                     uint32_t blocks_per_cta, uint16_t const *__restrict__ colIndex,
                     uint32_t const *__restrict__ add_start, uint4 const *__restrict__ info,
@@ -242,7 +247,8 @@ sho_add_simt_kernel(T *__restrict__ y, T const *__restrict__ cad, uint32_t nrhs,
     if (b0 >= b1) return;
     uint32_t const T0 = add_start[b0], T1 = add_start[b1];
     if (T0 >= T1) return;                                  // no atoms near any of these blocks
-    int const tid = threadIdx.x, reim = tid >> 6, j = tid & 63;
+    constexpr int NT = kThreads*ZS, NP = 64/ZS;             // threads, point sums per thread
+    int const tid = threadIdx.x, zh = tid/kThreads, reim = (tid >> 6) & 1, j = tid & 63;
     size_t const cstride = size_t(nrhs)*128;
 
     // the block owning pair t: blocks are visited in order, skipping blocks without pairs
@@ -256,18 +262,18 @@ sho_add_simt_kernel(T *__restrict__ y, T const *__restrict__ cad, uint32_t nrhs,
         T const *src = cad + (size_t(inf.y)*nrhs + src_col)*128;
         T *dst = cbuf + buf*NCMAX*128;
         constexpr int CPR = 128/TE;                        // 16-byte copies per coefficient row
-        for (int q = tid; q < nc*CPR; q += kThreads) {
+        for (int q = tid; q < nc*CPR; q += NT) {
             int const row = q/CPR, part = (q % CPR)*TE;
             cp_async16(dst + row*128 + part, src + size_t(row)*cstride + part);
         }
         if (tid < (L + 1)*12/TE) cp_async16(&tbuf[buf][tid*TE], slot_H + size_t(inf.x)*stride + tid*TE);
-        if (tid == kThreads - 1) cp_async8(&mbuf[buf], slot_mask + inf.x);
+        if (tid == NT - 1) cp_async8(&mbuf[buf], slot_mask + inf.x);
     };
     auto stage_y = [&](uint32_t blk) {
         T const *src = y + size_t(blk)*kBlk;
 #pragma unroll
-        for (int r = 0; r < kBlk/(TE*kThreads); ++r) {
-            int const o = (r*kThreads + tid)*TE;
+        for (int r = 0; r < kBlk/(TE*NT); ++r) {
+            int const o = (r*NT + tid)*TE;
             cp_async16(ybuf + o, src + o);
         }
     };
@@ -278,9 +284,9 @@ sho_add_simt_kernel(T *__restrict__ y, T const *__restrict__ cad, uint32_t nrhs,
         return colIndex[c];
     };
 
-    T acc[64];
+    T acc[NP];
 #pragma unroll
-    for (int i = 0; i < 64; ++i) acc[i] = T(0);
+    for (int i = 0; i < NP; ++i) acc[i] = T(0);
     uint64_t mask_all = 0;
     uint4 const zero4 = make_uint4(0u, 0u, 0u, 0u);
     uint4 cur = info[T0];
@@ -301,14 +307,14 @@ sho_add_simt_kernel(T *__restrict__ y, T const *__restrict__ cad, uint32_t nrhs,
             T const *tab = tbuf[buf];
             T const *c = cbuf + buf*NCMAX*128 + reim*64 + j;
             int const L = int(cur.z);                      // uniform over the CTA
-            if (L == LMAX) add_image_L<T, LMAX>(acc, tab, mask, c, 128);
-            else if (LMAX > 0 && L == 0) add_image_L<T, 0>(acc, tab, mask, c, 128);
-            else if (LMAX > 1 && L == 1) add_image_L<T, (LMAX > 1 ? 1 : 0)>(acc, tab, mask, c, 128);
-            else if (LMAX > 2 && L == 2) add_image_L<T, (LMAX > 2 ? 2 : 0)>(acc, tab, mask, c, 128);
-            else if (LMAX > 3 && L == 3) add_image_L<T, (LMAX > 3 ? 3 : 0)>(acc, tab, mask, c, 128);
-            else if (LMAX > 4 && L == 4) add_image_L<T, (LMAX > 4 ? 4 : 0)>(acc, tab, mask, c, 128);
-            else if (LMAX > 5 && L == 5) add_image_L<T, (LMAX > 5 ? 5 : 0)>(acc, tab, mask, c, 128);
-            else if (LMAX > 6 && L == 6) add_image_L<T, (LMAX > 6 ? 6 : 0)>(acc, tab, mask, c, 128);
+            if (L == LMAX) add_image_L<T, LMAX, ZS>(acc, tab, mask, c, 128, zh);
+            else if (LMAX > 0 && L == 0) add_image_L<T, 0, ZS>(acc, tab, mask, c, 128, zh);
+            else if (LMAX > 1 && L == 1) add_image_L<T, (LMAX > 1 ? 1 : 0), ZS>(acc, tab, mask, c, 128, zh);
+            else if (LMAX > 2 && L == 2) add_image_L<T, (LMAX > 2 ? 2 : 0), ZS>(acc, tab, mask, c, 128, zh);
+            else if (LMAX > 3 && L == 3) add_image_L<T, (LMAX > 3 ? 3 : 0), ZS>(acc, tab, mask, c, 128, zh);
+            else if (LMAX > 4 && L == 4) add_image_L<T, (LMAX > 4 ? 4 : 0), ZS>(acc, tab, mask, c, 128, zh);
+            else if (LMAX > 5 && L == 5) add_image_L<T, (LMAX > 5 ? 5 : 0), ZS>(acc, tab, mask, c, 128, zh);
+            else if (LMAX > 6 && L == 6) add_image_L<T, (LMAX > 6 ? 6 : 0), ZS>(acc, tab, mask, c, 128, zh);
         }
         cur = nxt; nxt = after;
         if (t + 1 == bend) {
@@ -318,9 +324,10 @@ sho_add_simt_kernel(T *__restrict__ y, T const *__restrict__ cad, uint32_t nrhs,
             T const *yb_s = ybuf + reim*4096 + j;
             T *yb = y + size_t(bb)*kBlk + reim*4096 + j;
 #pragma unroll
-            for (int p = 0; p < 64; ++p) {
-                if ((mask_all >> p) & 1u) yb[p*64] = yb_s[p*64] + acc[p];
-                acc[p] = T(0);
+            for (int pl = 0; pl < NP; ++pl) {
+                int const p = zh*NP + pl;                  // this thread's points
+                if ((mask_all >> p) & 1u) yb[p*64] = yb_s[p*64] + acc[pl];
+                acc[pl] = T(0);
             }
             mask_all = 0;
             __syncthreads();                               // ybuf free
@@ -357,7 +364,7 @@ void launch_add_L(DevicePlan &dp, T *y, uint16_t const *colIndex, cudaStream_t s
     constexpr int smem = (2*nsho_of(LMAX)*128 + kBlk)*int(sizeof(T));
     uint32_t const per_cta = std::max<uint32_t>(1, dp.add_blocks);
     unsigned const grid = (dp.nnzb + per_cta - 1)/per_cta;
-    sho_add_simt_kernel<T, LMAX><<<grid, kThreads, smem, st>>>(y, dptr<T>(dp.cad), dp.nCols, dp.nnzb, per_cta,
+    sho_add_simt_kernel<T, LMAX><<<grid, kThreads*(int(sizeof(T))/4), smem, st>>>(y, dptr<T>(dp.cad), dp.nCols, dp.nnzb, per_cta,
         colIndex, dptr<uint32_t>(dp.add_start), dptr<uint4>(dp.add_info), simt_table<T>(dp),
         dptr<uint64_t>(dp.slot_mask), dp.table_stride);
 }
@@ -366,9 +373,8 @@ template <typename T, int L>
 void set_smem_attributes() {
     cudaFuncSetAttribute(sho_project_simt_kernel<T, L>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          2*kBlk*int(sizeof(T)));
-    if constexpr (sizeof(T) == 4)
-        cudaFuncSetAttribute(sho_add_simt_kernel<T, L>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (2*nsho_of(L)*128 + kBlk)*int(sizeof(T)));
+    cudaFuncSetAttribute(sho_add_simt_kernel<T, L>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (2*nsho_of(L)*128 + kBlk)*int(sizeof(T)));
 }
 
 } // namespace
@@ -405,8 +411,7 @@ bool launch_project_simt(DevicePlan &dp, T const *x, cudaStream_t st) {
     return true;
 }
 
-// (FP32 only: in FP64 the 64 point sums per thread do not fit the registers; the FP64 action
-// keeps the generic addition kernel)
+// (FP64 up to numax 5: its two coefficient stages and y fit 227 KB of shared memory)
 template <typename T>
 bool launch_add_simt(DevicePlan &dp, T *y, uint16_t const *colIndex, cudaStream_t st) {
     switch (dp.lmax_max) {
@@ -431,5 +436,6 @@ bool launch_add_simt(DevicePlan &dp, T *y, uint16_t const *colIndex, cudaStream_
 template bool launch_project_simt<float>(DevicePlan &, float const *, cudaStream_t);
 template bool launch_project_simt<double>(DevicePlan &, double const *, cudaStream_t);
 template bool launch_add_simt<float>(DevicePlan &, float *, uint16_t const *, cudaStream_t);
+template bool launch_add_simt<double>(DevicePlan &, double *, uint16_t const *, cudaStream_t);
 
 } // namespace a43g

@@ -420,7 +420,9 @@ __global__ void s_half2(ColState *cs, Acc *acc, uint32_t ncol, double tol, int32
     if (tau <= 0.5*s.tau_ref) { s.tau_ref = tau; s.m_ref = m; }
     if (est <= tol*s.bnorm) {
         s.status = 1; s.be_re = s.be_im = 0; s.al_re = s.al_im = 0;
-    } else if (stall_level > 0 && est <= stall_level*s.bnorm && m - s.m_ref > stall_window) {
+    } else if (stall_level > 0 && m - s.m_ref > (est <= stall_level*s.bnorm ? stall_window : 4*stall_window)) {
+        // FP32 sweep: no halving of tau for stall_window half steps below the stall level, or
+        // for four times as long above it (a sweep that lost its way; the refinement restarts it)
         s.status = 4; s.be_re = s.be_im = 0; s.al_re = s.al_im = 0;
     } else if (rnr*rnr + rni*rni == 0.0) {
         s.status = 2; s.be_re = s.be_im = 0; s.al_re = s.al_im = 0; atomicAdd(&counters[1], 1);

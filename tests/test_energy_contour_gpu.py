@@ -13,12 +13,12 @@ def test_integrate_matches_individual_solves():
     w = workloads.make("periodic4_1atom")
     p = gf.construct_Green_function(w.geometry)
     gf.update_potential(p, w.Vcell, w.mats, w.offsets, layout="cells")
-    E, W = ec.get_energy_mesh(2e-2, -1.0, 2, 3, 2, 1)
+    E, W = ec.get_energy_mesh(5e-2, -1.0, 2, 3, 2, 1)     # lowest point at Im E = pi kT = 0.16
     ks = [np.zeros(3), np.array([0.25, 0.0, 0.0])]
     kw = [0.5, 0.5]
-    opts = dict(tolerance=1e-10, max_iterations=3000, precision="float64", check_every=5)
+    opts = dict(tolerance=1e-9, max_iterations=4000, precision="float64", check_every=5)
     rho, resp, stats = ec.integrate(p, E, W, ks, kw, w.dVol, fermi_level=-0.1, **opts)
-    assert len(stats) == len(E) * len(ks) and all(s["converged"] for s in stats)
+    assert len(stats) == len(E) * len(ks) and all(s["converged"] for s in stats), stats
     total = 0
     for e, we in zip(E, W):
         for k, wk in zip(ks, kw):
