@@ -26,7 +26,8 @@ constexpr int kThreads = 256;
 constexpr int kA = 32768;            // bytes of one 128 x 64 FP32 operand
 constexpr int kB = 16384;            // bytes of one 64 x 64 FP32 operand
 constexpr int kStage = 2*kA + 2*kB;  // A_hi, A_lo, B_hi, B_lo
-constexpr int kSmem = 2*kStage + 1024;
+constexpr int kRaw = 32768;          // one FP32 block as it is in memory, prefetched by cp.async
+constexpr int kSmem = 2*kStage + kRaw;        // 224 KB of the 227 KB a CTA may use
 constexpr uint64_t kWaitNs = 500000000ull;    // 0.5 s per wait: far beyond any MMA latency
 constexpr uint32_t kIdesc = tc::idesc_tf32(128, 64, false, false);  // A and B K-major
 
@@ -49,32 +50,28 @@ __device__ __forceinline__ void issue_mmas(uint32_t tmem, uint32_t sA_hi, uint32
     }
 }
 
-// stage a 128 x 64 FP32 matrix, element (m = reim*64 + j, k) at src[reim*plane + k*ld_k + j],
-// as the split K-major operand; rows k >= kmax are zero.  Each thread reads a 4 (k) x 4 (m)
-// tile with four coalesced float4 loads along m and stores it transposed, 4 k-values per
-// 16-byte chunk.
-__device__ __forceinline__ void stage_A(char *sA_hi, char *sA_lo, float const *__restrict__ src, size_t plane,
+// stage a 128 x 64 FP32 matrix, element (m = reim*64 + j, k) at src[reim*plane + k*ld_k + j]
+// (shared memory), as the split K-major operand; rows k >= kmax are zero.  Thread (m, kh)
+// gathers column m for the 32 values k = kh*32 ... (scalar loads, consecutive m in consecutive
+// banks) and stores 4 k-values per 16-byte chunk: the 8 threads of a store phase write the 8
+// rows of one core matrix, 128 contiguous bytes, so neither loads nor stores conflict.
+__device__ __forceinline__ void stage_A(char *sA_hi, char *sA_lo, float const *src, size_t plane,
                                         size_t ld_k, int kmax, int tid) {
+    static_assert(kThreads == 256, "one thread per (row, half of K)");
+    int const m = tid & 127, kh = tid >> 7;
+    float const *col = src + (m >> 6)*plane + (m & 63);
 #pragma unroll
-    for (int r = 0; r < 512/kThreads; ++r) {
-        int const q = r*kThreads + tid;
-        int const m0 = (q & 31)*4, k0 = (q >> 5)*4;
-        float t[4][4];                               // t[kk][mm]
+    for (int c = 0; c < 8; ++c) {                    // 4 k-values per chunk
+        int const k0 = kh*32 + c*4;
+        float v[4];
 #pragma unroll
-        for (int kk = 0; kk < 4; ++kk) {
-            float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (k0 + kk < kmax) v = __ldg(reinterpret_cast<float4 const*>(src + (m0 >> 6)*plane + size_t(k0 + kk)*ld_k + (m0 & 63)));
-            t[kk][0] = v.x; t[kk][1] = v.y; t[kk][2] = v.z; t[kk][3] = v.w;
-        }
-#pragma unroll
-        for (int mm = 0; mm < 4; ++mm) {
-            float4 h, l;
-            tc::split_tf32(t[0][mm], h.x, l.x); tc::split_tf32(t[1][mm], h.y, l.y);
-            tc::split_tf32(t[2][mm], h.z, l.z); tc::split_tf32(t[3][mm], h.w, l.w);
-            uint32_t const o = offA(m0 + mm, k0);
-            *reinterpret_cast<float4*>(sA_hi + o) = h;
-            *reinterpret_cast<float4*>(sA_lo + o) = l;
-        }
+        for (int kk = 0; kk < 4; ++kk) v[kk] = (k0 + kk < kmax) ? col[size_t(k0 + kk)*ld_k] : 0.f;
+        float4 h, l;
+        tc::split_tf32(v[0], h.x, l.x); tc::split_tf32(v[1], h.y, l.y);
+        tc::split_tf32(v[2], h.z, l.z); tc::split_tf32(v[3], h.w, l.w);
+        uint32_t const o = offA(m, k0);
+        *reinterpret_cast<float4*>(sA_hi + o) = h;
+        *reinterpret_cast<float4*>(sA_lo + o) = l;
     }
 }
 
@@ -96,20 +93,30 @@ __device__ __forceinline__ float pval(float const (*H)[3][4], ShoIdx const &t, u
 
 __device__ __forceinline__ void record_error(int *err, int code) { atomicCAS(err, 0, code); }
 
+__device__ __forceinline__ void cp_async16(void *dst, void const *src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" :: "r"(tc::smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void *dst, void const *src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" :: "r"(tc::smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
 // ---------------------------------------------------------------- projection
 
 __global__ void __launch_bounds__(kThreads, 1)
 sho_project_tc_kernel(float *__restrict__ apc, float const *__restrict__ x, uint32_t nrhs,
                       uint32_t const *__restrict__ images, uint32_t nAI, uint32_t const *__restrict__ prj_start,
                       uint32_t const *__restrict__ prj_col, uint64_t const *__restrict__ prj_coloff,
-                      uint32_t const *__restrict__ prj_slot, double const *__restrict__ slot_H,
+                      uint32_t const *__restrict__ prj_slot, float const *__restrict__ slot_H,
                       uint64_t const *__restrict__ slot_mask, int stride, uint32_t const *__restrict__ img_starts,
                       int8_t const *__restrict__ img_lmax, int *err)
 {
-    extern __shared__ __align__(1024) char smem[];
-    __shared__ float Hs[2][8][3][4];
+    extern __shared__ __align__(128) char smem[];
+    __shared__ __align__(16) float Hs[2][8][3][4];
     __shared__ ShoIdx sidx;
     __shared__ uint64_t mbar[2];
+    __shared__ uint64_t mk[2];
     __shared__ uint32_t tmem_base;
     int const tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     uint32_t const a = images[blockIdx.x];
@@ -133,6 +140,21 @@ sho_project_tc_kernel(float *__restrict__ apc, float const *__restrict__ x, uint
     uint32_t const tmem = tmem_base;
     bool ok = true;
     int issued = 0;                                  // commits issued (block-uniform)
+    float *raw = reinterpret_cast<float*>(smem + 2*kStage);
+    // block k (as stored), its 1D tables and mask go to shared memory one block ahead
+    auto prefetch = [&](uint32_t k, int st) {
+        float const *src = x + size_t(prj_col[off + k])*8192;
+        uint32_t const slot = prj_slot[off + k];
+#pragma unroll
+        for (int r = 0; r < kRaw/(16*kThreads); ++r) {
+            int const o = (r*kThreads + tid)*4;
+            cp_async16(raw + o, src + o);
+        }
+        if (tid < (lmax + 1)*3) cp_async16(&Hs[st][0][0][0] + tid*4, slot_H + size_t(slot)*stride + tid*4);
+        if (tid == kThreads - 1) cp_async8(&mk[st], slot_mask + slot);
+        cp_async_commit();
+    };
+    prefetch(k0, 0);
     for (uint32_t k = k0; k < k1; ++k) {
         int const it = int(k - k0), st = it & 1;
         char *sA_hi = smem + st*kStage, *sA_lo = sA_hi + kA, *sB_hi = sA_lo + kA, *sB_lo = sB_hi + kB;
@@ -142,11 +164,12 @@ sho_project_tc_kernel(float *__restrict__ apc, float const *__restrict__ x, uint
             ok = __syncthreads_and(w);               // block-uniform decision
             if (!ok) break;
         }
-        uint32_t const b = prj_col[off + k], slot = prj_slot[off + k];
-        if (tid < (lmax + 1)*12) (&Hs[st][0][0][0])[tid] = float(slot_H[size_t(slot)*stride + tid]);
-        uint64_t const mask = slot_mask[slot];
-        stage_A(sA_hi, sA_lo, x + size_t(b)*8192, 4096, 64, 64, tid);   // A = X^T: m = (reim, j), k = point i
-        __syncthreads();                             // tables staged
+        cp_async_wait0();                            // block k, its tables and mask have landed
+        __syncthreads();
+        uint64_t const mask = mk[st];
+        stage_A(sA_hi, sA_lo, raw, 4096, 64, 64, tid);   // A = X^T: m = (reim, j), k = point i
+        __syncthreads();                             // raw is free: fetch the next block meanwhile
+        if (k + 1 < k1) prefetch(k + 1, st ^ 1);
         // B = P^T: n = sho, k = point i; float4 along k
 #pragma unroll 2
         for (int r = 0; r < 1024/kThreads; ++r) {
@@ -171,6 +194,7 @@ sho_project_tc_kernel(float *__restrict__ apc, float const *__restrict__ x, uint
         }
         ++issued;
     }
+    cp_async_wait0();                                // no copy outstanding when the CTA ends
     int const last = issued - 1;
     if (last >= 0) {
         bool w = ok;
@@ -205,13 +229,15 @@ __global__ void __launch_bounds__(kThreads, 1)
 sho_add_tc_kernel(float *__restrict__ y, float const *__restrict__ cad, uint32_t nrhs,
                   uint16_t const *__restrict__ colIndex, uint32_t const *__restrict__ add_start,
                   uint32_t const *__restrict__ add_col, uint32_t const *__restrict__ add_slot,
-                  double const *__restrict__ slot_H, uint64_t const *__restrict__ slot_mask, int stride,
+                  float const *__restrict__ slot_H, uint64_t const *__restrict__ slot_mask, int stride,
                   int8_t const *__restrict__ img_lmax, uint32_t const *__restrict__ img_starts, int *err)
 {
-    extern __shared__ __align__(1024) char smem[];
-    __shared__ float Hs[2][8][3][4];
+    extern __shared__ __align__(128) char smem[];
+    __shared__ __align__(16) float Hs[2][8][3][4];
     __shared__ ShoIdx sidx[2];
     __shared__ uint64_t mbar[2];
+    __shared__ uint64_t mk[2];
+    __shared__ int lm[2];
     __shared__ uint32_t tmem_base;
     int const tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     uint32_t const b = blockIdx.x;
@@ -227,6 +253,25 @@ sho_add_tc_kernel(float *__restrict__ y, float const *__restrict__ cad, uint32_t
     uint64_t mask_all = 0;
     bool ok = true;
     int issued = 0;                                  // commits issued (block-uniform)
+    float *raw = reinterpret_cast<float*>(smem + 2*kStage);
+    size_t const cstride = size_t(nrhs)*128;
+    // coefficients (nSHO rows of 128 floats), tables and mask of image k go to shared memory
+    // one image ahead
+    auto prefetch = [&](uint32_t k, int st) {
+        uint32_t const a = add_col[k], slot = add_slot[k];
+        int const lmax = img_lmax[a], nsho = ((lmax + 1)*(lmax + 2)*(lmax + 3))/6;
+        float const *src = cad + (size_t(img_starts[a])*nrhs + s)*128;
+        for (int q = tid; q < nsho*32; q += kThreads) {
+            int const row = q >> 5, part = (q & 31)*4;
+            cp_async16(raw + row*128 + part, src + size_t(row)*cstride + part);
+        }
+        if (tid < (lmax + 1)*3) cp_async16(&Hs[st][0][0][0] + tid*4, slot_H + size_t(slot)*stride + tid*4);
+        if (tid == kThreads - 1) cp_async8(&mk[st], slot_mask + slot);
+        fill_sho_index(sidx[st], lmax, tid);
+        if (0 == tid) lm[st] = lmax;
+        cp_async_commit();
+    };
+    prefetch(k0, 0);
     for (uint32_t k = k0; k < k1; ++k) {
         int const it = int(k - k0), st = it & 1;
         char *sA_hi = smem + st*kStage, *sA_lo = sA_hi + kA, *sB_hi = sA_lo + kA, *sB_lo = sB_hi + kB;
@@ -236,15 +281,15 @@ sho_add_tc_kernel(float *__restrict__ y, float const *__restrict__ cad, uint32_t
             ok = __syncthreads_and(w);               // block-uniform decision
             if (!ok) break;
         }
-        uint32_t const a = add_col[k], slot = add_slot[k];
-        int const lmax = img_lmax[a], nsho = ((lmax + 1)*(lmax + 2)*(lmax + 3))/6;
-        fill_sho_index(sidx[st], lmax, tid);
-        if (tid < (lmax + 1)*12) (&Hs[st][0][0][0])[tid] = float(slot_H[size_t(slot)*stride + tid]);
-        uint64_t const mask = slot_mask[slot];
+        cp_async_wait0();                            // coefficients, tables and mask of image k
+        __syncthreads();
+        int const lmax = lm[st], nsho = ((lmax + 1)*(lmax + 2)*(lmax + 3))/6;
+        uint64_t const mask = mk[st];
         mask_all |= mask;
         // A = Cad^T: m = (reim, j), k = sho (rows beyond nsho zero)
-        stage_A(sA_hi, sA_lo, cad + (size_t(img_starts[a])*nrhs + s)*128, 64, size_t(nrhs)*128, nsho, tid);
-        __syncthreads();
+        stage_A(sA_hi, sA_lo, raw, 64, 128, nsho, tid);
+        __syncthreads();                             // raw is free: fetch the next image meanwhile
+        if (k + 1 < k1) prefetch(k + 1, st ^ 1);
         // B = P: n = point i, k = sho; float4 along sho
 #pragma unroll 2
         for (int r = 0; r < 1024/kThreads; ++r) {
@@ -269,6 +314,7 @@ sho_add_tc_kernel(float *__restrict__ y, float const *__restrict__ cad, uint32_t
         }
         ++issued;
     }
+    cp_async_wait0();                                // no copy outstanding when the CTA ends
     int const last = issued - 1;
     if (last >= 0) {
         bool w = ok;
@@ -300,11 +346,22 @@ sho_add_tc_kernel(float *__restrict__ y, float const *__restrict__ cad, uint32_t
 
 } // namespace
 
-bool tc_projector_supported(DevicePlan const &dp) { return dp.lmax_max >= 0 && dp.lmax_max <= 5; }
+namespace { bool g_tc_ready[64] = {}; }   // per device: the kernels got their shared memory
+
+bool tc_projector_supported(DevicePlan const &dp) {
+    int dev = 0;
+    if (cudaSuccess != cudaGetDevice(&dev) || dev < 0 || dev >= 64 || !g_tc_ready[dev]) return false;
+    return dp.lmax_max >= 0 && dp.lmax_max <= 5;
+}
 
 bool prepare_tc_kernels() {
-    A43G_CUDA_TRY(cudaFuncSetAttribute(sho_project_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmem));
-    A43G_CUDA_TRY(cudaFuncSetAttribute(sho_add_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmem));
+    // a device on which the kernels cannot get their shared memory keeps the CUDA-core projector
+    int dev = 0;
+    if (cudaSuccess != cudaGetDevice(&dev) || dev < 0 || dev >= 64) return true;
+    bool const ok = cudaSuccess == cudaFuncSetAttribute(sho_project_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmem) &&
+                    cudaSuccess == cudaFuncSetAttribute(sho_add_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmem);
+    if (!ok) cudaGetLastError();                     // clear the error: the rest of the library is unaffected
+    g_tc_ready[dev] = ok;
     return true;
 }
 
@@ -315,7 +372,7 @@ bool launch_project_tc(DevicePlan &dp, float const *x, cudaStream_t st) {
         dim3 const grid(g.count, dp.nCols);
         sho_project_tc_kernel<<<grid, kThreads, kSmem, st>>>(dptr<float>(dp.apc), x, dp.nCols,
             dptr<uint32_t>(g.images), dp.nAI, dptr<uint32_t>(dp.prj_start), dptr<uint32_t>(dp.prj_col),
-            dptr<uint64_t>(dp.prj_coloff), dptr<uint32_t>(dp.prj_slot), dptr<double>(dp.slot_H),
+            dptr<uint64_t>(dp.prj_coloff), dptr<uint32_t>(dp.prj_slot), dptr<float>(dp.slot_H32),
             dptr<uint64_t>(dp.slot_mask), dp.table_stride, dptr<uint32_t>(dp.img_starts), dptr<int8_t>(dp.img_lmax),
             dptr<int>(dp.dev_error));
         count_launch();
@@ -327,7 +384,7 @@ bool launch_project_tc(DevicePlan &dp, float const *x, cudaStream_t st) {
 bool launch_add_tc(DevicePlan &dp, float *y, uint16_t const *colIndex, cudaStream_t st) {
     sho_add_tc_kernel<<<dp.nnzb, kThreads, kSmem, st>>>(y, dptr<float>(dp.cad), dp.nCols, colIndex,
         dptr<uint32_t>(dp.add_start), dptr<uint32_t>(dp.add_col), dptr<uint32_t>(dp.add_slot),
-        dptr<double>(dp.slot_H), dptr<uint64_t>(dp.slot_mask), dp.table_stride, dptr<int8_t>(dp.img_lmax),
+        dptr<float>(dp.slot_H32), dptr<uint64_t>(dp.slot_mask), dp.table_stride, dptr<int8_t>(dp.img_lmax),
         dptr<uint32_t>(dp.img_starts), dptr<int>(dp.dev_error));
     count_launch();
     A43G_CUDA_TRY(cudaGetLastError());
