@@ -123,3 +123,41 @@ def autotune(plan, precision="float32", stream=0):
     st = ctypes.c_void_p(stream if isinstance(stream, int) else stream.cuda_stream)
     check(_lib.lib().a43g_plan_autotune(plan.handle, _dtype_code(precision), st, buf, len(buf)), "a43g_plan_autotune")
     return buf.value.decode()
+
+
+def solve_concurrent(geometry, V, atom_matrices, atom_offsets, energies, kpoints, dVol, workers=4,
+                     layout="cells", **kw):
+    """Batched solves of many (energy, k-point) pairs of one geometry, several at a time: one plan
+    and one CUDA stream per worker thread (plans are independent, so their solves overlap on the
+    GPU; small cells leave most of the GPU idle in a single solve).  Returns [(stats, rho)] in the
+    order of the pairs."""
+    import threading
+    import torch
+    from . import green_function as gf
+    pairs = list(zip(energies, kpoints))
+    out = [None] * len(pairs)
+    errors = []
+
+    def work(w):
+        try:
+            plan = gf.construct_Green_function(geometry)
+            gf.update_potential(plan, V, atom_matrices, atom_offsets, layout=layout)
+            stream = torch.cuda.Stream()
+            for i in range(w, len(pairs), workers):
+                E, k = pairs[i]
+                gf.update_energy_parameter(plan, E, dVol)
+                gf.update_phases(plan, k)
+                out[i] = solve(plan, stream=stream, **kw)
+            stream.synchronize()
+            plan.close()
+        except Exception as e:          # reported after all workers ended
+            errors.append(e)
+
+    threads = [threading.Thread(target=work, args=(w,)) for w in range(max(1, min(workers, len(pairs))))]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    if errors:
+        raise errors[0]
+    return out

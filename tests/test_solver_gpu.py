@@ -96,3 +96,22 @@ def test_graph_replay_matches_direct_launches(precision):
     assert s0["converged"] and s1["converged"], (s0, s1)
     err = ((X0 - X1).abs().max() / X0.abs().max()).item()
     assert err < 1e-8
+
+
+def test_solve_concurrent_matches_sequential():
+    """Batched solves of several (E, k) pairs on worker plans and streams give the densities of
+    the same solves done one after the other."""
+    w = workloads.make("periodic4_1atom")
+    energies = [complex(-0.3 + 0.05 * i, 0.05 + 0.05 * i) for i in range(6)]
+    kpoints = [np.zeros(3) if i % 2 == 0 else np.array([0.1, 0.0, 0.2]) for i in range(6)]
+    opts = dict(tolerance=1e-10, max_iterations=1500, precision="float64")
+    out = green_action.solve_concurrent(w.geometry, w.Vcell, w.mats, w.offsets, energies, kpoints, w.dVol,
+                                        workers=3, **opts)
+    p = gf.construct_Green_function(w.geometry)
+    gf.update_potential(p, w.Vcell, w.mats, w.offsets, layout="cells")
+    for (st, rho), E, k in zip(out, energies, kpoints):
+        assert st["converged"], st
+        gf.update_energy_parameter(p, E, w.dVol)
+        gf.update_phases(p, k)
+        st0, rho0 = green_action.solve(p, **opts)
+        assert np.abs(rho - rho0).max() <= 1e-8 * np.abs(rho0).max()
