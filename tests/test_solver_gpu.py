@@ -115,3 +115,30 @@ def test_solve_concurrent_matches_sequential():
         gf.update_phases(p, k)
         st0, rho0 = green_action.solve(p, **opts)
         assert np.abs(rho - rho0).max() <= 1e-8 * np.abs(rho0).max()
+
+
+@pytest.mark.parametrize("name", ["iso6_fd16", "mixed_iso_peri_vac", "repeat_aniso", "wrap8"])
+@pytest.mark.parametrize("precision", ["float64", "float32"])
+def test_solve_geometries_true_residual(name, precision):
+    """Solves on every kind of boundary condition and both stencil orders: the true residual of
+    the returned solution, recomputed with the oracle's FP64 action, meets the tolerance."""
+    from helpers import GEOMETRIES, inputs_for, product_plan
+    g = GEOMETRIES[name]()
+    Vc, mats, offs, E, k, dVol, na = inputs_for(g)
+    E = complex(E.real, 0.3)
+    p = product_plan(g, Vc, mats, offs, E, k, dVol)
+    X = torch.zeros((p.nnzb, 2, 64, 64), device="cuda", dtype=torch.float64)
+    stats, _ = green_action.solve(p, X=X, tolerance=1e-9, max_iterations=4000, precision=precision,
+                                  stream=torch.cuda.Stream())
+    assert stats["converged"], stats
+    a = p.export()
+    o = oracle.RestatedOracle(a, Vc, E)
+    Xn = X.cpu().numpy()
+    B = np.zeros_like(Xn)
+    for c, b in enumerate(a["subset"]):
+        B[b, 0][np.arange(64), np.arange(64)] = 1.0
+    R = B - o.action(Xn)
+    Rc = R[:, 0] + 1j * R[:, 1]
+    colres = np.zeros((p.nCols, 64))
+    np.add.at(colres, a["colindx"].astype(np.int64), (np.abs(Rc) ** 2).sum(axis=1))
+    assert np.sqrt(colres.max()) <= 2e-9
