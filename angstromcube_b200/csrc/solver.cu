@@ -261,6 +261,48 @@ __global__ void __launch_bounds__(256) k_DX(TX *X, T *D, T *U1, T const *U2, T c
     }
 }
 
+// K_DX of an FP32 sweep with 16-byte accesses: thread (column group of 4, row group of 4 rows);
+// each row moves 10 float4 loads and 6 float4 stores, and the 12 coefficients of its 4 columns
+// are 12 float4 loads per block
+__device__ __forceinline__ float4 ld4(float const *p) { return *reinterpret_cast<float4 const*>(p); }
+__device__ __forceinline__ void st4(float *p, float4 v) { *reinterpret_cast<float4*>(p) = v; }
+
+__global__ void __launch_bounds__(256, 2) k_DX32(float *X, float *D, float *U1, float const *U2, float const *W,
+                                                 uint32_t nnzb, uint16_t const *colindx, float const *cf, uint32_t ncol) {
+    int const cg = threadIdx.x & 15, rg = threadIdx.x >> 4;
+    int const j0 = cg*4;
+    for (uint32_t b = blockIdx.x; b < nnzb; b += gridDim.x) {
+        uint32_t const col = colindx[b]*64 + j0;
+        float4 const g_r = ld4(cf + 2*size_t(ncol) + col), g_i = ld4(cf + 3*size_t(ncol) + col);
+        float4 const a_r = ld4(cf + 4*size_t(ncol) + col), a_i = ld4(cf + 5*size_t(ncol) + col);
+        float4 const b_r = ld4(cf + 6*size_t(ncol) + col), b_i = ld4(cf + 7*size_t(ncol) + col);
+        float4 const c_r = ld4(cf + 8*size_t(ncol) + col), c_i = ld4(cf + 9*size_t(ncol) + col);
+        float4 const d_r = ld4(cf + 10*size_t(ncol) + col), d_i = ld4(cf + 11*size_t(ncol) + col);
+        float4 const e_r = ld4(cf + 12*size_t(ncol) + col), e_i = ld4(cf + 13*size_t(ncol) + col);
+#pragma unroll 2
+        for (int i = rg*4; i < rg*4 + 4; ++i) {
+            size_t const o = size_t(b)*kBlk + i*64 + j0;
+            float4 const u1r = ld4(U1 + o), u1i = ld4(U1 + o + 4096), u2r = ld4(U2 + o), u2i = ld4(U2 + o + 4096);
+            float4 const dr = ld4(D + o), di = ld4(D + o + 4096), wr = ld4(W + o), wi = ld4(W + o + 4096);
+            float4 xr = ld4(X + o), xi = ld4(X + o + 4096);
+            float4 nd_r, nd_i, nu_r, nu_i;
+#define A43G_DX_LANE(c) \
+            xr.c = fmaf(a_r.c, u1r.c, fmaf(-a_i.c, u1i.c, xr.c)); xi.c = fmaf(a_r.c, u1i.c, fmaf(a_i.c, u1r.c, xi.c)); \
+            xr.c = fmaf(b_r.c, u2r.c, fmaf(-b_i.c, u2i.c, xr.c)); xi.c = fmaf(b_r.c, u2i.c, fmaf(b_i.c, u2r.c, xi.c)); \
+            xr.c = fmaf(c_r.c, dr.c, fmaf(-c_i.c, di.c, xr.c));   xi.c = fmaf(c_r.c, di.c, fmaf(c_i.c, dr.c, xi.c)); \
+            nd_r.c = fmaf(d_r.c, u1r.c, fmaf(-d_i.c, u1i.c, fmaf(e_r.c, dr.c, fmaf(-e_i.c, di.c, u2r.c)))); \
+            nd_i.c = fmaf(d_r.c, u1i.c, fmaf(d_i.c, u1r.c, fmaf(e_r.c, di.c, fmaf(e_i.c, dr.c, u2i.c)))); \
+            nu_r.c = fmaf(g_r.c, u2r.c, fmaf(-g_i.c, u2i.c, wr.c)); \
+            nu_i.c = fmaf(g_r.c, u2i.c, fmaf(g_i.c, u2r.c, wi.c));
+            A43G_DX_LANE(x) A43G_DX_LANE(y) A43G_DX_LANE(z) A43G_DX_LANE(w)
+#undef A43G_DX_LANE
+            st4(X + o, xr); st4(X + o + 4096, xi);
+            st4(D + o, nd_r); st4(D + o + 4096, nd_i);
+            st4(U1 + o, nu_r); st4(U1 + o + 4096, nu_i);
+        }
+    }
+}
+
 // K_E: V = AU1 + beta (AU2 + beta V) ; acc rt^H V
 template <typename T>
 __global__ void __launch_bounds__(256) k_E(T *V, T const *AU1, T const *AU2, uint32_t nnzb,
@@ -592,7 +634,10 @@ bool tfqmr_inner(DevicePlan &dp, SolverWorkspace &ws, TfqmrVectors &v, TX *Xs, d
         count_launch();
         s_half2<<<gs, 256, 0, st>>>(cs, accA, ncol, tol, cnt, stall_level, kStallWindow, cf);
         count_launch();
-        k_DX<T, TX><<<g, 256, 0, st>>>(X, D, U1, U2, W, nnzb, ci, cs, cf, ncol);
+        if constexpr (sizeof(T) == 4 && sizeof(TX) == 4)
+            k_DX32<<<g, 256, 0, st>>>(X, D, U1, U2, W, nnzb, ci, cf, ncol);
+        else
+            k_DX<T, TX><<<g, 256, 0, st>>>(X, D, U1, U2, W, nnzb, ci, cs, cf, ncol);
         count_launch();
         if (!launch_action<T>(dp, AU1, U1, ci, st)) return false;
         k_E<T><<<g, 256, 0, st>>>(V, AU1, AU2, nnzb, ci, cs, accA, seed, cf, ncol);
