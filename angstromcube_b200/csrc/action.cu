@@ -363,6 +363,212 @@ local_fused_pf_kernel(T *__restrict__ y, T const *__restrict__ x,
     }
 }
 
+// Pencil variant (FP32): one CTA per (z-line, slice of S = 32 columns); thread (zq, j) owns the
+// four y-rows (zq, y = 0..3) of every cube of the line for column j, so one warp covers 32
+// consecutive columns of one z-plane (128-byte loads and stores).  The x- and y-stencils run in
+// registers: the x- and y-neighbour rows come straight from global memory (the L2) and are
+// applied in scatter form as they arrive.  Only the z-stencil reads shared memory, where the
+// previous, current and next cube of the line are staged as 16-byte rows, [slot][plane][row][S]
+// (a quarter warp reads 128 contiguous bytes: no bank conflicts).  Per output point this reads
+// half the shared-memory bytes of the row kernel above and passes a barrier a quarter as often.
+// The z-successor of the next cube is requested one step ahead.
+constexpr int kPencilS = 32;
+constexpr int kPencilSmem = 3*2*16*kPencilS*16;   // bytes of the three z-slots
+
+struct Quad { float v[2][16]; };                 // [plane][y*4 + x] of one z-plane of a cube
+
+__device__ __forceinline__ void quad_raw(float const *__restrict__ x, int32_t e, int zq, int col, Quad &q) {
+    if (-1 == e) {
+#pragma unroll
+        for (int i = 0; i < 16; ++i) { q.v[0][i] = 0.f; q.v[1][i] = 0.f; }
+        return;
+    }
+    float const *b = x + size_t(nbr_block(e))*kBlockReals + (zq*16)*64 + col;
+#pragma unroll
+    for (int i = 0; i < 16; ++i) { q.v[0][i] = __ldg(b + i*64); q.v[1][i] = __ldg(b + 4096 + i*64); }
+}
+
+__device__ __forceinline__ void quad_phase(int32_t e, float pr, float pi, Quad &q) {
+    if (e < -1) {
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+            float const a = pr*q.v[0][i] - pi*q.v[1][i], c = pr*q.v[1][i] + pi*q.v[0][i];
+            q.v[0][i] = a; q.v[1][i] = c;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(4*kPencilS, 4)
+local_pencil_kernel(float *__restrict__ y, float const *__restrict__ x,
+                    uint32_t const *__restrict__ zstart, int32_t const *__restrict__ zlist,
+                    int32_t const *__restrict__ nbr, int32_t const *__restrict__ veff,
+                    float const *__restrict__ Vcell, LocalArgs<float> const a)
+{
+    constexpr int S = kPencilS, NSL = 64/S;
+    extern __shared__ __align__(16) float4 slot4[];   // [3][2][16][S]
+    __shared__ int32_t code[kMaxLine][8];              // per step: block, x-, x+, y-, y+, veff, z-next
+    __shared__ int32_t zleft, nline;
+    int const line = blockIdx.x/NSL, slice = blockIdx.x % NSL;
+    int const tid = threadIdx.x, j = tid % S, zq = tid/S, col = slice*S + j;
+    int32_t const *L = zlist + zstart[line];
+    if (0 == tid) {
+        int n = 0;
+        while (L[4 + n] > 0) ++n;                   // lists end with 4 non-positive entries
+        nline = n; zleft = list_code(L[3]);
+    }
+    __syncthreads();
+    int const n = nline;
+    if (0 == n) return;                             // uniform: nothing on this line
+    for (int k = tid; k < n; k += 4*S) {
+        int32_t const b = L[4 + k] - 1;
+        int32_t const *nb = nbr + 6*size_t(b);
+        code[k][0] = b; code[k][1] = nb[0]; code[k][2] = nb[1]; code[k][3] = nb[2]; code[k][4] = nb[3];
+        code[k][5] = veff[b]; code[k][6] = list_code(L[5 + k]);
+    }
+    auto srow = [&](int slot, int pl, int row) -> float4 & { return slot4[((slot*2 + pl)*16 + row)*S + j]; };
+    auto put = [&](int slot, Quad const &q) {
+#pragma unroll
+        for (int yy = 0; yy < 4; ++yy)
+#pragma unroll
+            for (int pl = 0; pl < 2; ++pl)
+                srow(slot, pl, zq*4 + yy) = make_float4(q.v[pl][yy*4], q.v[pl][yy*4 + 1], q.v[pl][yy*4 + 2], q.v[pl][yy*4 + 3]);
+    };
+    float const (&cx)[5] = a.st.c[0];
+    float const (&cy)[5] = a.st.c[1];
+    float const (&cz)[5] = a.st.c[2];
+    float const c0 = cx[0] + cy[0] + cz[0];
+    __syncthreads();                                // code[] complete
+    {
+        Quad h;
+        quad_raw(x, zleft, zq, col, h);
+        quad_phase(zleft, a.ph[2][0][0], a.ph[2][0][1], h);
+        put(0, h);
+        quad_raw(x, code[0][0], zq, col, h);
+        put(1, h);
+    }
+    Quad nx;                                        // rows of the z-successor, one step ahead
+    quad_raw(x, code[0][6], zq, col, nx);
+    int sp = 0, sc = 1, sn = 2;
+    for (int k = 0; k < n; ++k) {
+        int32_t const b = code[k][0];
+        quad_phase(code[k][6], a.ph[2][1][0], a.ph[2][1][1], nx);   // only the line end has a phase
+        __syncthreads();                            // the previous step finished reading slot sn
+        put(sn, nx);
+        __syncthreads();
+        if (k + 1 < n) quad_raw(x, code[k + 1][6], zq, col, nx);   // arrives during this step
+        Quad cur;
+#pragma unroll
+        for (int yy = 0; yy < 4; ++yy)
+#pragma unroll
+            for (int pl = 0; pl < 2; ++pl) {
+                float4 const v = srow(sc, pl, zq*4 + yy);
+                cur.v[pl][yy*4] = v.x; cur.v[pl][yy*4 + 1] = v.y; cur.v[pl][yy*4 + 2] = v.z; cur.v[pl][yy*4 + 3] = v.w;
+            }
+        float acc[2][16];
+        // potential and centre
+        int32_t const iloc = code[k][5];
+        float V[16];
+        if (iloc < 0) {
+#pragma unroll
+            for (int i = 0; i < 16; ++i) V[i] = 0.f;
+        } else {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                float4 const v = __ldg(reinterpret_cast<float4 const*>(Vcell + size_t(iloc)*64 + zq*16 + q*4));
+                V[q*4] = v.x; V[q*4 + 1] = v.y; V[q*4 + 2] = v.z; V[q*4 + 3] = v.w;
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+            float const Vt = V[i] - a.E_re;
+            acc[0][i] = Vt*cur.v[0][i] + a.E_im*cur.v[1][i] + c0*cur.v[0][i];
+            acc[1][i] = Vt*cur.v[1][i] - a.E_im*cur.v[0][i] + c0*cur.v[1][i];
+        }
+        // y-stencil inside the cube
+#pragma unroll
+        for (int pl = 0; pl < 2; ++pl)
+#pragma unroll
+            for (int yy = 0; yy < 4; ++yy)
+#pragma unroll
+                for (int yo = 0; yo < 4; ++yo) {
+                    if (yo == yy) continue;
+                    int const d = (yo > yy) ? yo - yy : yy - yo;
+#pragma unroll
+                    for (int i = 0; i < 4; ++i) acc[pl][yy*4 + i] += cy[d]*cur.v[pl][yo*4 + i];
+                }
+        // x-stencil: the rows of the x-neighbours at (zq, yy)
+#pragma unroll
+        for (int yy = 0; yy < 4; ++yy) {
+            Rows<float> xm, xp;
+            row_raw(x, code[k][1], zq*4 + yy, col, xm);
+            row_raw(x, code[k][2], zq*4 + yy, col, xp);
+            row_phase(code[k][1], a.ph[0][0][0], a.ph[0][0][1], xm);
+            row_phase(code[k][2], a.ph[0][1][0], a.ph[0][1][1], xp);
+            float lr[12], li[12];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                lr[i] = xm.re[i]; li[i] = xm.im[i];
+                lr[4 + i] = cur.v[0][yy*4 + i]; li[4 + i] = cur.v[1][yy*4 + i];
+                lr[8 + i] = xp.re[i]; li[8 + i] = xp.im[i];
+            }
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int d = 1; d <= 4; ++d) {
+                    acc[0][yy*4 + i] += cx[d]*(lr[4 + i - d] + lr[4 + i + d]);
+                    acc[1][yy*4 + i] += cx[d]*(li[4 + i - d] + li[4 + i + d]);
+                }
+        }
+        // y-neighbour cubes: row yo of y- sits at y = yo - 4, row yo of y+ at y = yo + 4
+#pragma unroll
+        for (int yo = 0; yo < 4; ++yo) {
+            Rows<float> ym, yp;
+            row_raw(x, code[k][3], zq*4 + yo, col, ym);
+            row_raw(x, code[k][4], zq*4 + yo, col, yp);
+            row_phase(code[k][3], a.ph[1][0][0], a.ph[1][0][1], ym);
+            row_phase(code[k][4], a.ph[1][1][0], a.ph[1][1][1], yp);
+#pragma unroll
+            for (int yy = 0; yy < 4; ++yy) {
+                if (yy <= yo) {
+#pragma unroll
+                    for (int i = 0; i < 4; ++i) {
+                        acc[0][yy*4 + i] += cy[yy - yo + 4]*ym.re[i];
+                        acc[1][yy*4 + i] += cy[yy - yo + 4]*ym.im[i];
+                    }
+                }
+                if (yy >= yo) {
+#pragma unroll
+                    for (int i = 0; i < 4; ++i) {
+                        acc[0][yy*4 + i] += cy[yo + 4 - yy]*yp.re[i];
+                        acc[1][yy*4 + i] += cy[yo + 4 - yy]*yp.im[i];
+                    }
+                }
+            }
+        }
+        // z-stencil from the three staged cubes (previous, current, next)
+#pragma unroll
+        for (int yy = 0; yy < 4; ++yy)
+#pragma unroll
+            for (int d = 1; d <= 4; ++d) {
+                int const zm = zq - d, zp = zq + d;
+                int const s_m = (zm < 0) ? sp : sc, s_p = (zp > 3) ? sn : sc;
+                int const r_m = (zm & 3)*4 + yy, r_p = (zp & 3)*4 + yy;
+#pragma unroll
+                for (int pl = 0; pl < 2; ++pl) {
+                    float4 const m = srow(s_m, pl, r_m), p = srow(s_p, pl, r_p);
+                    acc[pl][yy*4 + 0] += cz[d]*(m.x + p.x);
+                    acc[pl][yy*4 + 1] += cz[d]*(m.y + p.y);
+                    acc[pl][yy*4 + 2] += cz[d]*(m.z + p.z);
+                    acc[pl][yy*4 + 3] += cz[d]*(m.w + p.w);
+                }
+            }
+        float *yb = y + size_t(b)*kBlockReals + (zq*16)*64 + col;
+#pragma unroll
+        for (int i = 0; i < 16; ++i) { yb[i*64] = acc[0][i]; yb[4096 + i*64] = acc[1][i]; }
+        int const t = sp; sp = sc; sc = sn; sn = t;  // rotate the z-slots
+    }
+}
+
 // ---------------------------------------------------------------- generic local path
 
 // y = (V - E) x for every block (include/green_potential.hxx:15-139, collinear)
@@ -717,6 +923,12 @@ void launch_project_L(DevicePlan &dp, T const *x, cudaStream_t st) {
 
 } // namespace
 
+bool prepare_local_kernels() {
+    // the pencil kernel's three z-slots are 48 KB of dynamic shared memory beside its static part
+    A43G_CUDA_TRY(cudaFuncSetAttribute(local_pencil_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kPencilSmem));
+    return true;
+}
+
 template <typename T>
 bool launch_local(DevicePlan &dp, T *y, T const *x, cudaStream_t st) {
     if (0 == dp.nnzb) return true;
@@ -727,6 +939,16 @@ bool launch_local(DevicePlan &dp, T *y, T const *x, cudaStream_t st) {
         for (int d = 0; d < 3; ++d) for (int s = 0; s < 2; ++s) for (int c = 0; c < 2; ++c) a.ph[d][s][c] = T(dp.phase[d][s][c]);
         constexpr int S = (sizeof(T) == 8) ? 8 : 16;
         unsigned const nblk = dp.nlists[2]*(64/S);
+        if constexpr (sizeof(T) == 4) {
+            if (dp.nlists[2] && dp.max_zline <= kMaxLine && 2 == dp.local_variant) {
+                local_pencil_kernel<<<dp.nlists[2]*(64/kPencilS), 4*kPencilS, kPencilSmem, st>>>(y, x,
+                    dptr<uint32_t>(dp.lists_start[2]), dptr<int32_t>(dp.lists[2]), dptr<int32_t>(dp.nbr),
+                    dptr<int32_t>(dp.veff_index), vcell<T>(dp), a);
+                count_launch();
+                A43G_CUDA_TRY(cudaGetLastError());
+                return true;
+            }
+        }
         if (nblk && sizeof(T) == 4 && dp.max_zline <= kMaxLine && 0 == dp.local_variant) {
             local_fused_pf_kernel<T, S><<<nblk, S*16, 0, st>>>(y, x, dptr<uint32_t>(dp.lists_start[2]),
                 dptr<int32_t>(dp.lists[2]), dptr<int32_t>(dp.nbr), dptr<int32_t>(dp.veff_index), vcell<T>(dp), a);

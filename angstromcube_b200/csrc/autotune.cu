@@ -6,7 +6,8 @@
 //                   schedule of the projection: longer chunks amortize the pipeline start and
 //                   the coefficient atomics, shorter ones balance the load)   {8, 16, 32}
 //   * add_blocks  : consecutive blocks per CTA of the FP32 addition        {8, 16, 32}
-//   * local_variant: local kernel with one-step-ahead loads or the plain one {0, 1}
+//   * local_variant: FP32 local kernel on rows with one-step-ahead loads, on plain rows, or on
+//                   y-pencils                                                  {0, 1, 2}
 //   * use_tc      : FP32 projector on the tensor cores (3xTF32) or on the CUDA cores
 // Each parameter is tuned in turn (coordinate descent), every candidate timed with CUDA events
 // on the caller's stream: two untimed applications, then the mean of three.  Scratch vectors
@@ -95,18 +96,21 @@ bool autotune(GreenPlan const &hp, DevicePlan &dp, cudaStream_t st, std::string 
             }
         }
     }
+    char const *const local_name[3] = {"rows with loads ahead", "plain rows", "pencils"};
     if (sizeof(T) == 4 && dp.fused_local) {
-        float t[2] = {0, 0};
-        for (int v = 0; v < 2; ++v) {
+        float t[3] = {0, 0, 0};
+        int best = 0;
+        for (int v = 0; v < 3; ++v) {
             dp.local_variant = v;
             if (!time_part<T>(dp, 0, y, x, ci, st, t[v])) return false;
-            std::snprintf(line, sizeof(line), "local kernel %s: %.3f ms\n", v ? "plain" : "with loads ahead", t[v]);
+            std::snprintf(line, sizeof(line), "local kernel, %s: %.3f ms\n", local_name[v], t[v]);
             report += line;
+            if (t[v] < t[best]) best = v;
         }
-        dp.local_variant = (t[1] < t[0]) ? 1 : 0;
+        dp.local_variant = best;
     }
     std::snprintf(line, sizeof(line), "chosen: projector chunk %u, addition %u blocks per CTA, local %s, %s projector\n",
-                  dp.prj_chunk, dp.add_blocks, dp.local_variant ? "plain" : "with loads ahead",
+                  dp.prj_chunk, dp.add_blocks, local_name[dp.local_variant],
                   dp.use_tc ? "tensor-core" : "CUDA-core");
     report += line;
     A43G_CUDA_TRY(cudaStreamSynchronize(st));

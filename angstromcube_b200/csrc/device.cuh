@@ -47,7 +47,7 @@ struct DevicePlan {
     // schedule parameters, set by the autotuner (autotune.cu) or left at these defaults
     uint32_t prj_chunk = 16;         // blocks per projection work item
     uint32_t add_blocks = 16;        // blocks per CTA of the FP32 addition
-    int local_variant = 0;           // 0: local kernel with one-step-ahead loads, 1: plain
+    int local_variant = 2;           // FP32: 0 rows with one-step-ahead loads, 1 plain rows, 2 pencils
     uint32_t nlists[3] = {0, 0, 0};
 
     DeviceBuffer veff_index;     // int32 [nnzb]
@@ -85,6 +85,7 @@ struct DevicePlan {
 bool upload_plan(GreenPlan const &hp, DevicePlan &dp);
 // kernel attributes (dynamic shared memory above 48 KB) of the current device
 bool prepare_simt_kernels();
+bool prepare_local_kernels();
 bool prepare_tc_kernels();
 // kernel launch counter: n launches at once (replays of a captured graph)
 void count_launches(uint64_t n);

@@ -67,7 +67,7 @@ std::vector<int32_t> neighbour_table(GreenPlan const &hp) {
 } // namespace
 
 bool upload_plan(GreenPlan const &hp, DevicePlan &dp) {
-    if (!prepare_simt_kernels() || !prepare_tc_kernels()) return false;
+    if (!prepare_simt_kernels() || !prepare_tc_kernels() || !prepare_local_kernels()) return false;
     dp.nnzb = uint32_t(hp.nnzb()); dp.nRows = hp.nRows; dp.nCols = hp.nCols;
     dp.nAtoms = hp.nAtoms; dp.nAI = hp.nAtomImages;
     dp.ncoeffI = uint32_t(hp.ncoeff_images()); dp.ncoeffA = uint32_t(hp.ncoeff_atoms());
@@ -146,6 +146,9 @@ bool upload_plan(GreenPlan const &hp, DevicePlan &dp) {
         // FP32 projector: SIMT (default) or the tensor cores ("tc"); the FP64 path is always SIMT
         char const *e = std::getenv("A43G_PROJECTOR");
         dp.use_tc = (e && 0 == std::strcmp(e, "tc"));
+        // FP32 local kernel: y-"pencils" (default), "rows" with loads ahead or "plain" rows
+        char const *l = std::getenv("A43G_LOCAL");
+        dp.local_variant = (l && 0 == std::strcmp(l, "plain")) ? 1 : ((l && 0 == std::strcmp(l, "rows")) ? 0 : 2);
     }
     if (!dp.aac.alloc(std::max<size_t>(16, size_t(dp.ncoeffA)*dp.nCols*128*sizeof(double)))) return false;
     if (!dp.cadd.alloc(std::max<size_t>(16, size_t(dp.ncoeffA)*dp.nCols*128*sizeof(double)))) return false;

@@ -344,8 +344,15 @@ def measure_kernels(a, plan, w, stream, out, hbm, bf16, peak_kind):
     t_local = time_part(_lib, plan, 0, _lib.A43G_F32, x, y, 20, stream)
     bytes_local = 2*nnzb*8192*4 + plan.sizes["ncells"]*64*4 + nnzb*(7*4) + plan.sizes["lists_nnz2"]*4
     ach = bytes_local/t_local/1e9
-    traffic = read_traffic("local_fused_pf_kernel_f32")
-    out["roofline"] = {"kernel": "local_fused_pf_kernel<float,16> (potential + 8th-order kinetic, one pass)",
+    chosen = " ".join(out.get("autotune", []))
+    if "local pencils" in chosen:
+        kname, tkey = "local_pencil_kernel (FP32 y-pencils: potential + 8th-order kinetic, one pass)", "local_pencil_kernel_f32"
+    elif "local plain rows" in chosen:
+        kname, tkey = "local_fused_kernel<float,16> (potential + 8th-order kinetic, one pass)", None
+    else:
+        kname, tkey = "local_fused_pf_kernel<float,16> (potential + 8th-order kinetic, one pass)", "local_fused_pf_kernel_f32"
+    traffic = read_traffic(tkey) if tkey else None
+    out["roofline"] = {"kernel": kname,
                        "bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach/hbm,
                        "peak_kind": peak_kind, "algorithmic_bytes_per_launch": bytes_local,
                        "ms_per_launch": t_local*1e3,
