@@ -173,41 +173,46 @@ sho_project_simt_kernel(T *__restrict__ apc, T const *__restrict__ x, uint32_t n
 // ---------------------------------------------------------------- addition
 
 // contribution of one image with basis size L to the 64 point sums of this thread
-// ZS threads share a column and split its z-planes (FP64: the 64 sums of one thread would not
-// fit the registers); each computes the x and y stages in full and its planes zh*(4/ZS) ...
+// ZS threads share a column and split its x-points (FP64: the 64 sums of one thread would not
+// fit the registers): thread zh owns x = zh*(4/ZS) ... of every (z, y) row, so each stage of
+// the contraction (x, then y, then z) is split between them without repeating any work.  The
+// sums are ordered acc[(z*4 + y)*(4/ZS) + x - zh*(4/ZS)].
 template <typename T, int L, bool FULL, int ZS>
 __device__ __forceinline__ void add_image(T (&acc)[64/ZS], Tables<T, L> const &t, uint64_t mask,
                                           T const *__restrict__ c, size_t cstride, int zh) {
     constexpr int kUnrollZ = (8 == sizeof(T)) ? 1 : L + 1;     // FP64: one z-order at a time (registers)
+    constexpr int NX = 4/ZS;                                   // x-points of this thread
+    int const x0 = (1 == ZS) ? 0 : zh*NX;
     int sho = 0;
 #pragma unroll kUnrollZ
     for (int iz = 0; iz <= L; ++iz) {
-        T byx[16];
+        T byx[4*NX];
 #pragma unroll
-        for (int i = 0; i < 16; ++i) byx[i] = T(0);
+        for (int i = 0; i < 4*NX; ++i) byx[i] = T(0);
 #pragma unroll
         for (int iy = 0; iy <= L - iz; ++iy) {
-            T ax[4] = {T(0), T(0), T(0), T(0)};
+            T ax[NX];
+#pragma unroll
+            for (int xl = 0; xl < NX; ++xl) ax[xl] = T(0);
 #pragma unroll
             for (int ix = 0; ix <= L - iz - iy; ++ix, ++sho) {
                 T const cv = c[size_t(sho)*cstride];
 #pragma unroll
-                for (int xx = 0; xx < 4; ++xx) ax[xx] = fmat(t(ix, 0, xx), cv, ax[xx]);
+                for (int xl = 0; xl < NX; ++xl) ax[xl] = fmat(t(ix, 0, x0 + xl), cv, ax[xl]);
             }
 #pragma unroll
             for (int yy = 0; yy < 4; ++yy) {
                 T const hy = t(iy, 1, yy);
 #pragma unroll
-                for (int xx = 0; xx < 4; ++xx) byx[yy*4 + xx] = fmat(hy, ax[xx], byx[yy*4 + xx]);
+                for (int xl = 0; xl < NX; ++xl) byx[yy*NX + xl] = fmat(hy, ax[xl], byx[yy*NX + xl]);
             }
         }
 #pragma unroll
-        for (int zz = 0; zz < 4/ZS; ++zz) {
-            int const z = zh*(4/ZS) + zz;
+        for (int z = 0; z < 4; ++z) {
             T const hz = t(iz, 2, z);
 #pragma unroll
-            for (int q = 0; q < 16; ++q) {
-                int const p = z*16 + q, pl = zz*16 + q;
+            for (int q = 0; q < 4*NX; ++q) {
+                int const pl = z*4*NX + q, p = z*16 + (q/NX)*4 + x0 + (q % NX);
                 if (FULL) acc[pl] = fmat(hz, byx[q], acc[pl]);
                 else acc[pl] = ((mask >> p) & 1u) ? fmat(hz, byx[q], acc[pl]) : acc[pl];
             }
@@ -325,7 +330,7 @@ sho_add_simt_kernel(T *__restrict__ y, T const *__restrict__ cad, uint32_t nrhs,
             T *yb = y + size_t(bb)*kBlk + reim*4096 + j;
 #pragma unroll
             for (int pl = 0; pl < NP; ++pl) {
-                int const p = zh*NP + pl;                  // this thread's points
+                int const p = (pl/(4/ZS))*4 + zh*(4/ZS) + pl % (4/ZS);   // this thread's points
                 if ((mask_all >> p) & 1u) yb[p*64] = yb_s[p*64] + acc[pl];
                 acc[pl] = T(0);
             }
