@@ -230,6 +230,17 @@ def read_traffic(kernel):
     return None
 
 
+def local_kernel_of(tune_lines):
+    """Name of the FP32 local kernel the autotuner chose (from its "chosen: ..." line) and the key
+    of its DRAM traffic in profiles/traffic.txt (None where no capture exists)."""
+    chosen = " ".join(tune_lines)
+    if "local pencils" in chosen:
+        return "local_pencil_kernel (FP32 y-pencils: potential + 8th-order kinetic, one pass)", "local_pencil_kernel_f32"
+    if "local plain rows" in chosen:
+        return "local_fused_kernel<float,16> (potential + 8th-order kinetic, one pass)", None
+    return "local_fused_pf_kernel<float,16> (potential + 8th-order kinetic, one pass)", "local_fused_pf_kernel_f32"
+
+
 def our_arm(a):
     import numpy as np
     import torch
@@ -350,13 +361,7 @@ def measure_kernels(a, plan, w, stream, out, hbm, bf16, peak_kind):
     t_local = time_part(_lib, plan, 0, _lib.A43G_F32, x, y, 20, stream)
     bytes_local = 2*nnzb*8192*4 + plan.sizes["ncells"]*64*4 + nnzb*(7*4) + plan.sizes["lists_nnz2"]*4
     ach = bytes_local/t_local/1e9
-    chosen = " ".join(out.get("autotune", []))
-    if "local pencils" in chosen:
-        kname, tkey = "local_pencil_kernel (FP32 y-pencils: potential + 8th-order kinetic, one pass)", "local_pencil_kernel_f32"
-    elif "local plain rows" in chosen:
-        kname, tkey = "local_fused_kernel<float,16> (potential + 8th-order kinetic, one pass)", None
-    else:
-        kname, tkey = "local_fused_pf_kernel<float,16> (potential + 8th-order kinetic, one pass)", "local_fused_pf_kernel_f32"
+    kname, tkey = local_kernel_of(out.get("autotune", []))
     traffic = read_traffic(tkey) if tkey else None
     out["roofline"] = {"kernel": kname,
                        "bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach/hbm,
