@@ -1,9 +1,9 @@
 // The action without any device allocation (a43g_action_multiply_noalloc).
 //
-// Some callers cannot let a library call cudaMalloc: code that runs while a CUDA graph is being
-// captured (an allocation there is not allowed), hosts that hand out all device memory through
-// their own pool and forbid allocations behind their back, and latency-bound loops where the
-// device-wide synchronization of cudaMalloc/cudaFree would stall other streams.  The ordinary
+// Some callers cannot let a library call cudaMalloc: hosts that hand out all device memory
+// through their own pool and forbid allocations behind their back, processes that have already
+// claimed nearly all of the GPU's memory, and latency-bound loops where the device-wide
+// synchronization of cudaMalloc/cudaFree would stall other streams.  The ordinary
 // a43g_action_multiply allocates the projector coefficient scratch of a plan on its first call;
 // this variant keeps that scratch in one fixed array in device memory instead, compiled into the
 // library: kScratchBytes (16 MiB) on every GPU that loads the library, held until the process

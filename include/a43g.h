@@ -128,8 +128,8 @@ int a43g_action_multiply(a43g_plan_t *plan, void *y, const void *x, const uint16
 
 /* ---- the same action without any device allocation.  No counterpart in the reference (its
  * action allocates its projector scratch on every call).  For callers that must not let a
- * library allocate device memory: work recorded into a CUDA graph, hosts whose memory pool owns
- * all device memory, loops that cannot afford the device-wide synchronization of cudaMalloc.
+ * library allocate device memory: hosts whose memory pool owns all device memory, loops that
+ * cannot afford the device-wide synchronization of cudaMalloc.
  * The projector coefficients live in one fixed 16 MiB array compiled into the library (present
  * on every GPU that loads it until the process exits); plans that need more are rejected with
  * A43G_ERR_UNSUPPORTED.  The plan must already be current on the calling device

@@ -1,5 +1,6 @@
 """The allocation-free action (a43g_action_multiply_noalloc), for callers that cannot let the
-library allocate device memory (graph capture, externally owned memory pools): two calls in a
+library allocate device memory (hosts whose own pool owns the GPU's memory, loops that cannot
+take the synchronization of cudaMalloc): two calls in a
 row agree with a43g_action_multiply on the same inputs, within the tolerances of the action
 tests (1e-12 relative in FP64, 3e-5 in FP32); plans needing more than the fixed scratch, and
 plans not yet current on the device, are refused with an error.  This file is collected last."""
