@@ -13,6 +13,10 @@
 // the projection accumulates into is zeroed by each call; everything else is overwritten before
 // it is read.  Calls whose GPU work overlaps (on different streams, from different threads or
 // for different plans) therefore race on the array and must be serialized by the caller.
+//
+// The device address of the array is looked up once per device and kept.  A cudaDeviceReset
+// destroys the context that holds the array; the kept address is then stale, so this entry point
+// must not be used on a device after the caller has reset it.
 #include "device.cuh"
 #include "noalloc.hpp"
 

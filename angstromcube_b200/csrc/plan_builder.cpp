@@ -80,7 +80,8 @@ std::string GreenPlan::build(Geometry const &g) {
         off[d] = (int32_t(n_blocks[d]) - nsrc[d])/2;
     }
     size_t const nrhs = size_t(nsrc[X])*nsrc[Y]*nsrc[Z];
-    if (nrhs > 65536) return "at most 65536 source cubes (uint16 column indices)";
+    // uint16 column indices, and the per-column kernels launch one CTA row per source (CUDA grid y <= 65535)
+    if (nrhs > 65535) return "at most 65535 source cubes (uint16 column indices, CUDA grid y limit)";
     nCols = uint32_t(nrhs);
     source_coords.resize(3*nrhs);
     {

@@ -9,7 +9,8 @@ parameter and a k-point.  The numbers follow the workloads the benchmarks are qu
   periodic16_64atoms   16^3 cubes, periodic, 64 Gaussians, 64 atoms on a 4^3 lattice with
                        +-0.3 Bohr jitter, numax 5 sigma 0.6, 4x4x1 source cubes, r_trunc 12,
                        E = -0.2 + 0.02i
-  wrapped32_256atoms   32^3 cubes, truncation sphere fits (wrapped), 256 atoms, 4x4x2 sources
+  wrapped32_256atoms   32^3 cubes, truncation sphere fits (wrapped), 256 atoms on an 8x8x4
+                       lattice over the whole cell with +-0.3 Bohr jitter, 4x4x2 sources, r_trunc 12
 plus scaled-down variants used by the tests.  Potentials are periodic sums over minimum
 images; atom matrices are real symmetric with N(0, 0.1) entries, the overlap part shifted to
 be positive definite, then multiplied by the SHO prefactors (the caller-side rescaling of
@@ -147,9 +148,10 @@ def make(name, seed=0):
         L = ng[0] * h
         centres = rng.uniform(-L / 2, L / 2, size=(256, 3))
         Vc, _ = _potential_cells(ng, (h,) * 3, centres, -1.0, 1.5, 1e-3, rng)
-        m = 8; a = L / m
-        grid = (np.arange(m) + 0.5) * a - L / 2
-        pos = np.array(np.meshgrid(grid, grid, grid[:4], indexing="ij")).reshape(3, -1).T
+        # 8 x 8 x 4 sites over the whole cell (4 Bohr apart in x and y, 8 Bohr in z)
+        gxy = (np.arange(8) + 0.5) * (L / 8) - L / 2
+        gz = (np.arange(4) + 0.5) * (L / 4) - L / 2
+        pos = np.array(np.meshgrid(gxy, gxy, gz, indexing="ij")).reshape(3, -1).T
         pos = pos + rng.uniform(-0.3, 0.3, size=pos.shape)
         natoms = len(pos)
         atoms = np.zeros((natoms, 8))

@@ -135,8 +135,10 @@ int a43g_action_multiply(a43g_plan_t *plan, void *y, const void *x, const uint16
  * A43G_ERR_UNSUPPORTED.  The plan must already be current on the calling device
  * (a43g_plan_upload after the last change of potential, matrices, energy or k-point), else
  * A43G_ERR_STATE.  The first call on each device looks up the array's device address; make it
- * before any stream capture.  All calls on a device share the array: calls whose GPU work
- * overlaps race on it and must be serialized by the caller.  Arguments as a43g_action_multiply. */
+ * before any stream capture.  The looked-up address is kept for the life of the process, so the
+ * entry point must not be used on a device after a cudaDeviceReset of it.  All calls on a device
+ * share the array: calls whose GPU work overlaps race on it and must be serialized by the caller.
+ * Arguments as a43g_action_multiply. */
 int a43g_action_multiply_noalloc(a43g_plan_t *plan, void *y, const void *x, const uint16_t *colIndex,
                                  uint32_t nnzb, uint32_t nCols, void *stream, int dtype, double *flops);
 

@@ -72,6 +72,31 @@ def test_action_matches_reference_build():
     assert rel_err(apply(p, x, np.float32), r.action(x.astype(np.float32)).astype(np.float64)) < FP32_TOL
 
 
+@pytest.mark.parametrize("kpoint", [(0.0, 0.0, 0.0), (0.125, -0.25, 1 / 3.0)])
+def test_benchmark_cell_matches_reference_build(kpoint):
+    """The benchmark cell itself (periodic 16^3 cubes, 64 atoms numax 5 sigma 0.6, its potential,
+    atom matrices and energy E = -0.2 + 0.02i) with one source cube (4,096 blocks), against the
+    reference's action_t<double,2,1>::multiply on identical inputs: FP64 and FP32 actions."""
+    if not oracle.ref_available():
+        pytest.skip("oracle/_ref not built")
+    w = workloads.make("periodic16_64atoms_s1x1x1")
+    k = np.array(kpoint)
+    r = oracle.RefGreen(w.geometry)
+    r.set_potential(w.Vcell)
+    r.set_atom_matrices(w.mats, w.offsets)
+    r.set_energy(w.E, w.dVol)
+    r.set_kpoint(k)
+    p = gf.construct_Green_function(w.geometry)
+    gf.update_potential(p, w.Vcell, w.mats, w.offsets, layout="cells")
+    gf.update_energy_parameter(p, w.E, w.dVol)
+    gf.update_phases(p, k)
+    assert p.nnzb == r.sizes["nnzb"] == 4096
+    x = np.random.default_rng(21).standard_normal((p.nnzb, 2, 64, 64))
+    y_ref = r.action(x)
+    assert rel_err(apply(p, x, np.float64), y_ref) < FP64_TOL
+    assert rel_err(apply(p, x, np.float32), y_ref) < FP32_TOL
+
+
 def test_action_mid_size_workload():
     w = workloads.make("periodic8_8atoms_s2x2x1")
     p = gf.construct_Green_function(w.geometry)

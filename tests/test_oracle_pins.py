@@ -111,8 +111,6 @@ def test_action_matches_golden():
 @pytest.mark.parametrize("name", sorted(GEOMETRIES))
 def test_restated_action_matches_reference(name):
     g = GEOMETRIES[name]()
-    if np.prod(np.array(g.ng) // 4) > 300:
-        pytest.skip("large cell, covered on the GPU side")
     Vc, mats, offs, E, k, dVol, na = inputs_for(g)
     ref = reference_plan(g, Vc, mats, offs, E, k, dVol)
     o = oracle.RestatedOracle(ref.export(), Vc, E)

@@ -42,6 +42,22 @@ def test_plan_matches_reference_workloads(name):
     compare(ref.export(), pl.export())
 
 
+@needs_ref
+@pytest.mark.parametrize("name", ["periodic16_64atoms", "periodic16_64atoms_s1x1x1", "wrapped32_256atoms"])
+def test_plan_matches_reference_benchmark_cells(name):
+    """The benchmark cells themselves: the dense periodic 16^3-cube cell with 64 atoms (16 and
+    one source cubes) and the wrapped 32^3-cube cell with 256 atoms and 32 source cubes
+    (300,960 blocks, the truncation sphere with the 8/27-corner test of the reference's
+    default build)."""
+    w = workloads.make(name)
+    ref = oracle.RefGreen(w.geometry)
+    pl = gf.construct_Green_function(w.geometry)
+    assert ref.sizes["nnzb"] == pl.sizes["nnzb"]
+    if name == "wrapped32_256atoms":
+        assert pl.sizes["nnzb"] == 300960 and pl.sizes["nCols"] == 32
+    compare(ref.export(), pl.export())
+
+
 def test_plan_matches_golden():
     """Committed plan arrays generated by the reference (tests/golden/make_golden.py)."""
     path = os.path.join(GOLDEN, "plan_wrap6.npz")
@@ -68,6 +84,14 @@ def test_dense_periodic_sizes():
     assert pl.sizes["nnzb"] == 16 ** 3 * 16
     assert pl.sizes["nRows"] == 16 ** 3 and pl.sizes["nCols"] == 16
     assert pl.sizes["FD_range0"] == 4
+
+
+def test_source_count_limit():
+    """65535 source cubes are the most a plan takes (uint16 column indices, one CTA row per
+    source in the per-column kernels): 65536 are refused when the plan is built."""
+    g = workloads.Geometry((4 * 256, 4 * 256, 4), (1, 1, 1), (0.25,) * 3, 0.5, (-1, -1, -1))
+    with pytest.raises(RuntimeError, match="65535"):
+        gf.construct_Green_function(g)
 
 
 def test_invalid_geometry_is_an_error():

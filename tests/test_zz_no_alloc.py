@@ -49,6 +49,31 @@ def test_noalloc_matches_multiply_twice(name, dtype):
         assert rel_err(y.double().cpu().numpy(), y_ref.double().cpu().numpy()) < TOL[dtype]
 
 
+def test_noalloc_allocates_nothing():
+    """After a first call (which loads the library's device code and looks up the array), further
+    calls leave the device's free memory and the torch caching allocator's reservation unchanged."""
+    g = GEOMETRIES["wrap8"]()
+    Vc, mats, offs, E, k, dVol, na = inputs_for(g)
+    p = product_plan(g, Vc, mats, offs, E, k, dVol)
+    p.upload()
+    ci = torch.from_numpy(p.export()["colindx"].astype(np.int16)).cuda()
+    x = torch.randn((p.nnzb, 2, 64, 64), device="cuda", dtype=torch.float64)
+    y = torch.empty_like(x)
+    x32, y32 = x.float(), torch.empty((p.nnzb, 2, 64, 64), device="cuda", dtype=torch.float32)
+    for xx, yy, code in ((x, y, _lib.A43G_F64), (x32, y32, _lib.A43G_F32)):
+        assert noalloc(p, yy, xx, ci, code)[0] == 0, _lib.lib().a43g_last_error()
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    reserved0 = torch.cuda.memory_reserved()
+    for _ in range(3):
+        for xx, yy, code in ((x, y, _lib.A43G_F64), (x32, y32, _lib.A43G_F32)):
+            assert noalloc(p, yy, xx, ci, code)[0] == 0, _lib.lib().a43g_last_error()
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0
+    assert torch.cuda.memory_reserved() == reserved0
+
+
 def test_noalloc_refuses_large_and_stale_plans():
     g = GEOMETRIES["wrap8_fd16_numax5"]()            # about 74 MB of FP64 projector scratch
     Vc, mats, offs, E, k, dVol, na = inputs_for(g)
