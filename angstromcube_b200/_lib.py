@@ -50,17 +50,21 @@ class PlanExport(ctypes.Structure):
                 [(n, ctypes.c_void_p) for n in _EXPORT_NAMES2])
 
 
+A43G_SOLVE_NO_RETIRE = 1
+
+
 class SolveOptions(ctypes.Structure):
     _fields_ = [("tolerance", ctypes.c_double), ("max_iterations", ctypes.c_int32), ("precision", ctypes.c_int32),
-                ("inner_tolerance", ctypes.c_double), ("max_refinements", ctypes.c_int32),
-                ("check_every", ctypes.c_int32), ("seed", ctypes.c_uint64), ("echo", ctypes.c_int32)]
+                ("update_factor", ctypes.c_double), ("update_gap", ctypes.c_int32),
+                ("check_every", ctypes.c_int32), ("seed", ctypes.c_uint64), ("echo", ctypes.c_int32),
+                ("flags", ctypes.c_int32), ("batch", ctypes.c_int32), ("pad", ctypes.c_int32)]
 
 
 class SolveStats(ctypes.Structure):
     _fields_ = [("iterations", ctypes.c_int32), ("refinements", ctypes.c_int32), ("converged", ctypes.c_int32),
                 ("breakdowns", ctypes.c_int32), ("residual_max", ctypes.c_double),
                 ("residual_estimate", ctypes.c_double), ("operator_applications", ctypes.c_double),
-                ("seconds", ctypes.c_double)]
+                ("seconds", ctypes.c_double), ("fp64_sources", ctypes.c_int32), ("pad", ctypes.c_int32)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

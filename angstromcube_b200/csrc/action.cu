@@ -36,12 +36,38 @@ Stencil9<T> make_stencil9(DevicePlan const &dp) {
     return s;
 }
 
+// energy and Bloch phases of one (energy, k-point) pair of a batch plan
+template <typename T>
+struct PairArgs { T E_re, E_im; T ph[3][2][2]; };
+
 template <typename T>
 struct LocalArgs {
     Stencil9<T> st;
     T E_re, E_im;
     T ph[3][2][2];                   // Bloch phases [dd][left,right][re,im]
+    PairArgs<T> const *pairs;        // batch plan: per-pair values (nullptr: the values above)
+    uint16_t const *colindx;         // block -> source column (batch plans and retirement)
+    uint8_t const *active;           // per-source flag: 0 = retired, skip (nullptr: all active)
+    uint32_t nsrc_pair;              // sources per pair
 };
+
+// the values of the pair that owns block b (uniform over a CTA that works on one z-line: the
+// lines of a batch plan never mix sources); false if b's source is retired
+template <typename T>
+__device__ __forceinline__ bool line_args(LocalArgs<T> &a, int32_t b) {
+    if (!a.colindx) return true;
+    uint32_t const s = a.colindx[b];
+    if (a.active && !a.active[s]) return false;
+    if (a.pairs) {
+        PairArgs<T> const &q = a.pairs[s/a.nsrc_pair];
+        a.E_re = q.E_re; a.E_im = q.E_im;
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+#pragma unroll
+            for (int u = 0; u < 2; ++u) { a.ph[d][u][0] = q.ph[d][u][0]; a.ph[d][u][1] = q.ph[d][u][1]; }
+    }
+    return true;
+}
 
 // 4 consecutive points (x = 0..3 of one (z, y) row) of one column from shared memory
 template <typename T> struct Row4 { T v[4]; };
@@ -119,7 +145,7 @@ __global__ void __launch_bounds__(S*16)
 local_fused_kernel(T *__restrict__ y, T const *__restrict__ x,
                    uint32_t const *__restrict__ zstart, int32_t const *__restrict__ zlist,
                    int32_t const *__restrict__ nbr, int32_t const *__restrict__ veff,
-                   T const *__restrict__ Vcell, LocalArgs<T> const a)
+                   T const *__restrict__ Vcell, LocalArgs<T> a)
 {
     constexpr int NSL = 64/S, PAD = 68;
     __shared__ __align__(16) T sm[5][2][S][PAD];   // slots: 3 rotating z-slots, y-, y+
@@ -129,6 +155,7 @@ local_fused_kernel(T *__restrict__ y, T const *__restrict__ x,
     int32_t const *L = zlist + zstart[line];
     int n = 0;
     while (L[4 + n] > 0) ++n;        // lists end with 4 non-positive entries
+    if (0 == n || !line_args(a, L[4] - 1)) return;           // uniform over the CTA
     T const (&cx)[5] = a.st.c[0];
     T const (&cy)[5] = a.st.c[1];
     T const (&cz)[5] = a.st.c[2];
@@ -247,7 +274,7 @@ __global__ void __launch_bounds__(S*16, 2)
 local_fused_pf_kernel(T *__restrict__ y, T const *__restrict__ x,
                       uint32_t const *__restrict__ zstart, int32_t const *__restrict__ zlist,
                       int32_t const *__restrict__ nbr, int32_t const *__restrict__ veff,
-                      T const *__restrict__ Vcell, LocalArgs<T> const a)
+                      T const *__restrict__ Vcell, LocalArgs<T> a)
 {
     constexpr int NSL = 64/S, PAD = 68;
     __shared__ __align__(16) T sm[5][2][S][PAD];   // slots: 3 rotating z-slots, y-, y+
@@ -264,7 +291,7 @@ local_fused_pf_kernel(T *__restrict__ y, T const *__restrict__ x,
     }
     __syncthreads();
     int const n = nline;
-    if (0 == n) return;                             // uniform: nothing on this line
+    if (0 == n || !line_args(a, L[4] - 1)) return;  // uniform: nothing on this line, or retired
     for (int k = tid; k < n; k += S*16) {
         int32_t const b = L[4 + k] - 1;
         int32_t const *nb = nbr + 6*size_t(b);
@@ -402,7 +429,7 @@ __global__ void __launch_bounds__(4*kPencilS, 4)
 local_pencil_kernel(float *__restrict__ y, float const *__restrict__ x,
                     uint32_t const *__restrict__ zstart, int32_t const *__restrict__ zlist,
                     int32_t const *__restrict__ nbr, int32_t const *__restrict__ veff,
-                    float const *__restrict__ Vcell, LocalArgs<float> const a)
+                    float const *__restrict__ Vcell, LocalArgs<float> a)
 {
     constexpr int S = kPencilS, NSL = 64/S;
     extern __shared__ __align__(16) float4 slot4[];   // [3][2][16][S]
@@ -418,7 +445,7 @@ local_pencil_kernel(float *__restrict__ y, float const *__restrict__ x,
     }
     __syncthreads();
     int const n = nline;
-    if (0 == n) return;                             // uniform: nothing on this line
+    if (0 == n || !line_args(a, L[4] - 1)) return;  // uniform: nothing on this line, or retired
     for (int k = tid; k < n; k += 4*S) {
         int32_t const b = L[4 + k] - 1;
         int32_t const *nb = nbr + 6*size_t(b);
@@ -575,9 +602,12 @@ local_pencil_kernel(float *__restrict__ y, float const *__restrict__ x,
 template <typename T>
 __global__ void __launch_bounds__(256)
 potential_kernel(T *__restrict__ y, T const *__restrict__ x, int32_t const *__restrict__ veff,
-                 T const *__restrict__ Vcell, uint32_t nnzb, T Er, T Ei)
+                 T const *__restrict__ Vcell, uint32_t nnzb, LocalArgs<T> const a0)
 {
     for (uint32_t b = blockIdx.x; b < nnzb; b += gridDim.x) {
+        LocalArgs<T> a = a0;
+        if (!line_args(a, int32_t(b))) continue;          // uniform: the CTA works on block b
+        T const Er = a.E_re, Ei = a.E_im;
         int32_t const iloc = veff[b];
         T const *xb = x + size_t(b)*kBlockReals;
         T *yb = y + size_t(b)*kBlockReals;
@@ -599,8 +629,8 @@ struct Coef17 { T c[9]; };
 template <typename T, int NH>
 __global__ void __launch_bounds__(64)
 kinetic_list_kernel(T *__restrict__ y, T const *__restrict__ x, uint32_t const *__restrict__ lstart,
-                    int32_t const *__restrict__ lists, int stride, Coef17<T> const coef,
-                    T plr, T pli, T prr, T pri)
+                    int32_t const *__restrict__ lists, int stride, Coef17<T> const coef, int dd,
+                    LocalArgs<T> a)
 {
     constexpr int W = 4*(2*NH + 1);   // window points: NH cubes left, current, NH right
     constexpr int R = 4*NH;           // stencil reach in points
@@ -609,6 +639,8 @@ kinetic_list_kernel(T *__restrict__ y, T const *__restrict__ x, uint32_t const *
     int32_t const *L = lists + lstart[blockIdx.x];
     int n = 0;
     while (L[4 + n] > 0) ++n;
+    if (0 == n || !line_args(a, L[4] - 1)) return;      // uniform: empty list, or a retired source
+    T const plr = a.ph[dd][0][0], pli = a.ph[dd][0][1], prr = a.ph[dd][1][0], pri = a.ph[dd][1][1];
     T c[R + 1];
 #pragma unroll
     for (int k = 0; k <= R; ++k) c[k] = coef.c[k];
@@ -747,14 +779,25 @@ sho_project_kernel(T *__restrict__ apc, T const *__restrict__ x, uint32_t nrhs,
 
 // aac[(a0 + c)*nrhs + s] = sum over the images i of atom A of phase_i * apc[(i0 + c)*nrhs + s]
 // (collect) in double (include/green_dyadic.hxx:600-702).  Grid (nAtoms, nrhs), 64 threads.
+// per-source selection of the pair values of a batch plan (image phases and atom matrices
+// stored [pair][...]) and the retirement flags (nullptr: every source active)
+struct DyadicPairs {
+    uint32_t nsrc_pair;              // sources per pair (= nrhs for a one-pair plan)
+    size_t img_stride, mat_stride;   // doubles per pair of img_phase and of the atom matrices
+    uint8_t const *active;
+};
+
 template <typename T>
 __global__ void __launch_bounds__(64)
 sho_collect_kernel(double *__restrict__ aac, T const *__restrict__ apc, uint32_t nrhs,
                    uint32_t const *__restrict__ atom_starts, int8_t const *__restrict__ atom_lmax,
                    uint32_t const *__restrict__ sum_start, uint32_t const *__restrict__ sum_col,
-                   uint32_t const *__restrict__ img_starts, double const *__restrict__ img_phase)
+                   uint32_t const *__restrict__ img_starts, double const *__restrict__ img_phase,
+                   DyadicPairs const bp)
 {
     int const A = blockIdx.x, s = blockIdx.y, j = threadIdx.x;
+    if (bp.active && !bp.active[s]) return;
+    img_phase += (s/bp.nsrc_pair)*bp.img_stride;
     int const nc = nsho_c(atom_lmax[A]);
     size_t const a0 = atom_starts[A];
     for (int c = 0; c < nc; ++c) {
@@ -778,9 +821,11 @@ template <typename Tin, typename Tout>
 __global__ void __launch_bounds__(64)
 sho_mul_kernel(Tout *__restrict__ out, Tin const *__restrict__ in, uint32_t nrhs,
                uint32_t const *__restrict__ atom_starts, int8_t const *__restrict__ atom_lmax,
-               double const *__restrict__ mats, uint32_t const *__restrict__ mat_off)
+               double const *__restrict__ mats, uint32_t const *__restrict__ mat_off, DyadicPairs const bp)
 {
     int const A = blockIdx.x, s = blockIdx.y, j = threadIdx.x;
+    if (bp.active && !bp.active[s]) return;
+    mats += (s/bp.nsrc_pair)*bp.mat_stride;
     int const nc = nsho_c(atom_lmax[A]);
     size_t const a0 = atom_starts[A];
     double const *Mr = mats + mat_off[A], *Mi = Mr + nc*nc;
@@ -816,9 +861,12 @@ __global__ void __launch_bounds__(64)
 sho_broadcast_kernel(T *__restrict__ cad, double const *__restrict__ cadd, uint32_t nrhs,
                      uint32_t const *__restrict__ atom_starts, int8_t const *__restrict__ atom_lmax,
                      uint32_t const *__restrict__ sum_start, uint32_t const *__restrict__ sum_col,
-                     uint32_t const *__restrict__ img_starts, double const *__restrict__ img_phase)
+                     uint32_t const *__restrict__ img_starts, double const *__restrict__ img_phase,
+                     DyadicPairs const bp)
 {
     int const A = blockIdx.x, s = blockIdx.y, j = threadIdx.x;
+    if (bp.active && !bp.active[s]) return;
+    img_phase += (s/bp.nsrc_pair)*bp.img_stride;
     int const nc = nsho_c(atom_lmax[A]);
     size_t const a0 = atom_starts[A];
     for (uint32_t k = sum_start[A]; k < sum_start[A + 1]; ++k) {
@@ -905,6 +953,15 @@ sho_add_kernel(T *__restrict__ y, T const *__restrict__ cad, uint32_t nrhs, uint
     for (int p = 0; p < 64; ++p) if ((mask_all >> p) & 1) yb[p*64] += acc[p];
 }
 
+DyadicPairs dyadic_pairs(DevicePlan const &dp) {
+    DyadicPairs bp;
+    bp.nsrc_pair = dp.nsrc_pair ? dp.nsrc_pair : std::max(1u, dp.nCols);
+    bp.img_stride = (dp.npairs > 1) ? size_t(dp.nAI)*4 : 0;
+    bp.mat_stride = (dp.npairs > 1) ? dp.mat_stride : 0;
+    bp.active = dp.retire ? dptr<uint8_t>(dp.src_active) : nullptr;
+    return bp;
+}
+
 template <typename T> T const *vcell(DevicePlan &dp);
 template <> double const *vcell<double>(DevicePlan &dp) { return dptr<double>(dp.Vcell64); }
 template <> float const *vcell<float>(DevicePlan &dp) { return dptr<float>(dp.Vcell32); }
@@ -929,14 +986,27 @@ bool prepare_local_kernels() {
     return true;
 }
 
+// kernel arguments of the local part: stencil, energy and phases of a one-pair plan, or the
+// per-pair table of a batch plan; the source flags when some sources are retired
+template <typename T>
+LocalArgs<T> local_args(DevicePlan const &dp) {
+    LocalArgs<T> a;
+    a.st = make_stencil9<T>(dp);
+    a.E_re = T(dp.E_re); a.E_im = T(dp.E_im);
+    for (int d = 0; d < 3; ++d) for (int s = 0; s < 2; ++s) for (int c = 0; c < 2; ++c) a.ph[d][s][c] = T(dp.phase[d][s][c]);
+    bool const batch = dp.npairs > 1;
+    a.pairs = batch ? dptr<PairArgs<T>>(sizeof(T) == 8 ? dp.pair_args64 : dp.pair_args32) : nullptr;
+    a.active = dp.retire ? dptr<uint8_t>(dp.src_active) : nullptr;
+    a.colindx = (batch || a.active) ? dptr<uint16_t>(dp.colindx) : nullptr;
+    a.nsrc_pair = dp.nsrc_pair ? dp.nsrc_pair : dp.nCols;
+    return a;
+}
+
 template <typename T>
 bool launch_local(DevicePlan &dp, T *y, T const *x, cudaStream_t st) {
     if (0 == dp.nnzb) return true;
+    LocalArgs<T> a = local_args<T>(dp);
     if (dp.fused_local) {
-        LocalArgs<T> a;
-        a.st = make_stencil9<T>(dp);
-        a.E_re = T(dp.E_re); a.E_im = T(dp.E_im);
-        for (int d = 0; d < 3; ++d) for (int s = 0; s < 2; ++s) for (int c = 0; c < 2; ++c) a.ph[d][s][c] = T(dp.phase[d][s][c]);
         constexpr int S = (sizeof(T) == 8) ? 8 : 16;
         unsigned const nblk = dp.nlists[2]*(64/S);
         if constexpr (sizeof(T) == 4) {
@@ -960,14 +1030,11 @@ bool launch_local(DevicePlan &dp, T *y, T const *x, cudaStream_t st) {
         }
     } else {
         unsigned const nb = std::min<uint32_t>(dp.nnzb, 148u*16);
-        potential_kernel<T><<<nb, 256, 0, st>>>(y, x, dptr<int32_t>(dp.veff_index), vcell<T>(dp), dp.nnzb,
-                                                T(dp.E_re), T(dp.E_im));
+        potential_kernel<T><<<nb, 256, 0, st>>>(y, x, dptr<int32_t>(dp.veff_index), vcell<T>(dp), dp.nnzb, a);
         count_launch();
         for (int d = 0; d < 3; ++d) {
             int const nFD = dp.FD_range[d];
             if (nFD < 1 || 0 == dp.nlists[d]) continue;
-            T const pl_r = T(dp.phase[d][0][0]), pl_i = T(dp.phase[d][0][1]);
-            T const pr_r = T(dp.phase[d][1][0]), pr_i = T(dp.phase[d][1][1]);
             dim3 const grid(dp.nlists[d], 16);
             // 8th order {-14350, 8064, -1008, 128, -9}/5040 or 16th order
             // {-924708642, 538137600, -94174080, 22830080, -5350800, 1053696, -156800, 15360, -735}/302702400,
@@ -983,9 +1050,9 @@ bool launch_local(DevicePlan &dp, T *y, T const *x, cudaStream_t st) {
                 for (int k = 0; k < 9; ++k) coef.c[k] = T(k < 5 ? w[k]*norm : 0.0);
             }
             if (8 == nFD) kinetic_list_kernel<T, 2><<<grid, 64, 0, st>>>(y, x, dptr<uint32_t>(dp.lists_start[d]),
-                              dptr<int32_t>(dp.lists[d]), 1 << (2*d), coef, pl_r, pl_i, pr_r, pr_i);
+                              dptr<int32_t>(dp.lists[d]), 1 << (2*d), coef, d, a);
             else kinetic_list_kernel<T, 1><<<grid, 64, 0, st>>>(y, x, dptr<uint32_t>(dp.lists_start[d]),
-                              dptr<int32_t>(dp.lists[d]), 1 << (2*d), coef, pl_r, pl_i, pr_r, pr_i);
+                              dptr<int32_t>(dp.lists[d]), 1 << (2*d), coef, d, a);
             count_launch();
         }
     }
@@ -1017,18 +1084,18 @@ bool launch_dyadic(DevicePlan &dp, T *y, T const *x, uint16_t const *colIndex, c
     if (dp.nAI > dp.nAtoms) {
         sho_collect_kernel<T><<<ga, 64, 0, st>>>(dptr<double>(dp.aac), dptr<T>(dp.apc), dp.nCols,
             dptr<uint32_t>(dp.atom_starts), dptr<int8_t>(dp.atom_lmax), dptr<uint32_t>(dp.sum_start),
-            dptr<uint32_t>(dp.sum_col), dptr<uint32_t>(dp.img_starts), dptr<double>(dp.img_phase));
+            dptr<uint32_t>(dp.sum_col), dptr<uint32_t>(dp.img_starts), dptr<double>(dp.img_phase), dyadic_pairs(dp));
         count_launch();
         sho_mul_kernel<double, double><<<ga, 64, 0, st>>>(dptr<double>(dp.cadd), dptr<double>(dp.aac), dp.nCols,
-            dptr<uint32_t>(dp.atom_starts), dptr<int8_t>(dp.atom_lmax), dptr<double>(dp.atom_mat), dptr<uint32_t>(dp.atom_mat_off));
+            dptr<uint32_t>(dp.atom_starts), dptr<int8_t>(dp.atom_lmax), dptr<double>(dp.atom_mat), dptr<uint32_t>(dp.atom_mat_off), dyadic_pairs(dp));
         count_launch();
         sho_broadcast_kernel<T><<<ga, 64, 0, st>>>(dptr<T>(dp.cad), dptr<double>(dp.cadd), dp.nCols,
             dptr<uint32_t>(dp.atom_starts), dptr<int8_t>(dp.atom_lmax), dptr<uint32_t>(dp.sum_start),
-            dptr<uint32_t>(dp.sum_col), dptr<uint32_t>(dp.img_starts), dptr<double>(dp.img_phase));
+            dptr<uint32_t>(dp.sum_col), dptr<uint32_t>(dp.img_starts), dptr<double>(dp.img_phase), dyadic_pairs(dp));
         count_launch();
     } else {
         sho_mul_kernel<T, T><<<ga, 64, 0, st>>>(dptr<T>(dp.cad), dptr<T>(dp.apc), dp.nCols,
-            dptr<uint32_t>(dp.atom_starts), dptr<int8_t>(dp.atom_lmax), dptr<double>(dp.atom_mat), dptr<uint32_t>(dp.atom_mat_off));
+            dptr<uint32_t>(dp.atom_starts), dptr<int8_t>(dp.atom_lmax), dptr<double>(dp.atom_mat), dptr<uint32_t>(dp.atom_mat_off), dyadic_pairs(dp));
         count_launch();
     }
     if (tc) {
@@ -1087,7 +1154,7 @@ bool launch_collect_with(DevicePlan &dp, double *aac, double const *apc, double 
     dim3 const ga(dp.nAtoms, dp.nCols);
     sho_collect_kernel<double><<<ga, 64, 0, st>>>(aac, apc, dp.nCols, dptr<uint32_t>(dp.atom_starts),
         dptr<int8_t>(dp.atom_lmax), dptr<uint32_t>(dp.sum_start), dptr<uint32_t>(dp.sum_col),
-        dptr<uint32_t>(dp.img_starts), img_phase);
+        dptr<uint32_t>(dp.img_starts), img_phase, dyadic_pairs(dp));
     count_launch();
     A43G_CUDA_TRY(cudaGetLastError());
     return true;
@@ -1096,7 +1163,7 @@ bool launch_collect_with(DevicePlan &dp, double *aac, double const *apc, double 
 bool launch_mul_with(DevicePlan &dp, double *out, double const *in, cudaStream_t st) {
     dim3 const ga(dp.nAtoms, dp.nCols);
     sho_mul_kernel<double, double><<<ga, 64, 0, st>>>(out, in, dp.nCols, dptr<uint32_t>(dp.atom_starts),
-        dptr<int8_t>(dp.atom_lmax), dptr<double>(dp.atom_mat), dptr<uint32_t>(dp.atom_mat_off));
+        dptr<int8_t>(dp.atom_lmax), dptr<double>(dp.atom_mat), dptr<uint32_t>(dp.atom_mat_off), dyadic_pairs(dp));
     count_launch();
     A43G_CUDA_TRY(cudaGetLastError());
     return true;
@@ -1114,18 +1181,18 @@ bool launch_action_scratch(DevicePlan &dp, T *y, T const *x, uint16_t const *col
     if (dp.nAI > dp.nAtoms) {
         sho_collect_kernel<T><<<ga, 64, 0, st>>>(sc.aac, apc, dp.nCols,
             dptr<uint32_t>(dp.atom_starts), dptr<int8_t>(dp.atom_lmax), dptr<uint32_t>(dp.sum_start),
-            dptr<uint32_t>(dp.sum_col), dptr<uint32_t>(dp.img_starts), dptr<double>(dp.img_phase));
+            dptr<uint32_t>(dp.sum_col), dptr<uint32_t>(dp.img_starts), dptr<double>(dp.img_phase), dyadic_pairs(dp));
         count_launch();
         sho_mul_kernel<double, double><<<ga, 64, 0, st>>>(sc.cadd, sc.aac, dp.nCols,
-            dptr<uint32_t>(dp.atom_starts), dptr<int8_t>(dp.atom_lmax), dptr<double>(dp.atom_mat), dptr<uint32_t>(dp.atom_mat_off));
+            dptr<uint32_t>(dp.atom_starts), dptr<int8_t>(dp.atom_lmax), dptr<double>(dp.atom_mat), dptr<uint32_t>(dp.atom_mat_off), dyadic_pairs(dp));
         count_launch();
         sho_broadcast_kernel<T><<<ga, 64, 0, st>>>(cad, sc.cadd, dp.nCols,
             dptr<uint32_t>(dp.atom_starts), dptr<int8_t>(dp.atom_lmax), dptr<uint32_t>(dp.sum_start),
-            dptr<uint32_t>(dp.sum_col), dptr<uint32_t>(dp.img_starts), dptr<double>(dp.img_phase));
+            dptr<uint32_t>(dp.sum_col), dptr<uint32_t>(dp.img_starts), dptr<double>(dp.img_phase), dyadic_pairs(dp));
         count_launch();
     } else {
         sho_mul_kernel<T, T><<<ga, 64, 0, st>>>(cad, apc, dp.nCols,
-            dptr<uint32_t>(dp.atom_starts), dptr<int8_t>(dp.atom_lmax), dptr<double>(dp.atom_mat), dptr<uint32_t>(dp.atom_mat_off));
+            dptr<uint32_t>(dp.atom_starts), dptr<int8_t>(dp.atom_lmax), dptr<double>(dp.atom_mat), dptr<uint32_t>(dp.atom_mat_off), dyadic_pairs(dp));
         count_launch();
     }
     sho_add_kernel<T><<<dp.nnzb, 128, 0, st>>>(y, cad, dp.nCols, dp.nnzb, colIndex,

@@ -15,6 +15,7 @@ struct a43g_plan {
     a43g::GreenPlan host;
     a43g::DevicePlan dev;
     a43g::SolverWorkspace solver;
+    a43g::BatchCache batch;          // batch plan and vectors of a43g_solve_batched
     a43g::VjpWorkspace vjpws;
     bool energy_set = false;
     bool matrices_set = false;
@@ -331,7 +332,7 @@ int a43g_solve_batched(a43g_plan_t *plan, const a43g_solve_options_t *opts, int3
     if (!plan->matrices_set && plan->host.nAtoms > 0) return fail(A43G_ERR_STATE, "atom matrices not set");
     int const rc = ensure_device(plan);
     if (rc) return rc;
-    return a43g::solve_batched(plan->host, plan->dev, plan->solver, *opts, n, energies, kpoints, dVol,
+    return a43g::solve_batched(plan->host, plan->dev, plan->batch, *opts, n, energies, kpoints, dVol,
                                rho, stats, (cudaStream_t)stream);
 }
 

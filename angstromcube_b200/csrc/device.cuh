@@ -74,7 +74,22 @@ struct DevicePlan {
     struct ImageGroup { uint32_t count = 0; DeviceBuffer images; } img_group[8];  // images by basis size
     // SIMT projection work items by basis size: (image, source, first, last) list positions,
     // each at most kPrjChunk blocks, so that long block lists are spread over many CTAs
-    struct PrjItems { uint32_t count = 0; DeviceBuffer items; } prj_items[8];
+    // items8 adds the item's group (the items of one (image, source) pair): first item, count,
+    // group index, first partial-sum slot; tickets[group] counts finished items (deterministic
+    // fixed-order sum of the partials by the last one, projector_simt.cu)
+    struct PrjItems { uint32_t count = 0, part_items = 0; DeviceBuffer items, items8, tickets; } prj_items[8];
+    DeviceBuffer prj_part;       // partial projection sums of multi-item groups
+    // batch plans (GreenPlan::replicate): npairs (energy, k-point) pairs of nsrc_pair sources each
+    uint32_t npairs = 1, nsrc_pair = 0;
+    size_t mat_stride = 0;       // doubles of atom matrices per pair
+    DeviceBuffer pair_args32, pair_args64;   // per pair: E_re, E_im, phases [3][2][2] (float, double)
+    // retirement: sources whose columns have all finished are skipped by every kernel of the
+    // action and of the solver while retire is set (uint8 per source, 1 = active)
+    bool retire = false;
+    DeviceBuffer src_active;
+    // the blocks of every source in order (the solver's fixed-order column reductions)
+    DeviceBuffer src_start, src_blocks;      // uint32 [nCols + 1], uint32 [nnzb]
+    uint32_t max_src_blocks = 0;
     // scratch of the dyadic part (allocated once per plan, never per call)
     DeviceBuffer apc;            // real_t [ncoeffI*nCols][2][64] image projection coefficients
     DeviceBuffer aac, cadd;      // double [ncoeffA*nCols][2][64]
@@ -97,6 +112,8 @@ bool build_prj_items(GreenPlan const &hp, DevicePlan &dp);
 template <typename T>
 bool autotune(GreenPlan const &hp, DevicePlan &dp, cudaStream_t st, std::string &report);
 bool ensure_dyadic_scratch(DevicePlan &dp, size_t elem_bytes);
+// partial-sum buffer of the deterministic SIMT projection for reals of elem_bytes
+bool ensure_prj_part(DevicePlan &dp, size_t elem_bytes);
 
 // the action y = (H - E S) x on real_t = double or float
 template <typename T>

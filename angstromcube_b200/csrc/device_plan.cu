@@ -141,6 +141,21 @@ bool upload_plan(GreenPlan const &hp, DevicePlan &dp) {
         if (!put(dp.add_info, info)) return false;
     }
     if (!put(dp.subset_dev, hp.subset)) return false;
+    {   // blocks of every source, in block order
+        std::vector<uint32_t> start(hp.nCols + 1, 0), blocks(hp.nnzb());
+        for (size_t b = 0; b < hp.nnzb(); ++b) ++start[hp.colindx[b] + 1];
+        for (uint32_t c = 0; c < hp.nCols; ++c) start[c + 1] += start[c];
+        std::vector<uint32_t> fill(start.begin(), start.end() - 1);
+        for (size_t b = 0; b < hp.nnzb(); ++b) blocks[fill[hp.colindx[b]]++] = uint32_t(b);
+        dp.max_src_blocks = 0;
+        for (uint32_t c = 0; c < hp.nCols; ++c) dp.max_src_blocks = std::max(dp.max_src_blocks, start[c + 1] - start[c]);
+        if (!put(dp.src_start, start) || !put(dp.src_blocks, blocks)) return false;
+        if (!put(dp.src_active, std::vector<uint8_t>(std::max<size_t>(hp.nCols, 1), uint8_t(1)))) return false;
+        dp.retire = false;
+    }
+    dp.npairs = hp.npairs;
+    dp.nsrc_pair = (hp.npairs > 1) ? hp.nsrc_pair : hp.nCols;
+    dp.mat_stride = hp.AtomMatrices.size();
     if (!put(dp.dev_error, std::vector<int32_t>(4, 0))) return false;
     {
         // FP32 projector: SIMT (default) or the tensor cores ("tc"); the FP64 path is always SIMT
@@ -159,31 +174,64 @@ bool upload_plan(GreenPlan const &hp, DevicePlan &dp) {
 
 bool build_prj_items(GreenPlan const &hp, DevicePlan &dp) {
     uint32_t const chunk = std::max<uint32_t>(1, dp.prj_chunk);
-    std::vector<uint32_t> items[8];
+    std::vector<uint32_t> items[8], items8[8];
+    uint32_t groups[8] = {0}, parts[8] = {0};
     for (uint32_t s = 0; s < hp.nCols; ++s) {
         auto const &c = hp.SHOprj[s];
         if (c.start.empty()) continue;
         for (uint32_t a = 0; a < hp.nAtomImages; ++a) {
             int const L = hp.AtomImageLmax[a];
-            for (uint32_t k = c.start[a]; k < c.start[a + 1]; k += chunk) {
-                uint32_t const it[4] = {a, s, k, std::min(k + chunk, c.start[a + 1])};
+            uint32_t const k0 = c.start[a], k1 = c.start[a + 1];
+            if (k0 >= k1) continue;
+            uint32_t const n = (k1 - k0 + chunk - 1)/chunk, first = uint32_t(items[L].size()/4);
+            uint32_t const part = (n > 1) ? parts[L] : 0u;
+            for (uint32_t k = k0; k < k1; k += chunk) {
+                uint32_t const it[4] = {a, s, k, std::min(k + chunk, k1)};
                 items[L].insert(items[L].end(), it, it + 4);
+                uint32_t const it8[8] = {a, s, k, std::min(k + chunk, k1), first, n, groups[L], part};
+                items8[L].insert(items8[L].end(), it8, it8 + 8);
             }
+            ++groups[L];
+            if (n > 1) parts[L] += n;
         }
     }
     for (int L = 0; L < 8; ++L) {
-        dp.prj_items[L].count = uint32_t(items[L].size()/4);
-        if (!put(dp.prj_items[L].items, items[L])) return false;
+        auto &g = dp.prj_items[L];
+        g.count = uint32_t(items[L].size()/4);
+        g.part_items = parts[L];
+        if (!put(g.items, items[L]) || !put(g.items8, items8[L])) return false;
+        if (!put(g.tickets, std::vector<uint32_t>(std::max<uint32_t>(groups[L], 1), 0u))) return false;
     }
     return true;
+}
+
+bool ensure_prj_part(DevicePlan &dp, size_t elem_bytes) {
+    size_t n = 16;
+    for (int L = 0; L < 8; ++L)
+        n = std::max(n, size_t(dp.prj_items[L].part_items)*size_t(((L + 1)*(L + 2)*(L + 3))/6)*128*elem_bytes);
+    return dp.prj_part.alloc(n);
 }
 
 bool upload_values(GreenPlan const &hp, DevicePlan &dp) {
     if (!put(dp.Vcell64, hp.Vcell)) return false;
     std::vector<float> v32(hp.Vcell.begin(), hp.Vcell.end());
     if (!put(dp.Vcell32, v32)) return false;
-    if (!put(dp.atom_mat, hp.AtomMatrices)) return false;
-    if (!put(dp.img_phase, hp.AtomImagePhase)) return false;
+    if (hp.npairs > 1) {
+        // batch plan: image phases and atom matrices [pair][...], energies and phases per pair
+        if (!put(dp.atom_mat, hp.pair_mats)) return false;
+        if (!put(dp.img_phase, hp.pair_img_phase)) return false;
+        std::vector<double> a64(14*size_t(hp.npairs));
+        std::vector<float> a32(14*size_t(hp.npairs));
+        for (uint32_t p = 0; p < hp.npairs; ++p) {
+            a64[14*p] = hp.pair_E[2*p]; a64[14*p + 1] = hp.pair_E[2*p + 1];
+            for (int k = 0; k < 12; ++k) a64[14*p + 2 + k] = hp.pair_phase[12*size_t(p) + k];
+        }
+        for (size_t k = 0; k < a64.size(); ++k) a32[k] = float(a64[k]);
+        if (!put(dp.pair_args64, a64) || !put(dp.pair_args32, a32)) return false;
+    } else {
+        if (!put(dp.atom_mat, hp.AtomMatrices)) return false;
+        if (!put(dp.img_phase, hp.AtomImagePhase)) return false;
+    }
     std::memcpy(dp.phase, hp.phase, sizeof(dp.phase));
     dp.E_re = hp.E_re; dp.E_im = hp.E_im;
     dp.values_dirty = false;

@@ -106,6 +106,14 @@ struct GreenPlan {
     double E_re = 0, E_im = 0;
     std::vector<double> Vcell;                 // [ncells][64]
 
+    // batch of independent (energy, k-point) pairs on one geometry (replicate): the sources of
+    // pair p are s + p*nsrc_pair, every pair has its own energy, phases and atom matrices
+    uint32_t npairs = 1, nsrc_pair = 0;        // nsrc_pair = nCols / npairs
+    std::vector<double> pair_E;                // [npairs][2]
+    std::vector<double> pair_phase;            // [npairs][3][2][2]
+    std::vector<double> pair_img_phase;        // [npairs][nAI][4]
+    std::vector<double> pair_mats;             // [npairs][AtomMatrices.size()]
+
     size_t nnzb() const { return colindx.size(); }
     size_t ncells() const { return size_t(n_blocks[0])*n_blocks[1]*n_blocks[2]; }
     size_t ncoeff_images() const { return AtomImageStarts.empty() ? 0 : AtomImageStarts.back(); }
@@ -126,6 +134,11 @@ struct GreenPlan {
     // slot_H with the functions of direction dir replaced by their derivative with respect to
     // the atom position (vector-Jacobian products; the reference has no derivatives)
     std::vector<double> position_derivative_tables(int dir) const;
+    // this plan as npairs copies of the one-pair plan `one` (same geometry, potential and atom
+    // matrices; no reference counterpart: the reference solves its (E, k) points one by one)
+    std::string replicate(GreenPlan const &one, uint32_t npairs);
+    // energy and k-point of pair p of a replicated plan (the one-pair set_energy/set_kpoint)
+    std::string set_pair(uint32_t p, double Er, double Ei, double dVol, double const k[3]);
 };
 
 // set_phase (src/kinetic_plan.cxx:214-269): returns the deviation of the purified values

@@ -612,3 +612,122 @@ std::vector<double> GreenPlan::position_derivative_tables(int dir) const {
 }
 
 } // namespace a43g
+
+namespace a43g {
+
+// Batch plan: npairs copies of the one-pair plan `one`.  Every row r keeps its target cube; its
+// blocks are those of `one` repeated once per pair, pair-major, so the block of pair p at position
+// i of row r is  npairs*rowstart[r] + p*len_r + i  and its source column is  c + p*nsrc.  Every
+// array indexed by block or source is remapped accordingly; the atom images, projector tables and
+// potential are shared by all pairs.
+std::string GreenPlan::replicate(GreenPlan const &one, uint32_t P) {
+    if (P < 1) return "at least one (energy, k-point) pair";
+    if (one.npairs != 1) return "replicate needs a one-pair plan";
+    size_t const nsrc = one.nCols;
+    if (size_t(P)*nsrc > 65535) return "at most 65535 source cubes in a batch (uint16 column indices)";
+    *this = one;
+    npairs = P; nsrc_pair = uint32_t(nsrc);
+    nCols = uint32_t(P*nsrc);
+    size_t const nnzb1 = one.nnzb(), nnzb = nnzb1*P;
+    // block map
+    std::vector<uint32_t> map(nnzb1*P);
+    rowstart.assign(one.nRows + 1, 0);
+    colindx.resize(nnzb); rowindx.resize(nnzb); veff_index.resize(nnzb);
+    target_minus_source.resize(4*nnzb);
+    for (uint32_t r = 0; r < one.nRows; ++r) {
+        uint32_t const b0 = one.rowstart[r], len = one.rowstart[r + 1] - b0;
+        rowstart[r] = uint32_t(P*size_t(b0));
+        for (uint32_t p = 0; p < P; ++p)
+            for (uint32_t i = 0; i < len; ++i) {
+                size_t const nb = P*size_t(b0) + size_t(p)*len + i, ob = b0 + i;
+                map[size_t(p)*nnzb1 + ob] = uint32_t(nb);
+                colindx[nb] = uint16_t(one.colindx[ob] + p*nsrc);
+                rowindx[nb] = one.rowindx[ob];
+                veff_index[nb] = one.veff_index[ob];
+                for (int k = 0; k < 4; ++k) target_minus_source[4*nb + k] = one.target_minus_source[4*ob + k];
+            }
+    }
+    rowstart[one.nRows] = uint32_t(nnzb);
+    auto remap = [&](uint32_t p, uint32_t b) { return map[size_t(p)*nnzb1 + b]; };
+    subset.resize(nCols); colCubePos.resize(4*size_t(nCols)); source_coords.resize(3*size_t(nCols));
+    for (uint32_t p = 0; p < P; ++p)
+        for (size_t s = 0; s < nsrc; ++s) {
+            subset[p*nsrc + s] = remap(p, one.subset[s]);
+            for (int k = 0; k < 4; ++k) colCubePos[4*(p*nsrc + s) + k] = one.colCubePos[4*s + k];
+            for (int k = 0; k < 3; ++k) source_coords[3*(p*nsrc + s) + k] = one.source_coords[3*s + k];
+        }
+    // finite-difference lists: every list of `one` once per pair, entries remapped
+    for (int dd = 0; dd < 3; ++dd) {
+        auto const &K1 = one.kinetic[dd];
+        auto &K = kinetic[dd];
+        K.start.assign(1, 0); K.entry.clear();
+        K.entry.reserve(K1.entry.size()*P);
+        for (uint32_t p = 0; p < P; ++p)
+            for (uint32_t il = 0; il < K1.nlists(); ++il) {
+                for (uint32_t k = K1.start[il]; k < K1.start[il + 1]; ++k) {
+                    int32_t const e = K1.entry[k];
+                    if (e > 0) K.entry.push_back(int32_t(remap(p, uint32_t(e - 1))) + 1);
+                    else if (e < 0) K.entry.push_back(-(int32_t(remap(p, uint32_t(-e - 1))) + 1));
+                    else K.entry.push_back(0);
+                }
+                K.start.push_back(uint32_t(K.entry.size()));
+            }
+    }
+    // projector sparsity: SHOprj per source (columns are blocks), SHOadd per block
+    SHOprj.assign(nCols, Csr{});
+    prj_slot.clear();
+    {
+        std::vector<size_t> slot_off(nsrc + 1, 0);
+        for (size_t s = 0; s < nsrc; ++s) slot_off[s + 1] = slot_off[s] + one.SHOprj[s].nnz();
+        for (uint32_t p = 0; p < P; ++p)
+            for (size_t s = 0; s < nsrc; ++s) {
+                Csr const &c1 = one.SHOprj[s];
+                Csr &c = SHOprj[p*nsrc + s];
+                c.start = c1.start;
+                c.col.resize(c1.col.size());
+                for (size_t k = 0; k < c1.col.size(); ++k) c.col[k] = remap(p, c1.col[k]);
+                prj_slot.insert(prj_slot.end(), one.prj_slot.begin() + slot_off[s], one.prj_slot.begin() + slot_off[s + 1]);
+            }
+    }
+    {
+        std::vector<uint32_t> inv(nnzb);                 // new block -> old block
+        for (uint32_t p = 0; p < P; ++p) for (size_t b = 0; b < nnzb1; ++b) inv[remap(p, uint32_t(b))] = uint32_t(b);
+        SHOadd.start.assign(1, 0); SHOadd.col.clear(); add_slot.clear();
+        SHOadd.col.reserve(one.SHOadd.nnz()*P); add_slot.reserve(one.SHOadd.nnz()*P);
+        for (size_t nb = 0; nb < nnzb; ++nb) {
+            uint32_t const ob = inv[nb];
+            for (uint32_t k = one.SHOadd.start[ob]; k < one.SHOadd.start[ob + 1]; ++k) {
+                SHOadd.col.push_back(one.SHOadd.col[k]);
+                add_slot.push_back(one.add_slot[k]);
+            }
+            SHOadd.start.push_back(uint32_t(SHOadd.col.size()));
+        }
+    }
+    // per-pair values start as copies of the one-pair values
+    pair_E.assign(2*size_t(P), 0);
+    pair_phase.resize(12*size_t(P));
+    pair_img_phase.resize(size_t(P)*AtomImagePhase.size());
+    pair_mats.resize(size_t(P)*AtomMatrices.size());
+    for (uint32_t p = 0; p < P; ++p) {
+        pair_E[2*p] = one.E_re; pair_E[2*p + 1] = one.E_im;
+        std::memcpy(&pair_phase[12*size_t(p)], one.phase, sizeof(one.phase));
+        std::copy(one.AtomImagePhase.begin(), one.AtomImagePhase.end(), pair_img_phase.begin() + size_t(p)*AtomImagePhase.size());
+        std::copy(one.AtomMatrices.begin(), one.AtomMatrices.end(), pair_mats.begin() + size_t(p)*AtomMatrices.size());
+    }
+    return "";
+}
+
+std::string GreenPlan::set_pair(uint32_t p, double Er, double Ei, double dVol, double const k[3]) {
+    if (p >= npairs) return "pair index beyond the batch";
+    // the one-pair updates on this plan's own arrays, then copied into the pair's slots
+    set_energy(Er, Ei, dVol);
+    auto const err = set_kpoint(k);
+    if (!err.empty()) return err;
+    pair_E[2*size_t(p)] = Er; pair_E[2*size_t(p) + 1] = Ei;
+    std::memcpy(&pair_phase[12*size_t(p)], phase, sizeof(phase));
+    std::copy(AtomImagePhase.begin(), AtomImagePhase.end(), pair_img_phase.begin() + size_t(p)*AtomImagePhase.size());
+    std::copy(AtomMatrices.begin(), AtomMatrices.end(), pair_mats.begin() + size_t(p)*AtomMatrices.size());
+    return "";
+}
+
+} // namespace a43g

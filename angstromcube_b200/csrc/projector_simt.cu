@@ -75,19 +75,27 @@ __device__ __forceinline__ void cp_async8(void *dst, void const *src) {
 
 // ---------------------------------------------------------------- projection
 
+// Work item w = (image a, source s, list positions [k0, k1)) of group (first, count): the items of
+// one (image, source) pair.  A group of one item writes its coefficients directly; otherwise
+// every item stores its partial sums in part[w] and the last item of the group to finish (ticket
+// counter) adds the partials in item order, so the result does not depend on the order in which
+// the items ran, and resets the counter for the next call.
 template <typename T, int L>
 __global__ void __launch_bounds__(kThreads, Occ<T>::project)
 sho_project_simt_kernel(T *__restrict__ apc, T const *__restrict__ x, uint32_t nrhs,
                        uint32_t const *__restrict__ items, uint32_t const *__restrict__ prj_col,
                        uint64_t const *__restrict__ prj_coloff, uint32_t const *__restrict__ prj_slot,
                        T const *__restrict__ slot_H, uint64_t const *__restrict__ slot_mask, int stride,
-                       uint32_t const *__restrict__ img_starts)
+                       uint32_t const *__restrict__ img_starts, uint8_t const *__restrict__ active,
+                       T *__restrict__ part, uint32_t *__restrict__ tickets)
 {
     constexpr int NS = nsho_of(L), N2 = n2_of(L);
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T *xs = reinterpret_cast<T*>(smem_raw);           // [2][kBlk]
-    uint32_t const *item = items + 4*size_t(blockIdx.x);
+    uint32_t const *item = items + 8*size_t(blockIdx.x);
     uint32_t const a = item[0], s = item[1], k0 = item[2], k1 = item[3];
+    uint32_t const g_first = item[4], g_count = item[5], g_id = item[6], g_part = item[7];
+    if (active && !active[s]) return;                 // uniform: a retired source
     int const tid = threadIdx.x, reim = tid >> 6, j = tid & 63;
     uint64_t const off = prj_coloff[s];
 
@@ -166,8 +174,31 @@ sho_project_simt_kernel(T *__restrict__ apc, T const *__restrict__ x, uint32_t n
         __syncthreads();                             // buffer buf is free for block k + 2
     }
     T *out = apc + (size_t(img_starts[a])*nrhs + s)*128 + reim*64 + j;
+    if (1 == g_count) {
 #pragma unroll
-    for (int sho = 0; sho < NS; ++sho) atomicAdd(out + size_t(sho)*nrhs*128, acc[sho]);
+        for (int sho = 0; sho < NS; ++sho) out[size_t(sho)*nrhs*128] = acc[sho];
+        return;
+    }
+    // partial sums of this item: part[(g_part + position in group)][sho][128]
+    uint32_t const q = blockIdx.x - g_first;
+    T *mine = part + (size_t(g_part) + q)*NS*128 + reim*64 + j;
+#pragma unroll
+    for (int sho = 0; sho < NS; ++sho) mine[size_t(sho)*128] = acc[sho];
+    __threadfence();                                  // partials visible before the ticket
+    __shared__ uint32_t ticket;
+    __syncthreads();
+    if (0 == tid) ticket = atomicAdd(&tickets[g_id], 1u);
+    __syncthreads();
+    if (ticket + 1 != g_count) return;                // uniform: not the last item of the group
+    __threadfence();
+    T const *pg = part + size_t(g_part)*NS*128 + reim*64 + j;
+#pragma unroll 4
+    for (int sho = 0; sho < NS; ++sho) {
+        T sum = T(0);
+        for (uint32_t i = 0; i < g_count; ++i) sum += __ldcg(pg + (size_t(i)*NS + sho)*128);
+        out[size_t(sho)*nrhs*128] = sum;
+    }
+    if (0 == tid) tickets[g_id] = 0u;                 // ready for the next call
 }
 
 // ---------------------------------------------------------------- addition
@@ -239,7 +270,8 @@ __global__ void __launch_bounds__(kThreads*ZS, Occ<T>::add)
 sho_add_simt_kernel(T *__restrict__ y, T const *__restrict__ cad, uint32_t nrhs, uint32_t nnzb,
                     uint32_t blocks_per_cta, uint16_t const *__restrict__ colIndex,
                     uint32_t const *__restrict__ add_start, uint4 const *__restrict__ info,
-                    T const *__restrict__ slot_H, uint64_t const *__restrict__ slot_mask, int stride)
+                    T const *__restrict__ slot_H, uint64_t const *__restrict__ slot_mask, int stride,
+                    uint8_t const *__restrict__ active)
 {
     constexpr int NCMAX = nsho_of(LMAX);
     constexpr int TE = 16/int(sizeof(T));                  // elements per 16-byte copy
@@ -262,7 +294,12 @@ sho_add_simt_kernel(T *__restrict__ y, T const *__restrict__ cad, uint32_t nrhs,
     uint32_t s = colIndex[bb];
     uint32_t bend = add_start[bb + 1];                     // first pair of the next block
 
+    // pairs of a retired source stage nothing and carry an empty mask: no work, no y update
     auto stage_pair = [&](uint4 const inf, uint32_t src_col, int buf) {
+        if (active && !active[src_col]) {
+            if (tid == NT - 1) mbuf[buf] = 0;
+            return;
+        }
         int const L = int(inf.z), nc = nsho_of(L);
         T const *src = cad + (size_t(inf.y)*nrhs + src_col)*128;
         T *dst = cbuf + buf*NCMAX*128;
@@ -275,6 +312,7 @@ sho_add_simt_kernel(T *__restrict__ y, T const *__restrict__ cad, uint32_t nrhs,
         if (tid == NT - 1) cp_async8(&mbuf[buf], slot_mask + inf.x);
     };
     auto stage_y = [&](uint32_t blk) {
+        if (active && !active[colIndex[blk]]) return;
         T const *src = y + size_t(blk)*kBlk;
 #pragma unroll
         for (int r = 0; r < kBlk/(TE*NT); ++r) {
@@ -358,9 +396,10 @@ void launch_project_L(DevicePlan &dp, T const *x, cudaStream_t st) {
     if (0 == g.count) return;
     constexpr int smem = 2*kBlk*int(sizeof(T));         // double-buffered block stage
     sho_project_simt_kernel<T, L><<<g.count, kThreads, smem, st>>>(
-        dptr<T>(dp.apc), x, dp.nCols, dptr<uint32_t>(g.items), dptr<uint32_t>(dp.prj_col),
+        dptr<T>(dp.apc), x, dp.nCols, dptr<uint32_t>(g.items8), dptr<uint32_t>(dp.prj_col),
         dptr<uint64_t>(dp.prj_coloff), dptr<uint32_t>(dp.prj_slot), simt_table<T>(dp),
-        dptr<uint64_t>(dp.slot_mask), dp.table_stride, dptr<uint32_t>(dp.img_starts));
+        dptr<uint64_t>(dp.slot_mask), dp.table_stride, dptr<uint32_t>(dp.img_starts),
+        dp.retire ? dptr<uint8_t>(dp.src_active) : nullptr, dptr<T>(dp.prj_part), dptr<uint32_t>(g.tickets));
     count_launch();
 }
 
@@ -371,7 +410,7 @@ void launch_add_L(DevicePlan &dp, T *y, uint16_t const *colIndex, cudaStream_t s
     unsigned const grid = (dp.nnzb + per_cta - 1)/per_cta;
     sho_add_simt_kernel<T, LMAX><<<grid, kThreads*(int(sizeof(T))/4), smem, st>>>(y, dptr<T>(dp.cad), dp.nCols, dp.nnzb, per_cta,
         colIndex, dptr<uint32_t>(dp.add_start), dptr<uint4>(dp.add_info), simt_table<T>(dp),
-        dptr<uint64_t>(dp.slot_mask), dp.table_stride);
+        dptr<uint64_t>(dp.slot_mask), dp.table_stride, dp.retire ? dptr<uint8_t>(dp.src_active) : nullptr);
 }
 
 template <typename T, int L>
@@ -405,6 +444,9 @@ bool simt_projector_supported(DevicePlan const &dp, void const *x, void const *y
 
 template <typename T>
 bool launch_project_simt(DevicePlan &dp, T const *x, cudaStream_t st) {
+    // every (image, source) pair with blocks is written by its items; images without blocks of a
+    // source keep zero coefficients
+    if (!ensure_prj_part(dp, sizeof(T))) return false;
     A43G_CUDA_TRY(cudaMemsetAsync(dp.apc.ptr, 0, size_t(dp.ncoeffI)*dp.nCols*128*sizeof(T), st));
     launch_project_L<T, 0>(dp, x, st); launch_project_L<T, 1>(dp, x, st);
     launch_project_L<T, 2>(dp, x, st); launch_project_L<T, 3>(dp, x, st);

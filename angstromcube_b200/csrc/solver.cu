@@ -1,35 +1,68 @@
 // Transpose-free QMR (Freund, SIAM J. Sci. Comput. 14:470, 1993) for all columns of the
-// block-sparse Green function at once, each column with its own scalars, plus mixed
-// precision (FP32 sweeps inside FP64 residual refinement).
+// block-sparse Green function at once, each column with its own scalars; the reference calls
+// the same algorithm from the external library tfQMRgpu (include/green_action.hxx:216).
+//
+// Two precisions:
+//  * FP64: every vector and the solution in FP64; a column has converged when its QMR residual
+//    bound tau*sqrt(m+1) falls below the tolerance (the test tfQMRgpu applies);
+//  * FP32 recurrences with an FP64 solution and residual replacement: the vectors W, U, V, D,
+//    A U are FP32 and the operator is the FP32 action; the solution is accumulated in FP64
+//    (X64 += X32 at every replacement, X32 = 0).  A replacement recomputes the true residual of
+//    the FP64 solution with the FP64 action, R = B - A X64, and restarts the recurrence of W
+//    from it: with the CGS iterate  x~ = x + theta^2 eta d  of the QMR iterate x,
+//    W = R - theta^2 eta A d  (A d with the FP32 action) is the true residual of x~.  The QMR
+//    smoothing (tau, theta, eta, D) and the search directions (U2, V) are kept, so the Krylov
+//    space is not restarted (residual replacement after Sleijpen & van der Vorst, Computing 56,
+//    1996, and van der Vorst & Ye, SIAM J. Sci. Comput. 22, 2000).  A column has converged when
+//    its true FP64 residual at a replacement is below the tolerance.  Each source cube (64
+//    columns) asks for a replacement when the largest residual estimate of its active columns
+//    has fallen by update_factor since its last one, when all of them are below the tolerance,
+//    or after update_gap iterations.  The CGS-type recurrences of tfQMR amplify the FP32
+//    rounding strongly where the energy lies close to the spectrum: a source cube whose largest
+//    true residual has not fallen by 10 % over stall_limit replacements (or is not finite) leaves the FP32
+//    recurrences, and all such sources then continue as FP64 tfQMR from their FP64 solution.
 //
 // One iteration = two operator applications.  The BLAS-1 work is fused so that every vector
 // is streamed as few times as possible:
 //   K_A   U2 = U1 - a V                 and |W - a AU1|^2
 //   K_C   W  = W - a (AU1 + AU2)        and |W|^2, rt^H W
-// (U1 = y_{2n-1}, U2 = y_{2n}, AU1 = A y_{2n-1}, AU2 = A y_{2n}, V = v_{n-1} in Freund's notation)
 //   K_DX  D, X advanced by both half steps at once;  U1 = W + b U2
 //   K_E   V  = AU1 + b (AU2 + b V)      and rt^H V
-// The shadow residual rt is a counter-based random vector regenerated on the fly, so it is
-// never stored.  FP32 sweeps do the vector arithmetic in FP32 and accumulate the inner
-// products in FP64.  Per-column reductions end in double atomics; the scalar recurrences run in
-// FP64 in one thread per column.  Finished columns (converged or broken down) get zero
-// coefficients, which freezes X and keeps all vectors finite.
+// (U1 = y_{2n-1}, U2 = y_{2n}, AU1 = A y_{2n-1}, AU2 = A y_{2n}, V = v_{n-1} in Freund's
+// notation).  The shadow residual rt is a counter-based random vector regenerated on the fly.
+//
+// Work units and reductions: every vector kernel runs one CTA per (source cube, chunk of its
+// blocks); the column sums of a unit go to a slot of their own, and the last CTA of a source to
+// finish (a ticket counter) adds the slots in chunk order, so every inner product is the same in
+// every run, and then advances the scalar recurrences of the source's 64 columns.
+//
+// Retirement: a source whose 64 columns have all finished is skipped by every vector kernel and
+// by every kernel of the action (DevicePlan::retire), so finished columns cost nothing.
+//
+// Batches: a plan built by GreenPlan::replicate holds several (energy, k-point) pairs as
+// independent sources of one block-sparse system; solve_batched solves them in waves.
 #include "solver.hpp"
 
 #include <algorithm>
-#include <cstdlib>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
+#include <cstring>
 #include <vector>
 
 namespace a43g {
 
+#define A43G_CUDA_TRY_RC(call) do { cudaError_t e_ = (call); if (cudaSuccess != e_) { \
+    ::a43g::set_error(std::string(#call) + ": " + cudaGetErrorString(e_)); return A43G_ERR_CUDA; } } while (0)
+
 namespace {
 
 constexpr int kBlk = 8192;
+constexpr int kCoef = 14;     // alpha, beta, the five complex K_DX coefficients
+constexpr int kSlots = 8;     // column sums per unit and column (at most 5 are used)
 
 struct ColState {
-    double rho_re, rho_im;       // rho_{n-1} = rt^H w
+    double rho_re, rho_im;       // rho = rt^H w
     double al_re, al_im;         // alpha
     double be_re, be_im;         // beta
     double eta_re, eta_im;       // eta of the last half step
@@ -40,13 +73,56 @@ struct ColState {
     // combined coefficients of K_DX (X and D advanced over both half steps)
     double cu1x_re, cu1x_im, cu2x_re, cu2x_im, cdx_re, cdx_im;
     double cu1d_re, cu1d_im, cdd_re, cdd_im;
-    double tau_ref;              // stall detection: tau at the last halving, and its half step
-    int32_t m_ref;
-    int32_t status;              // 0 active, 1 converged, 2 breakdown, 3 idle (zero column), 4 stalled
-    int32_t conv1;               // converged in the first half step of this iteration
+    double rhop_re, rhop_im;     // rho of the previous iteration (beta after a replacement)
+    double cup_re, cup_im;       // theta^2 eta:  x~ - x = cup d
+    double scale;                // estimate correction (true residual / estimate at a replacement, >= 1)
+    double res;                  // true relative residual at the last replacement, or at the end
+    int32_t m;                   // half steps done
+    int32_t status;              // 0 active, 1 converged, 2 breakdown, 3 idle (zero column), 5 left the
+                                 // FP32 recurrences for FP64
+    int32_t conv1;               // converged in the first half step of this iteration (FP64)
+    int32_t pad;
 };
 
-struct Acc { double n2, re, im, pad; };   // per-column reduction accumulator
+struct SrcState {
+    int32_t it;                  // iterations done while the source was active
+    int32_t since;               // iterations since its last replacement
+    int32_t upd;                 // replacement in this iteration
+    int32_t updates;             // replacements done
+    int32_t done;                // no active column left
+    int32_t stall;               // replacements since its largest true residual last fell by 10 %
+    int32_t fallback;            // left the FP32 recurrences for FP64
+    int32_t nonfinite;           // ... with a residual that was not finite
+    double est_ref;              // largest true residual of its active columns at the last replacement
+    double best;                 // smallest such residual so far
+};
+
+struct Ctl {
+    int32_t n_active;            // sources with an active column
+    int32_t breakdowns;
+    int32_t pad[2];
+};
+
+struct Ctx {
+    uint32_t const *src_start, *src_blocks;
+    uint32_t const *subset;
+    uint8_t const *active;       // retirement flags read by the vector kernels (nullptr: all)
+    uint8_t *src_active;         // the flags the action reads, cleared when a source retires
+    uint8_t *upd;                // per source: replacement in this iteration
+    uint32_t nch, ncol;          // chunks per source, columns (sources * 64)
+    double *part;                // [units][kSlots][64] column sums per unit
+    uint32_t *tickets;           // [sources]
+    ColState *cs;
+    SrcState *ss;
+    Ctl *ctl;
+    double *cd;                  // [kCoef][ncol] coefficients for the FP64 vector kernels
+    float *cf;                   // [kCoef][ncol] the same in FP32
+    uint32_t seed;
+    double tol, delta;
+    int32_t gap, mixed, retire;
+    int32_t stall_limit;         // replacements without progress of the true residual before FP64
+    int32_t abs_tol;             // the tolerance is absolute (the FP64 continuation of unit columns)
+};
 
 __device__ __forceinline__ uint32_t mix32(uint32_t h) {
     // murmur3 finaliser as a counter-based generator
@@ -54,299 +130,70 @@ __device__ __forceinline__ uint32_t mix32(uint32_t h) {
     return h;
 }
 
-// shadow residual element for (block, reim, i, j): uniform in [-1, 1)
+// shadow residual element for (block, reim, i, j): uniform in [-1, 1); FP32 sweeps use the
+// same values rounded to FP32
 __device__ __forceinline__ double shadow(uint32_t seed, uint32_t idx) {
     return double(int32_t(mix32(idx*0x9E3779B9u + seed))) * (1.0/2147483648.0);
 }
-
-// the same element in FP32 (the double value above rounded to float)
 __device__ __forceinline__ float shadow32(uint32_t seed, uint32_t idx) {
     return float(int32_t(mix32(idx*0x9E3779B9u + seed))) * (1.0f/2147483648.0f);
 }
+template <typename T> __device__ __forceinline__ T shadow_t(uint32_t seed, uint32_t idx);
+template <> __device__ __forceinline__ float shadow_t<float>(uint32_t seed, uint32_t idx) { return shadow32(seed, idx); }
+template <> __device__ __forceinline__ double shadow_t<double>(uint32_t seed, uint32_t idx) { return shadow(seed, idx); }
 
-template <typename T>
-__device__ __forceinline__ void cmul(double ar, double ai, T br, T bi, double &r, double &i) {
-    r = ar*double(br) - ai*double(bi); i = ar*double(bi) + ai*double(br);
+// the blocks [lo, hi) of src_blocks that unit u works on; false for a skipped source
+__device__ __forceinline__ bool unit_range(Ctx const &c, uint8_t const *active, uint32_t u, uint32_t &s,
+                                           uint32_t &lo, uint32_t &hi) {
+    s = u/c.nch;
+    uint32_t const q = u - s*c.nch;
+    if (active && !active[s]) return false;
+    uint32_t const a = c.src_start[s], n = c.src_start[s + 1] - a;
+    lo = a + uint32_t((uint64_t(n)*q)/c.nch);
+    hi = a + uint32_t((uint64_t(n)*(q + 1))/c.nch);
+    return true;
 }
 
-// block-local reduction of up to 3 values per column over the 4 row groups, then atomics
-__device__ __forceinline__ void reduce_cols(double (*red)[64][3], int q, int j, double v0, double v1, double v2,
-                                            Acc *acc, int ncomp) {
-    red[q][j][0] = v0; red[q][j][1] = v1; red[q][j][2] = v2;
+// Column sums of one unit (thread (q, j) holds its row group's share v[] of column j) into the
+// unit's slot; true in the last CTA of the source to finish, whose threads 0..63 then hold the
+// fixed-order total over all units of the source in out[].  Called by all 256 threads.
+template <int NC>
+__device__ bool reduce_source(Ctx const &c, uint32_t u, uint32_t s, double const (&v)[NC], double (&out)[NC]) {
+    __shared__ double red[4][64][NC];
+    __shared__ uint32_t ticket;
+    int const j = threadIdx.x & 63, q = threadIdx.x >> 6;
+#pragma unroll
+    for (int k = 0; k < NC; ++k) red[q][j][k] = v[k];
     __syncthreads();
     if (0 == q) {
-        double s0 = 0, s1 = 0, s2 = 0;
-        for (int k = 0; k < 4; ++k) { s0 += red[k][j][0]; s1 += red[k][j][1]; s2 += red[k][j][2]; }
-        atomicAdd(&acc->n2, s0);
-        if (ncomp > 1) { atomicAdd(&acc->re, s1); atomicAdd(&acc->im, s2); }
+#pragma unroll
+        for (int k = 0; k < NC; ++k)
+            c.part[(size_t(u)*kSlots + k)*64 + j] = ((red[0][j][k] + red[1][j][k]) + red[2][j][k]) + red[3][j][k];
+    }
+    __threadfence();
+    __syncthreads();
+    if (0 == threadIdx.x) ticket = atomicAdd(&c.tickets[s], 1u);
+    __syncthreads();
+    if (ticket + 1 != c.nch) return false;            // uniform over the CTA
+    __threadfence();
+    // thread (q, j) adds the units q, q + 4, ... of the source, then the four partial sums
+    double acc[NC];
+#pragma unroll
+    for (int k = 0; k < NC; ++k) acc[k] = 0;
+    for (uint32_t i = q; i < c.nch; i += 4) {
+        size_t const base = size_t(s)*c.nch + i;
+#pragma unroll
+        for (int k = 0; k < NC; ++k) acc[k] += __ldcg(&c.part[(base*kSlots + k)*64 + j]);
     }
     __syncthreads();
+#pragma unroll
+    for (int k = 0; k < NC; ++k) red[q][j][k] = acc[k];
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < NC; ++k) out[k] = ((red[0][j][k] + red[1][j][k]) + red[2][j][k]) + red[3][j][k];
+    if (0 == threadIdx.x) c.tickets[s] = 0u;
+    return true;
 }
-
-// ------------------------------------------------------------------ vector kernels
-// grid-stride over blocks; thread (q, j): column j, rows q*16 .. q*16+15, re and im
-
-template <typename T>
-__global__ void k_set_diag(T *W, T *U1, uint32_t const *subset, uint32_t ncols_blk) {
-    uint32_t const c = blockIdx.x; int const i = threadIdx.x;
-    if (c < ncols_blk) {
-        size_t const o = size_t(subset[c])*kBlk + size_t(i)*64 + i;
-        W[o] = T(1); U1[o] = T(1);
-    }
-}
-
-// initial reductions: |W|^2, rt^H W and rt^H V
-template <typename T>
-__global__ void __launch_bounds__(256) k_init_dots(T const *W, T const *V, uint32_t nnzb, uint16_t const *colindx,
-                                                   Acc *accW, Acc *accV, uint32_t seed) {
-    __shared__ double red[4][64][3];
-    int const j = threadIdx.x & 63, q = threadIdx.x >> 6;
-    for (uint32_t b = blockIdx.x; b < nnzb; b += gridDim.x) {
-        uint32_t const c = colindx[b];
-        double n2 = 0, wr = 0, wi = 0, vr = 0, vi = 0;
-#pragma unroll 8
-        for (int i = q*16; i < q*16 + 16; ++i) {
-            size_t const o = size_t(b)*kBlk + i*64 + j;
-            uint32_t const idx = uint32_t(o);
-            // FP32 sweeps use the shadow vector rounded to FP32 throughout
-            double const tr = (sizeof(T) == 4) ? double(shadow32(seed, idx)) : shadow(seed, idx);
-            double const ti = (sizeof(T) == 4) ? double(shadow32(seed, idx + 4096u)) : shadow(seed, idx + 4096u);
-            double const xr = W[o], xi = W[o + 4096], yr = V[o], yi = V[o + 4096];
-            n2 += xr*xr + xi*xi;
-            wr += tr*xr + ti*xi; wi += tr*xi - ti*xr;     // conj(rt) w
-            vr += tr*yr + ti*yi; vi += tr*yi - ti*yr;
-        }
-        reduce_cols(red, q, j, n2, wr, wi, &accW[c*64 + j], 3);
-        reduce_cols(red, q, j, 0.0, vr, vi, &accV[c*64 + j], 3);
-    }
-}
-
-// K_A: U2 = U1 - alpha V ; acc |W - alpha AU1|^2
-template <typename T>
-__global__ void __launch_bounds__(256) k_A(T *U2, T const *U1, T const *V, T const *W, T const *AU1, uint32_t nnzb,
-                                           uint16_t const *colindx, ColState const *cs, Acc *acc,
-                                           float const *cf, uint32_t ncol) {
-    __shared__ double red[4][64][3];
-    int const j = threadIdx.x & 63, q = threadIdx.x >> 6;
-    for (uint32_t b = blockIdx.x; b < nnzb; b += gridDim.x) {
-        uint32_t const col = colindx[b]*64 + j;
-        double n2 = 0;
-        if constexpr (sizeof(T) == 4) {
-            // FP32 sweep: vector arithmetic in FP32, 32-term partial sums in FP32, the rest in FP64
-            float const fr = cf[col], fi = cf[ncol + col];
-            float n2f = 0.f;
-#pragma unroll 8
-            for (int i = q*16; i < q*16 + 16; ++i) {
-                size_t const o = size_t(b)*kBlk + i*64 + j;
-                float const vr = V[o], vi = V[o + 4096];
-                U2[o] = fmaf(fi, vi, fmaf(-fr, vr, U1[o]));
-                U2[o + 4096] = fmaf(-fi, vr, fmaf(-fr, vi, U1[o + 4096]));
-                float const ur = AU1[o], ui = AU1[o + 4096];
-                float const wr = fmaf(fi, ui, fmaf(-fr, ur, W[o])), wi = fmaf(-fi, ur, fmaf(-fr, ui, W[o + 4096]));
-                n2f = fmaf(wr, wr, fmaf(wi, wi, n2f));
-            }
-            n2 = double(n2f);
-        } else {
-        double const ar = cs[col].al_re, ai = cs[col].al_im;
-#pragma unroll 8
-        for (int i = q*16; i < q*16 + 16; ++i) {
-            size_t const o = size_t(b)*kBlk + i*64 + j;
-            T const vr = V[o], vi = V[o + 4096];
-            double avr, avi; cmul(ar, ai, vr, vi, avr, avi);
-            U2[o] = T(double(U1[o]) - avr); U2[o + 4096] = T(double(U1[o + 4096]) - avi);
-            double aur, aui; cmul(ar, ai, AU1[o], AU1[o + 4096], aur, aui);
-            double const wr = double(W[o]) - aur, wi = double(W[o + 4096]) - aui;
-            n2 += wr*wr + wi*wi;
-        }
-        }
-        reduce_cols(red, q, j, n2, 0.0, 0.0, &acc[col], 1);
-    }
-}
-
-// K_C: W = W - alpha (AU1 + AU2) ; acc |W|^2 and rt^H W
-template <typename T>
-__global__ void __launch_bounds__(256) k_C(T *W, T const *AU1, T const *AU2, uint32_t nnzb,
-                                           uint16_t const *colindx, ColState const *cs, Acc *acc, uint32_t seed,
-                                           float const *cf, uint32_t ncol) {
-    __shared__ double red[4][64][3];
-    int const j = threadIdx.x & 63, q = threadIdx.x >> 6;
-    for (uint32_t b = blockIdx.x; b < nnzb; b += gridDim.x) {
-        uint32_t const col = colindx[b]*64 + j;
-        double const ar = (sizeof(T) == 8) ? cs[col].al_re : 0.0, ai = (sizeof(T) == 8) ? cs[col].al_im : 0.0;
-        double n2 = 0, dr = 0, di = 0;
-        if constexpr (sizeof(T) == 4) {
-            float const fr = cf[col], fi = cf[ncol + col];
-            float n2f = 0.f, drf = 0.f, dif = 0.f;
-#pragma unroll 8
-            for (int i = q*16; i < q*16 + 16; ++i) {
-                size_t const o = size_t(b)*kBlk + i*64 + j;
-                float const sr = AU1[o] + AU2[o], si = AU1[o + 4096] + AU2[o + 4096];
-                float const wr = fmaf(fi, si, fmaf(-fr, sr, W[o])), wi = fmaf(-fi, sr, fmaf(-fr, si, W[o + 4096]));
-                W[o] = wr; W[o + 4096] = wi;
-                uint32_t const idx = uint32_t(o);
-                float const tr = shadow32(seed, idx), ti = shadow32(seed, idx + 4096u);
-                n2f = fmaf(wr, wr, fmaf(wi, wi, n2f));
-                drf = fmaf(tr, wr, fmaf(ti, wi, drf)); dif = fmaf(tr, wi, fmaf(-ti, wr, dif));
-            }
-            n2 = double(n2f); dr = double(drf); di = double(dif);
-        } else
-#pragma unroll 8
-        for (int i = q*16; i < q*16 + 16; ++i) {
-            size_t const o = size_t(b)*kBlk + i*64 + j;
-            double const sr = double(AU1[o]) + double(AU2[o]), si = double(AU1[o + 4096]) + double(AU2[o + 4096]);
-            double const wr = double(W[o]) - (ar*sr - ai*si), wi = double(W[o + 4096]) - (ar*si + ai*sr);
-            T const tr_ = T(wr), ti_ = T(wi);
-            W[o] = tr_; W[o + 4096] = ti_;
-            double const xr = tr_, xi = ti_;
-            uint32_t const idx = uint32_t(o);
-            double const tr = shadow(seed, idx), ti = shadow(seed, idx + 4096u);
-            n2 += xr*xr + xi*xi;
-            dr += tr*xr + ti*xi; di += tr*xi - ti*xr;
-        }
-        reduce_cols(red, q, j, n2, dr, di, &acc[col], 3);
-    }
-}
-
-// K_DX: X += cu1x U1 + cu2x U2 + cdx D ; D = U2 + cu1d U1 + cdd D ; U1 = W + beta U2
-// (X may be kept in FP64 while the recurrence vectors are FP32: the solution then carries no
-// FP32 rounding, which lowers the residual floor of an FP32 sweep)
-template <typename T, typename TX>
-__global__ void __launch_bounds__(256) k_DX(TX *X, T *D, T *U1, T const *U2, T const *W, uint32_t nnzb,
-                                            uint16_t const *colindx, ColState const *cs, float const *cf, uint32_t ncol) {
-    int const j = threadIdx.x & 63, q = threadIdx.x >> 6;
-    for (uint32_t b = blockIdx.x; b < nnzb; b += gridDim.x) {
-        uint32_t const col = colindx[b]*64 + j;
-        if constexpr (sizeof(T) == 4 && sizeof(TX) == 4) {
-            float const g_r = cf[2*size_t(ncol) + col], g_i = cf[3*size_t(ncol) + col];
-            float const a_r = cf[4*size_t(ncol) + col], a_i = cf[5*size_t(ncol) + col];
-            float const b_r = cf[6*size_t(ncol) + col], b_i = cf[7*size_t(ncol) + col];
-            float const c_r = cf[8*size_t(ncol) + col], c_i = cf[9*size_t(ncol) + col];
-            float const d_r = cf[10*size_t(ncol) + col], d_i = cf[11*size_t(ncol) + col];
-            float const e_r = cf[12*size_t(ncol) + col], e_i = cf[13*size_t(ncol) + col];
-#pragma unroll 8
-            for (int i = q*16; i < q*16 + 16; ++i) {
-                size_t const o = size_t(b)*kBlk + i*64 + j;
-                float const u1r = U1[o], u1i = U1[o + 4096], u2r = U2[o], u2i = U2[o + 4096];
-                float const dr = D[o], di = D[o + 4096];
-                float xr = X[o], xi = X[o + 4096];
-                xr = fmaf(a_r, u1r, fmaf(-a_i, u1i, xr)); xi = fmaf(a_r, u1i, fmaf(a_i, u1r, xi));
-                xr = fmaf(b_r, u2r, fmaf(-b_i, u2i, xr)); xi = fmaf(b_r, u2i, fmaf(b_i, u2r, xi));
-                xr = fmaf(c_r, dr, fmaf(-c_i, di, xr));   xi = fmaf(c_r, di, fmaf(c_i, dr, xi));
-                X[o] = xr; X[o + 4096] = xi;
-                D[o] = fmaf(d_r, u1r, fmaf(-d_i, u1i, fmaf(e_r, dr, fmaf(-e_i, di, u2r))));
-                D[o + 4096] = fmaf(d_r, u1i, fmaf(d_i, u1r, fmaf(e_r, di, fmaf(e_i, dr, u2i))));
-                U1[o] = fmaf(g_r, u2r, fmaf(-g_i, u2i, W[o]));
-                U1[o + 4096] = fmaf(g_r, u2i, fmaf(g_i, u2r, W[o + 4096]));
-            }
-        } else {
-        ColState const &s = cs[col];
-        double const ax_r = s.cu1x_re, ax_i = s.cu1x_im, bx_r = s.cu2x_re, bx_i = s.cu2x_im, cx_r = s.cdx_re, cx_i = s.cdx_im;
-        double const ad_r = s.cu1d_re, ad_i = s.cu1d_im, cd_r = s.cdd_re, cd_i = s.cdd_im;
-        double const be_r = s.be_re, be_i = s.be_im;
-#pragma unroll 8
-        for (int i = q*16; i < q*16 + 16; ++i) {
-            size_t const o = size_t(b)*kBlk + i*64 + j;
-            double const u1r = U1[o], u1i = U1[o + 4096], u2r = U2[o], u2i = U2[o + 4096];
-            double const dr = D[o], di = D[o + 4096];
-            double const xr = double(X[o]) + (ax_r*u1r - ax_i*u1i) + (bx_r*u2r - bx_i*u2i) + (cx_r*dr - cx_i*di);
-            double const xi = double(X[o + 4096]) + (ax_r*u1i + ax_i*u1r) + (bx_r*u2i + bx_i*u2r) + (cx_r*di + cx_i*dr);
-            X[o] = TX(xr); X[o + 4096] = TX(xi);
-            D[o] = T(u2r + (ad_r*u1r - ad_i*u1i) + (cd_r*dr - cd_i*di));
-            D[o + 4096] = T(u2i + (ad_r*u1i + ad_i*u1r) + (cd_r*di + cd_i*dr));
-            double const wr = W[o], wi = W[o + 4096];
-            U1[o] = T(wr + (be_r*u2r - be_i*u2i));
-            U1[o + 4096] = T(wi + (be_r*u2i + be_i*u2r));
-        }
-        }
-    }
-}
-
-// K_DX of an FP32 sweep with 16-byte accesses: thread (column group of 4, row group of 4 rows);
-// each row moves 10 float4 loads and 6 float4 stores, and the 12 coefficients of its 4 columns
-// are 12 float4 loads per block
-__device__ __forceinline__ float4 ld4(float const *p) { return *reinterpret_cast<float4 const*>(p); }
-__device__ __forceinline__ void st4(float *p, float4 v) { *reinterpret_cast<float4*>(p) = v; }
-
-__global__ void __launch_bounds__(256, 2) k_DX32(float *X, float *D, float *U1, float const *U2, float const *W,
-                                                 uint32_t nnzb, uint16_t const *colindx, float const *cf, uint32_t ncol) {
-    int const cg = threadIdx.x & 15, rg = threadIdx.x >> 4;
-    int const j0 = cg*4;
-    for (uint32_t b = blockIdx.x; b < nnzb; b += gridDim.x) {
-        uint32_t const col = colindx[b]*64 + j0;
-        float4 const g_r = ld4(cf + 2*size_t(ncol) + col), g_i = ld4(cf + 3*size_t(ncol) + col);
-        float4 const a_r = ld4(cf + 4*size_t(ncol) + col), a_i = ld4(cf + 5*size_t(ncol) + col);
-        float4 const b_r = ld4(cf + 6*size_t(ncol) + col), b_i = ld4(cf + 7*size_t(ncol) + col);
-        float4 const c_r = ld4(cf + 8*size_t(ncol) + col), c_i = ld4(cf + 9*size_t(ncol) + col);
-        float4 const d_r = ld4(cf + 10*size_t(ncol) + col), d_i = ld4(cf + 11*size_t(ncol) + col);
-        float4 const e_r = ld4(cf + 12*size_t(ncol) + col), e_i = ld4(cf + 13*size_t(ncol) + col);
-#pragma unroll 2
-        for (int i = rg*4; i < rg*4 + 4; ++i) {
-            size_t const o = size_t(b)*kBlk + i*64 + j0;
-            float4 const u1r = ld4(U1 + o), u1i = ld4(U1 + o + 4096), u2r = ld4(U2 + o), u2i = ld4(U2 + o + 4096);
-            float4 const dr = ld4(D + o), di = ld4(D + o + 4096), wr = ld4(W + o), wi = ld4(W + o + 4096);
-            float4 xr = ld4(X + o), xi = ld4(X + o + 4096);
-            float4 nd_r, nd_i, nu_r, nu_i;
-#define A43G_DX_LANE(c) \
-            xr.c = fmaf(a_r.c, u1r.c, fmaf(-a_i.c, u1i.c, xr.c)); xi.c = fmaf(a_r.c, u1i.c, fmaf(a_i.c, u1r.c, xi.c)); \
-            xr.c = fmaf(b_r.c, u2r.c, fmaf(-b_i.c, u2i.c, xr.c)); xi.c = fmaf(b_r.c, u2i.c, fmaf(b_i.c, u2r.c, xi.c)); \
-            xr.c = fmaf(c_r.c, dr.c, fmaf(-c_i.c, di.c, xr.c));   xi.c = fmaf(c_r.c, di.c, fmaf(c_i.c, dr.c, xi.c)); \
-            nd_r.c = fmaf(d_r.c, u1r.c, fmaf(-d_i.c, u1i.c, fmaf(e_r.c, dr.c, fmaf(-e_i.c, di.c, u2r.c)))); \
-            nd_i.c = fmaf(d_r.c, u1i.c, fmaf(d_i.c, u1r.c, fmaf(e_r.c, di.c, fmaf(e_i.c, dr.c, u2i.c)))); \
-            nu_r.c = fmaf(g_r.c, u2r.c, fmaf(-g_i.c, u2i.c, wr.c)); \
-            nu_i.c = fmaf(g_r.c, u2i.c, fmaf(g_i.c, u2r.c, wi.c));
-            A43G_DX_LANE(x) A43G_DX_LANE(y) A43G_DX_LANE(z) A43G_DX_LANE(w)
-#undef A43G_DX_LANE
-            st4(X + o, xr); st4(X + o + 4096, xi);
-            st4(D + o, nd_r); st4(D + o + 4096, nd_i);
-            st4(U1 + o, nu_r); st4(U1 + o + 4096, nu_i);
-        }
-    }
-}
-
-// K_E: V = AU1 + beta (AU2 + beta V) ; acc rt^H V
-template <typename T>
-__global__ void __launch_bounds__(256) k_E(T *V, T const *AU1, T const *AU2, uint32_t nnzb,
-                                           uint16_t const *colindx, ColState const *cs, Acc *acc, uint32_t seed,
-                                           float const *cf, uint32_t ncol) {
-    __shared__ double red[4][64][3];
-    int const j = threadIdx.x & 63, q = threadIdx.x >> 6;
-    for (uint32_t b = blockIdx.x; b < nnzb; b += gridDim.x) {
-        uint32_t const col = colindx[b]*64 + j;
-        double const br = (sizeof(T) == 8) ? cs[col].be_re : 0.0, bi = (sizeof(T) == 8) ? cs[col].be_im : 0.0;
-        double dr = 0, di = 0;
-        if constexpr (sizeof(T) == 4) {
-            float const fr = cf[2*size_t(ncol) + col], fi = cf[3*size_t(ncol) + col];
-            float drf = 0.f, dif = 0.f;
-#pragma unroll 8
-            for (int i = q*16; i < q*16 + 16; ++i) {
-                size_t const o = size_t(b)*kBlk + i*64 + j;
-                float const vr = V[o], vi = V[o + 4096];
-                float const t1r = fmaf(-fi, vi, fmaf(fr, vr, AU2[o])), t1i = fmaf(fi, vr, fmaf(fr, vi, AU2[o + 4096]));
-                float const sr = fmaf(-fi, t1i, fmaf(fr, t1r, AU1[o])), si = fmaf(fi, t1r, fmaf(fr, t1i, AU1[o + 4096]));
-                V[o] = sr; V[o + 4096] = si;
-                uint32_t const idx = uint32_t(o);
-                float const tr = shadow32(seed, idx), ti = shadow32(seed, idx + 4096u);
-                drf = fmaf(tr, sr, fmaf(ti, si, drf)); dif = fmaf(tr, si, fmaf(-ti, sr, dif));
-            }
-            dr = double(drf); di = double(dif);
-        } else
-#pragma unroll 8
-        for (int i = q*16; i < q*16 + 16; ++i) {
-            size_t const o = size_t(b)*kBlk + i*64 + j;
-            double const vr = V[o], vi = V[o + 4096];
-            double const tr1 = double(AU2[o]) + (br*vr - bi*vi), ti1 = double(AU2[o + 4096]) + (br*vi + bi*vr);
-            double const nr = double(AU1[o]) + (br*tr1 - bi*ti1), ni = double(AU1[o + 4096]) + (br*ti1 + bi*tr1);
-            T const sr = T(nr), si = T(ni);
-            V[o] = sr; V[o + 4096] = si;
-            uint32_t const idx = uint32_t(o);
-            double const tr = shadow(seed, idx), ti = shadow(seed, idx + 4096u);
-            dr += tr*double(sr) + ti*double(si); di += tr*double(si) - ti*double(sr);
-        }
-        reduce_cols(red, q, j, 0.0, dr, di, &acc[col], 3);
-    }
-}
-
-// ------------------------------------------------------------------ scalar kernels (one thread per column)
 
 __device__ __forceinline__ void cdiv(double ar, double ai, double br, double bi, double &r, double &i) {
     double const d = br*br + bi*bi;
@@ -357,201 +204,564 @@ __device__ __forceinline__ void freeze(ColState &s) {
     s.al_re = s.al_im = s.be_re = s.be_im = 0;
     s.cu1x_re = s.cu1x_im = s.cu2x_re = s.cu2x_im = s.cdx_re = s.cdx_im = 0;
     s.cu1d_re = s.cu1d_im = s.cdd_re = s.cdd_im = 0;
+    s.cup_re = s.cup_im = 0;
 }
 
-// the coefficients the FP32 vector kernels use, as float columns cf[i][ncol] (coalesced loads):
-// alpha, beta, and the five complex K_DX coefficients
-constexpr int kCoef = 14;
-__device__ __forceinline__ void store_coef(float *cf, uint32_t ncol, uint32_t c, ColState const &s) {
+__device__ __forceinline__ void store_coef(Ctx const &c, uint32_t col, ColState const &s) {
     double const v[kCoef] = {s.al_re, s.al_im, s.be_re, s.be_im, s.cu1x_re, s.cu1x_im, s.cu2x_re, s.cu2x_im,
                              s.cdx_re, s.cdx_im, s.cu1d_re, s.cu1d_im, s.cdd_re, s.cdd_im};
 #pragma unroll
-    for (int i = 0; i < kCoef; ++i) cf[size_t(i)*ncol + c] = float(v[i]);
+    for (int i = 0; i < kCoef; ++i) { c.cd[size_t(i)*c.ncol + col] = v[i]; c.cf[size_t(i)*c.ncol + col] = float(v[i]); }
 }
 
-__global__ void s_init(ColState *cs, Acc *accW, Acc *accV, uint32_t ncol, int32_t *counters, float *cf) {
-    uint32_t const c = blockIdx.x*blockDim.x + threadIdx.x;
-    if (c >= ncol) return;
-    ColState s{};
-    double const bn = sqrt(accW[c].n2);
-    s.bnorm = bn; s.tau = bn; s.theta = 0; s.eta_re = s.eta_im = 0;
-    s.tau_ref = bn; s.m_ref = 0;
-    s.rho_re = accW[c].re; s.rho_im = accW[c].im;
-    double const sr = accV[c].re, si = accV[c].im;
-    if (!(bn > 0)) { s.status = 3; freeze(s); }
-    else if (sr*sr + si*si == 0.0 || s.rho_re*s.rho_re + s.rho_im*s.rho_im == 0.0) { s.status = 2; freeze(s); atomicAdd(&counters[1], 1); }
-    else { cdiv(s.rho_re, s.rho_im, sr, si, s.al_re, s.al_im); s.status = 0; }
-    cs[c] = s;
-    store_coef(cf, ncol, c, s);
-    accW[c] = Acc{0, 0, 0, 0}; accV[c] = Acc{0, 0, 0, 0};
-}
+template <typename T> __device__ __forceinline__ T coef(Ctx const &c, int i, uint32_t col);
+template <> __device__ __forceinline__ float coef<float>(Ctx const &c, int i, uint32_t col) { return c.cf[size_t(i)*c.ncol + col]; }
+template <> __device__ __forceinline__ double coef<double>(Ctx const &c, int i, uint32_t col) { return c.cd[size_t(i)*c.ncol + col]; }
 
-// first half step m = 2n-1
-// the iteration number n (1-based) is counters[2] + 1: s_alpha advances it at the end of each
-// iteration, so a captured iteration replays unchanged
-__global__ void s_half1(ColState *cs, Acc *acc, uint32_t ncol, int32_t const *counters, double tol) {
-    uint32_t const c = blockIdx.x*blockDim.x + threadIdx.x;
-    if (c >= ncol) return;
-    int const m = 2*(counters[2] + 1) - 1;
-    ColState s = cs[c];
-    double const wn = sqrt(acc[c].n2);
-    acc[c].n2 = 0;
-    s.conv1 = 0;
-    if (0 != s.status) { cs[c] = s; return; }
-    double const th = wn/s.tau;
-    double const c2 = 1.0/(1.0 + th*th);
-    double const tau = s.tau*th*sqrt(c2);
-    // kd = theta_{m-1}^2 eta_{m-1} / alpha ; eta = c^2 alpha
-    double kr, ki; cdiv(s.theta*s.theta*s.eta_re, s.theta*s.theta*s.eta_im, s.al_re, s.al_im, kr, ki);
-    s.kd1_re = kr; s.kd1_im = ki;
-    s.et1_re = c2*s.al_re; s.et1_im = c2*s.al_im;
-    s.theta = th; s.tau = tau;
-    s.eta_re = s.et1_re; s.eta_im = s.et1_im;
-    if (tau*sqrt(double(m) + 1.0) <= tol*s.bnorm) s.conv1 = 1;
-    cs[c] = s;
-}
+// ------------------------------------------------------------------ per-source steps
+// Called by all threads of the last CTA of source s; thread j < 64 owns column s*64 + j.
 
-// second half step m = 2n: coefficients of K_DX, beta, rho; counts active columns
-// stall_level > 0 (FP32 correction sweeps only): a column whose estimate is already below
-// stall_level and whose tau has not halved within stall_window half steps has reached the
-// rounding floor of the sweep; it is frozen like a converged one (the refinement step then
-// restarts from the true FP64 residual)
-__global__ void s_half2(ColState *cs, Acc *acc, uint32_t ncol, double tol, int32_t *counters,
-                        double stall_level, int stall_window, float *cf) {
-    uint32_t const c = blockIdx.x*blockDim.x + threadIdx.x;
-    if (c >= ncol) return;
-    int const m = 2*(counters[2] + 1);
-    ColState s = cs[c];
-    double const wn = sqrt(acc[c].n2), rnr = acc[c].re, rni = acc[c].im;
-    acc[c] = Acc{0, 0, 0, 0};
-    if (0 != s.status) { freeze(s); cs[c] = s; store_coef(cf, ncol, c, s); return; }
-    // first-half coefficients: D1 = U1 + kd1 D0 ; X1 = X0 + et1 D1
-    double const k1r = s.kd1_re, k1i = s.kd1_im, e1r = s.et1_re, e1i = s.et1_im;
-    if (s.conv1) {
-        // X = X0 + et1 (U1 + kd1 D0); the column is done
-        s.cu1x_re = e1r; s.cu1x_im = e1i; s.cu2x_re = s.cu2x_im = 0;
-        s.cdx_re = e1r*k1r - e1i*k1i; s.cdx_im = e1r*k1i + e1i*k1r;
-        s.cu1d_re = s.cu1d_im = s.cdd_re = s.cdd_im = 0;
-        s.be_re = s.be_im = 0; s.al_re = s.al_im = 0;
-        s.status = 1;
-        cs[c] = s;
-        store_coef(cf, ncol, c, s);
-        return;
+// a source without active columns is done: counted once, and retired if retirement is on
+__device__ void finish_source(Ctx const &c, uint32_t s, bool any_active, bool count_iteration) {
+    if (0 != threadIdx.x) return;
+    SrcState &src = c.ss[s];
+    if (count_iteration) src.it += 1;
+    if (!any_active && !src.done) {
+        src.done = 1;
+        atomicSub(&c.ctl->n_active, 1);
+        if (c.retire) c.src_active[s] = 0;
     }
-    double const th = wn/s.tau;
-    double const c2 = 1.0/(1.0 + th*th);
-    double const tau = s.tau*th*sqrt(c2);
-    double k2r, k2i; cdiv(s.theta*s.theta*s.eta_re, s.theta*s.theta*s.eta_im, s.al_re, s.al_im, k2r, k2i);
-    double const e2r = c2*s.al_re, e2i = c2*s.al_im;
-    // D2 = U2 + kd2 D1 = U2 + kd2 U1 + kd2 kd1 D0
-    // X2 = X0 + et1 D1 + et2 D2 = X0 + (et1 + et2 kd2) U1 + et2 U2 + (et1 kd1 + et2 kd2 kd1) D0
-    double const kkr = k2r*k1r - k2i*k1i, kki = k2r*k1i + k2i*k1r;       // kd2 kd1
-    double const ekr = e2r*k2r - e2i*k2i, eki = e2r*k2i + e2i*k2r;       // et2 kd2
-    s.cu1x_re = e1r + ekr; s.cu1x_im = e1i + eki;
-    s.cu2x_re = e2r; s.cu2x_im = e2i;
-    double const a1r = e1r*k1r - e1i*k1i, a1i = e1r*k1i + e1i*k1r;       // et1 kd1
-    double const a2r = e2r*kkr - e2i*kki, a2i = e2r*kki + e2i*kkr;       // et2 kd2 kd1
-    s.cdx_re = a1r + a2r; s.cdx_im = a1i + a2i;
-    s.cu1d_re = k2r; s.cu1d_im = k2i;
-    s.cdd_re = kkr; s.cdd_im = kki;
-    s.theta = th; s.tau = tau; s.eta_re = e2r; s.eta_im = e2i;
-    // beta = rho_n / rho_{n-1}
-    double br, bi; cdiv(rnr, rni, s.rho_re, s.rho_im, br, bi);
-    s.be_re = br; s.be_im = bi; s.rho_re = rnr; s.rho_im = rni;
-    double const est = tau*sqrt(double(m) + 1.0);
-    if (tau <= 0.5*s.tau_ref) { s.tau_ref = tau; s.m_ref = m; }
-    if (est <= tol*s.bnorm) {
-        s.status = 1; s.be_re = s.be_im = 0; s.al_re = s.al_im = 0;
-    } else if (stall_level > 0 && m - s.m_ref > (est <= stall_level*s.bnorm ? stall_window : 4*stall_window)) {
-        // FP32 sweep: no halving of tau for stall_window half steps below the stall level, or
-        // for four times as long above it (a sweep that lost its way; the refinement restarts it)
-        s.status = 4; s.be_re = s.be_im = 0; s.al_re = s.al_im = 0;
-    } else if (rnr*rnr + rni*rni == 0.0) {
-        s.status = 2; s.be_re = s.be_im = 0; s.al_re = s.al_im = 0; atomicAdd(&counters[1], 1);
-    } else {
-        atomicAdd(&counters[0], 1);
+}
+
+// r = |W|^2, rt^H W, rt^H V
+__device__ void step_init(Ctx const &c, uint32_t s, double const (&r)[5]) {
+    int const j = threadIdx.x;
+    bool act = false;
+    if (j < 64) {
+        uint32_t const col = s*64 + j;
+        ColState st{};
+        double const bn = sqrt(r[0]);
+        st.bnorm = bn; st.tau = bn; st.scale = 1; st.res = (bn > 0) ? 1.0 : 0.0;
+        st.rho_re = r[1]; st.rho_im = r[2]; st.rhop_re = r[1]; st.rhop_im = r[2];
+        double const sr = r[3], si = r[4];
+        if (!(bn > 0)) { st.status = 3; freeze(st); }
+        else if (sr*sr + si*si == 0.0 || r[1]*r[1] + r[2]*r[2] == 0.0) { st.status = 2; freeze(st); atomicAdd(&c.ctl->breakdowns, 1); }
+        else { cdiv(st.rho_re, st.rho_im, sr, si, st.al_re, st.al_im); st.status = 0; }
+        c.cs[col] = st;
+        store_coef(c, col, st);
+        act = (0 == st.status);
     }
-    cs[c] = s;
-    store_coef(cf, ncol, c, s);
-}
-
-// alpha = rho / (rt^H V)
-__global__ void s_alpha(ColState *cs, Acc *acc, uint32_t ncol, int32_t *counters, float *cf) {
-    uint32_t const c = blockIdx.x*blockDim.x + threadIdx.x;
-    if (0 == c) counters[2] += 1;                   // next iteration (read only by later kernels)
-    if (c >= ncol) return;
-    ColState s = cs[c];
-    double const sr = acc[c].re, si = acc[c].im;
-    acc[c] = Acc{0, 0, 0, 0};
-    // the K_DX coefficients have been applied: finished columns keep all-zero coefficients
-    if (0 != s.status) { freeze(s); cs[c] = s; store_coef(cf, ncol, c, s); return; }
-    if (sr*sr + si*si == 0.0) { s.status = 2; freeze(s); atomicAdd(&counters[1], 1); cs[c] = s; store_coef(cf, ncol, c, s); return; }
-    cdiv(s.rho_re, s.rho_im, sr, si, s.al_re, s.al_im);
-    cs[c] = s;
-    store_coef(cf, ncol, c, s);
-}
-
-__global__ void s_estimate(ColState const *cs, uint32_t ncol, int m, double *out) {
-    // max over active or converged columns of tau sqrt(m+1)/|b|
-    __shared__ double r[256];
-    double v = 0;
-    for (uint32_t c = threadIdx.x; c < ncol; c += blockDim.x)
-        if (cs[c].bnorm > 0) v = fmax(v, cs[c].tau*sqrt(double(m) + 1.0)/cs[c].bnorm);
-    r[threadIdx.x] = v;
+    bool const any = __syncthreads_or(act);
+    if (0 == threadIdx.x) {
+        SrcState z{}; z.est_ref = 1.0; z.best = 1e300;
+        c.ss[s] = z;
+        c.upd[s] = 0;
+    }
     __syncthreads();
-    for (int k = 128; k > 0; k >>= 1) { if (threadIdx.x < k) r[threadIdx.x] = fmax(r[threadIdx.x], r[threadIdx.x + k]); __syncthreads(); }
-    if (0 == threadIdx.x) *out = r[0];
+    finish_source(c, s, any, false);
 }
 
-// ------------------------------------------------------------------ refinement helpers
+// first half step m = 2n-1: r = |w_{2n-1}|^2
+__device__ void step_half1(Ctx const &c, uint32_t s, double const (&r)[1]) {
+    int const j = threadIdx.x;
+    if (j >= 64) return;
+    uint32_t const col = s*64 + j;
+    ColState st = c.cs[col];
+    st.conv1 = 0;
+    if (0 == st.status) {
+        double const wn = sqrt(r[0]);
+        int const m = st.m + 1;
+        double const th = wn/st.tau;
+        double const c2 = 1.0/(1.0 + th*th);
+        double const tau = st.tau*th*sqrt(c2);
+        // kd = theta_{m-1}^2 eta_{m-1} / alpha ; eta = c^2 alpha
+        double kr, ki; cdiv(st.theta*st.theta*st.eta_re, st.theta*st.theta*st.eta_im, st.al_re, st.al_im, kr, ki);
+        st.kd1_re = kr; st.kd1_im = ki;
+        st.et1_re = c2*st.al_re; st.et1_im = c2*st.al_im;
+        st.theta = th; st.tau = tau; st.m = m;
+        st.eta_re = st.et1_re; st.eta_im = st.et1_im;
+        if (!c.mixed && tau*sqrt(double(m) + 1.0) <= c.tol*(c.abs_tol ? 1.0 : st.bnorm)) st.conv1 = 1;
+    }
+    c.cs[col] = st;
+}
 
-// R = B - AX (FP64) and per-column |R|^2 into colnorm (atomics)
-__global__ void __launch_bounds__(256) k_residual(double *R, double const *AX, uint32_t nnzb, uint16_t const *colindx,
-                                                  uint32_t const *subset, double *colnorm) {
-    __shared__ double red[4][64];
+// second half step m = 2n: r = |w_{2n}|^2, rt^H w_{2n}; coefficients of K_DX, beta; the
+// replacement decision of the source (FP32 recurrences)
+__device__ void step_half2(Ctx const &c, uint32_t s, double const (&r)[3]) {
+    __shared__ double est_max[64];
+    __shared__ int below[64];
+    int const j = threadIdx.x;
+    bool act = false;
+    if (j < 64) {
+        uint32_t const col = s*64 + j;
+        ColState st = c.cs[col];
+        double est = 0;
+        if (0 != st.status) {
+            freeze(st);
+        } else if (st.conv1) {
+            // X = X0 + et1 (U1 + kd1 D0); the column is done
+            double const k1r = st.kd1_re, k1i = st.kd1_im, e1r = st.et1_re, e1i = st.et1_im;
+            st.cu1x_re = e1r; st.cu1x_im = e1i; st.cu2x_re = st.cu2x_im = 0;
+            st.cdx_re = e1r*k1r - e1i*k1i; st.cdx_im = e1r*k1i + e1i*k1r;
+            st.cu1d_re = st.cu1d_im = st.cdd_re = st.cdd_im = 0;
+            st.be_re = st.be_im = 0; st.al_re = st.al_im = 0;
+            st.status = 1;
+            st.res = st.tau*sqrt(double(st.m) + 1.0)/st.bnorm;
+        } else {
+            double const wn = sqrt(r[0]), rnr = r[1], rni = r[2];
+            int const m = st.m + 1;
+            double const k1r = st.kd1_re, k1i = st.kd1_im, e1r = st.et1_re, e1i = st.et1_im;
+            double const th = wn/st.tau;
+            double const c2 = 1.0/(1.0 + th*th);
+            double const tau = st.tau*th*sqrt(c2);
+            double k2r, k2i; cdiv(st.theta*st.theta*st.eta_re, st.theta*st.theta*st.eta_im, st.al_re, st.al_im, k2r, k2i);
+            double const e2r = c2*st.al_re, e2i = c2*st.al_im;
+            // D2 = U2 + kd2 D1 = U2 + kd2 U1 + kd2 kd1 D0
+            // X2 = X0 + et1 D1 + et2 D2 = X0 + (et1 + et2 kd2) U1 + et2 U2 + (et1 kd1 + et2 kd2 kd1) D0
+            double const kkr = k2r*k1r - k2i*k1i, kki = k2r*k1i + k2i*k1r;       // kd2 kd1
+            double const ekr = e2r*k2r - e2i*k2i, eki = e2r*k2i + e2i*k2r;       // et2 kd2
+            st.cu1x_re = e1r + ekr; st.cu1x_im = e1i + eki;
+            st.cu2x_re = e2r; st.cu2x_im = e2i;
+            double const a1r = e1r*k1r - e1i*k1i, a1i = e1r*k1i + e1i*k1r;       // et1 kd1
+            double const a2r = e2r*kkr - e2i*kki, a2i = e2r*kki + e2i*kkr;       // et2 kd2 kd1
+            st.cdx_re = a1r + a2r; st.cdx_im = a1i + a2i;
+            st.cu1d_re = k2r; st.cu1d_im = k2i;
+            st.cdd_re = kkr; st.cdd_im = kki;
+            st.theta = th; st.tau = tau; st.eta_re = e2r; st.eta_im = e2i; st.m = m;
+            st.cup_re = th*th*e2r; st.cup_im = th*th*e2i;
+            // beta = rho_n / rho_{n-1}
+            double br, bi; cdiv(rnr, rni, st.rho_re, st.rho_im, br, bi);
+            st.rhop_re = st.rho_re; st.rhop_im = st.rho_im;
+            st.be_re = br; st.be_im = bi; st.rho_re = rnr; st.rho_im = rni;
+            double const bound = tau*sqrt(double(m) + 1.0);
+            est = bound/st.bnorm*st.scale;
+            if (!c.mixed && bound <= c.tol*(c.abs_tol ? 1.0 : st.bnorm)) {
+                st.status = 1; st.be_re = st.be_im = 0; st.al_re = st.al_im = 0;
+                st.res = bound/st.bnorm;
+            } else if (rnr*rnr + rni*rni == 0.0) {
+                st.status = 2; st.be_re = st.be_im = 0; st.al_re = st.al_im = 0; atomicAdd(&c.ctl->breakdowns, 1);
+            }
+        }
+        c.cs[col] = st;
+        store_coef(c, col, st);
+        act = (0 == st.status);
+        est_max[j] = act ? est : 0.0;
+        below[j] = act ? (est <= c.tol) : 1;
+    }
+    if (!c.mixed) return;
+    bool const any = __syncthreads_or(act);
+    if (0 == threadIdx.x) {
+        double e = 0; int all = 1;
+        for (int k = 0; k < 64; ++k) { e = fmax(e, est_max[k]); all &= below[k]; }
+        SrcState &src = c.ss[s];
+        int const u = any && (e < c.delta*src.est_ref || all || src.since + 1 >= c.gap);
+        src.upd = u;
+        c.upd[s] = uint8_t(u);
+    }
+}
+
+// end of an iteration: r = rt^H v_n; alpha = rho / (rt^H v_n)
+__device__ void step_alpha(Ctx const &c, uint32_t s, double const (&r)[2]) {
+    int const j = threadIdx.x;
+    bool act = false;
+    if (j < 64) {
+        uint32_t const col = s*64 + j;
+        ColState st = c.cs[col];
+        double const sr = r[0], si = r[1];
+        if (0 != st.status) freeze(st);
+        else if (sr*sr + si*si == 0.0) { st.status = 2; freeze(st); atomicAdd(&c.ctl->breakdowns, 1); }
+        else cdiv(st.rho_re, st.rho_im, sr, si, st.al_re, st.al_im);
+        c.cs[col] = st;
+        store_coef(c, col, st);
+        act = (0 == st.status);
+    }
+    bool const any = __syncthreads_or(act);
+    if (0 == threadIdx.x) {
+        SrcState &src = c.ss[s];
+        src.since = src.upd ? 0 : src.since + 1;
+        src.upd = 0;
+        c.upd[s] = 0;
+    }
+    finish_source(c, s, any, true);
+}
+
+// residual replacement: r = |B - A X64|^2, rt^H W with the new W
+__device__ void step_replace(Ctx const &c, uint32_t s, double const (&r)[3]) {
+    __shared__ double resmax[64];
+    int const j = threadIdx.x;
+    bool act = false;
+    if (j < 64) {
+        uint32_t const col = s*64 + j;
+        ColState st = c.cs[col];
+        double const res = (st.bnorm > 0) ? sqrt(r[0])/st.bnorm : 0.0;
+        if (0 == st.status) {
+            st.res = res;
+            if (res <= c.tol) {
+                st.status = 1; freeze(st);
+            } else {
+                double const est = st.tau*sqrt(double(st.m) + 1.0)/st.bnorm;
+                st.scale = fmax(1.0, res/fmax(est, 1e-300));
+                double const rnr = r[1], rni = r[2];
+                if (rnr*rnr + rni*rni == 0.0) {
+                    st.status = 2; freeze(st); atomicAdd(&c.ctl->breakdowns, 1);
+                } else {
+                    double br, bi; cdiv(rnr, rni, st.rhop_re, st.rhop_im, br, bi);
+                    st.be_re = br; st.be_im = bi; st.rho_re = rnr; st.rho_im = rni;
+                }
+            }
+        }
+        c.cs[col] = st;
+        store_coef(c, col, st);
+        act = (0 == st.status);
+        resmax[j] = act ? res : 0.0;
+    }
+    bool any = __syncthreads_or(act);
+    __shared__ int fb;
+    if (0 == threadIdx.x) {
+        double e = 0;
+        bool finite = true;
+        for (int k = 0; k < 64; ++k) { e = fmax(e, resmax[k]); finite = finite && isfinite(resmax[k]); }
+        SrcState &src = c.ss[s];
+        src.est_ref = e;
+        src.updates += 1;
+        // progress: the largest true residual fell by 10 % since the best one so far
+        if (e < 0.9*src.best) { src.best = e; src.stall = 0; } else src.stall += 1;
+        fb = any && (!finite || src.stall >= c.stall_limit);
+        if (fb) { src.fallback = 1; src.nonfinite = !finite; }
+    }
+    __syncthreads();
+    if (fb) {
+        // the FP32 recurrences stopped making progress: the active columns continue in FP64
+        if (j < 64) {
+            ColState &st = c.cs[s*64 + j];
+            if (0 == st.status) { st.status = 5; freeze(st); store_coef(c, s*64 + j, st); }
+        }
+        any = false;
+    }
+    // a source that finished here is retired now; its last iteration counts
+    finish_source(c, s, any, !any);
+}
+
+// final true residuals: r = |B - A X|^2
+__device__ void step_final(Ctx const &c, uint32_t s, double const (&r)[1]) {
+    int const j = threadIdx.x;
+    if (j >= 64) return;
+    uint32_t const col = s*64 + j;
+    c.cs[col].res = sqrt(r[0]);      // |b| = 1: the right-hand sides are unit columns
+}
+
+// ------------------------------------------------------------------ vector kernels
+// one CTA of 256 threads per unit; thread (q, j): column j, rows q*16 .. q*16+15, re and im
+
+template <typename T>
+__global__ void k_set_diag(T *W, T *U1, uint32_t const *subset, uint32_t ncols_blk) {
+    uint32_t const c = blockIdx.x; int const i = threadIdx.x;
+    if (c < ncols_blk) {
+        size_t const o = size_t(subset[c])*kBlk + size_t(i)*64 + i;
+        W[o] = T(1); U1[o] = T(1);
+    }
+}
+
+// initial reductions: |W|^2, rt^H W, rt^H V
+template <typename T>
+__global__ void __launch_bounds__(256) k_init_dots(T const *W, T const *V, Ctx const c) {
+    uint32_t s, lo, hi;
+    if (!unit_range(c, c.active, blockIdx.x, s, lo, hi)) return;
     int const j = threadIdx.x & 63, q = threadIdx.x >> 6;
-    for (uint32_t b = blockIdx.x; b < nnzb; b += gridDim.x) {
-        uint32_t const c = colindx[b];
-        bool const diag = (subset[c] == b);
-        double n2 = 0;
+    double v[5] = {0, 0, 0, 0, 0};
+    for (uint32_t k = lo; k < hi; ++k) {
+        size_t const b = c.src_blocks[k];
+#pragma unroll 4
+        for (int i = q*16; i < q*16 + 16; ++i) {
+            size_t const o = b*kBlk + i*64 + j;
+            uint32_t const idx = uint32_t(o);
+            double const tr = double(shadow_t<T>(c.seed, idx)), ti = double(shadow_t<T>(c.seed, idx + 4096u));
+            double const xr = W[o], xi = W[o + 4096], yr = V[o], yi = V[o + 4096];
+            v[0] += xr*xr + xi*xi;
+            v[1] += tr*xr + ti*xi; v[2] += tr*xi - ti*xr;     // conj(rt) w
+            v[3] += tr*yr + ti*yi; v[4] += tr*yi - ti*yr;
+        }
+    }
+    double out[5];
+    if (reduce_source<5>(c, blockIdx.x, s, v, out)) step_init(c, s, out);
+}
+
+// K_A: U2 = U1 - alpha V ; |W - alpha AU1|^2
+template <typename T>
+__global__ void __launch_bounds__(256) k_A(T *U2, T const *U1, T const *V, T const *W, T const *AU1, Ctx const c) {
+    uint32_t s, lo, hi;
+    if (!unit_range(c, c.active, blockIdx.x, s, lo, hi)) return;
+    int const j = threadIdx.x & 63, q = threadIdx.x >> 6;
+    uint32_t const col = s*64 + j;
+    T const ar = coef<T>(c, 0, col), ai = coef<T>(c, 1, col);
+    double n2 = 0;
+    for (uint32_t k = lo; k < hi; ++k) {
+        size_t const b = c.src_blocks[k];
+        T n2t = T(0);                 // 16-row partial sums in the vector precision
 #pragma unroll 8
         for (int i = q*16; i < q*16 + 16; ++i) {
-            size_t const o = size_t(b)*kBlk + i*64 + j;
-            double const rr = ((diag && i == j) ? 1.0 : 0.0) - AX[o], ri = -AX[o + 4096];
-            R[o] = rr; R[o + 4096] = ri;
-            n2 += rr*rr + ri*ri;
+            size_t const o = b*kBlk + i*64 + j;
+            T const vr = V[o], vi = V[o + 4096];
+            U2[o] = fma(ai, vi, fma(-ar, vr, U1[o]));
+            U2[o + 4096] = fma(-ai, vr, fma(-ar, vi, U1[o + 4096]));
+            T const ur = AU1[o], ui = AU1[o + 4096];
+            T const wr = fma(ai, ui, fma(-ar, ur, W[o])), wi = fma(-ai, ur, fma(-ar, ui, W[o + 4096]));
+            n2t = fma(wr, wr, fma(wi, wi, n2t));
         }
-        red[q][j] = n2;
-        __syncthreads();
-        if (0 == q) atomicAdd(&colnorm[c*64 + j], red[0][j] + red[1][j] + red[2][j] + red[3][j]);
-        __syncthreads();
+        n2 += double(n2t);
+    }
+    double const v[1] = {n2};
+    double out[1];
+    if (reduce_source<1>(c, blockIdx.x, s, v, out)) step_half1(c, s, out);
+}
+
+// K_C: W = W - alpha (AU1 + AU2) ; |W|^2 and rt^H W
+template <typename T>
+__global__ void __launch_bounds__(256) k_C(T *W, T const *AU1, T const *AU2, Ctx const c) {
+    uint32_t s, lo, hi;
+    if (!unit_range(c, c.active, blockIdx.x, s, lo, hi)) return;
+    int const j = threadIdx.x & 63, q = threadIdx.x >> 6;
+    uint32_t const col = s*64 + j;
+    T const ar = coef<T>(c, 0, col), ai = coef<T>(c, 1, col);
+    double v[3] = {0, 0, 0};
+    for (uint32_t k = lo; k < hi; ++k) {
+        size_t const b = c.src_blocks[k];
+        T n2 = T(0), dr = T(0), di = T(0);
+#pragma unroll 8
+        for (int i = q*16; i < q*16 + 16; ++i) {
+            size_t const o = b*kBlk + i*64 + j;
+            T const sr = AU1[o] + AU2[o], si = AU1[o + 4096] + AU2[o + 4096];
+            T const wr = fma(ai, si, fma(-ar, sr, W[o])), wi = fma(-ai, sr, fma(-ar, si, W[o + 4096]));
+            W[o] = wr; W[o + 4096] = wi;
+            uint32_t const idx = uint32_t(o);
+            T const tr = shadow_t<T>(c.seed, idx), ti = shadow_t<T>(c.seed, idx + 4096u);
+            n2 = fma(wr, wr, fma(wi, wi, n2));
+            dr = fma(tr, wr, fma(ti, wi, dr)); di = fma(tr, wi, fma(-ti, wr, di));
+        }
+        v[0] += double(n2); v[1] += double(dr); v[2] += double(di);
+    }
+    double out[3];
+    if (reduce_source<3>(c, blockIdx.x, s, v, out)) step_half2(c, s, out);
+}
+
+// K_DX: X += cu1x U1 + cu2x U2 + cdx D ; D = U2 + cu1d U1 + cdd D ; U1 = W + beta U2
+template <typename T>
+__global__ void __launch_bounds__(256) k_DX(T *X, T *D, T *U1, T const *U2, T const *W, Ctx const c) {
+    uint32_t s, lo, hi;
+    if (!unit_range(c, c.active, blockIdx.x, s, lo, hi)) return;
+    int const j = threadIdx.x & 63, q = threadIdx.x >> 6;
+    uint32_t const col = s*64 + j;
+    T const g_r = coef<T>(c, 2, col), g_i = coef<T>(c, 3, col);
+    T const a_r = coef<T>(c, 4, col), a_i = coef<T>(c, 5, col);
+    T const b_r = coef<T>(c, 6, col), b_i = coef<T>(c, 7, col);
+    T const c_r = coef<T>(c, 8, col), c_i = coef<T>(c, 9, col);
+    T const d_r = coef<T>(c, 10, col), d_i = coef<T>(c, 11, col);
+    T const e_r = coef<T>(c, 12, col), e_i = coef<T>(c, 13, col);
+    for (uint32_t k = lo; k < hi; ++k) {
+        size_t const b = c.src_blocks[k];
+#pragma unroll 4
+        for (int i = q*16; i < q*16 + 16; ++i) {
+            size_t const o = b*kBlk + i*64 + j;
+            T const u1r = U1[o], u1i = U1[o + 4096], u2r = U2[o], u2i = U2[o + 4096];
+            T const dr = D[o], di = D[o + 4096];
+            T xr = X[o], xi = X[o + 4096];
+            xr = fma(a_r, u1r, fma(-a_i, u1i, xr)); xi = fma(a_r, u1i, fma(a_i, u1r, xi));
+            xr = fma(b_r, u2r, fma(-b_i, u2i, xr)); xi = fma(b_r, u2i, fma(b_i, u2r, xi));
+            xr = fma(c_r, dr, fma(-c_i, di, xr));   xi = fma(c_r, di, fma(c_i, dr, xi));
+            X[o] = xr; X[o + 4096] = xi;
+            D[o] = fma(d_r, u1r, fma(-d_i, u1i, fma(e_r, dr, fma(-e_i, di, u2r))));
+            D[o + 4096] = fma(d_r, u1i, fma(d_i, u1r, fma(e_r, di, fma(e_i, dr, u2i))));
+            U1[o] = fma(g_r, u2r, fma(-g_i, u2i, W[o]));
+            U1[o + 4096] = fma(g_r, u2i, fma(g_i, u2r, W[o + 4096]));
+        }
     }
 }
 
-// W = U1 = (T) R, D = 0  (right-hand side of a correction sweep)
-template <typename T>
-__global__ void __launch_bounds__(256) k_set_from(T *W, T *U1, T *D, double const *R, size_t n) {
-    for (size_t e = blockIdx.x*size_t(blockDim.x) + threadIdx.x; e < n; e += size_t(gridDim.x)*blockDim.x) {
-        T const r = T(R[e]);
-        W[e] = r; U1[e] = r; D[e] = T(0);
+// K_DX in FP32 with 16-byte accesses: thread (column group of 4, row group of 4 rows); each row
+// moves 10 float4 loads and 6 float4 stores
+__device__ __forceinline__ float4 ld4(float const *p) { return *reinterpret_cast<float4 const*>(p); }
+__device__ __forceinline__ void st4(float *p, float4 v) { *reinterpret_cast<float4*>(p) = v; }
+__device__ __forceinline__ float4 ldc4(Ctx const &c, int i, uint32_t col) { return ld4(c.cf + size_t(i)*c.ncol + col); }
+
+__global__ void __launch_bounds__(256, 2) k_DX32(float *X, float *D, float *U1, float const *U2, float const *W,
+                                                 Ctx const c) {
+    uint32_t s, lo, hi;
+    if (!unit_range(c, c.active, blockIdx.x, s, lo, hi)) return;
+    int const cg = threadIdx.x & 15, rg = threadIdx.x >> 4;
+    int const j0 = cg*4;
+    uint32_t const col = s*64 + j0;
+    float4 const g_r = ldc4(c, 2, col), g_i = ldc4(c, 3, col);
+    float4 const a_r = ldc4(c, 4, col), a_i = ldc4(c, 5, col);
+    float4 const b_r = ldc4(c, 6, col), b_i = ldc4(c, 7, col);
+    float4 const c_r = ldc4(c, 8, col), c_i = ldc4(c, 9, col);
+    float4 const d_r = ldc4(c, 10, col), d_i = ldc4(c, 11, col);
+    float4 const e_r = ldc4(c, 12, col), e_i = ldc4(c, 13, col);
+    for (uint32_t k = lo; k < hi; ++k) {
+        size_t const b = c.src_blocks[k];
+#pragma unroll 2
+        for (int i = rg*4; i < rg*4 + 4; ++i) {
+            size_t const o = b*kBlk + i*64 + j0;
+            float4 const u1r = ld4(U1 + o), u1i = ld4(U1 + o + 4096), u2r = ld4(U2 + o), u2i = ld4(U2 + o + 4096);
+            float4 const dr = ld4(D + o), di = ld4(D + o + 4096), wr = ld4(W + o), wi = ld4(W + o + 4096);
+            float4 xr = ld4(X + o), xi = ld4(X + o + 4096);
+            float4 nd_r, nd_i, nu_r, nu_i;
+#define A43G_DX_LANE(f) \
+            xr.f = fmaf(a_r.f, u1r.f, fmaf(-a_i.f, u1i.f, xr.f)); xi.f = fmaf(a_r.f, u1i.f, fmaf(a_i.f, u1r.f, xi.f)); \
+            xr.f = fmaf(b_r.f, u2r.f, fmaf(-b_i.f, u2i.f, xr.f)); xi.f = fmaf(b_r.f, u2i.f, fmaf(b_i.f, u2r.f, xi.f)); \
+            xr.f = fmaf(c_r.f, dr.f, fmaf(-c_i.f, di.f, xr.f));   xi.f = fmaf(c_r.f, di.f, fmaf(c_i.f, dr.f, xi.f)); \
+            nd_r.f = fmaf(d_r.f, u1r.f, fmaf(-d_i.f, u1i.f, fmaf(e_r.f, dr.f, fmaf(-e_i.f, di.f, u2r.f)))); \
+            nd_i.f = fmaf(d_r.f, u1i.f, fmaf(d_i.f, u1r.f, fmaf(e_r.f, di.f, fmaf(e_i.f, dr.f, u2i.f)))); \
+            nu_r.f = fmaf(g_r.f, u2r.f, fmaf(-g_i.f, u2i.f, wr.f)); \
+            nu_i.f = fmaf(g_r.f, u2i.f, fmaf(g_i.f, u2r.f, wi.f));
+            A43G_DX_LANE(x) A43G_DX_LANE(y) A43G_DX_LANE(z) A43G_DX_LANE(w)
+#undef A43G_DX_LANE
+            st4(X + o, xr); st4(X + o + 4096, xi);
+            st4(D + o, nd_r); st4(D + o + 4096, nd_i);
+            st4(U1 + o, nu_r); st4(U1 + o + 4096, nu_i);
+        }
     }
 }
 
-// X64 += (double) dX  (end of an FP32 correction sweep)
+// K_E: V = AU1 + beta (AU2 + beta V) ; rt^H V
 template <typename T>
-__global__ void __launch_bounds__(256) k_accumulate(double *X64, T const *dX, size_t n) {
-    for (size_t e = blockIdx.x*size_t(blockDim.x) + threadIdx.x; e < n; e += size_t(gridDim.x)*blockDim.x)
-        X64[e] += double(dX[e]);
+__global__ void __launch_bounds__(256) k_E(T *V, T const *AU1, T const *AU2, Ctx const c) {
+    uint32_t s, lo, hi;
+    if (!unit_range(c, c.active, blockIdx.x, s, lo, hi)) return;
+    int const j = threadIdx.x & 63, q = threadIdx.x >> 6;
+    uint32_t const col = s*64 + j;
+    T const fr = coef<T>(c, 2, col), fi = coef<T>(c, 3, col);
+    double v[2] = {0, 0};
+    for (uint32_t k = lo; k < hi; ++k) {
+        size_t const b = c.src_blocks[k];
+        T dr = T(0), di = T(0);
+#pragma unroll 8
+        for (int i = q*16; i < q*16 + 16; ++i) {
+            size_t const o = b*kBlk + i*64 + j;
+            T const vr = V[o], vi = V[o + 4096];
+            T const t1r = fma(-fi, vi, fma(fr, vr, AU2[o])), t1i = fma(fi, vr, fma(fr, vi, AU2[o + 4096]));
+            T const sr = fma(-fi, t1i, fma(fr, t1r, AU1[o])), si = fma(fi, t1r, fma(fr, t1i, AU1[o + 4096]));
+            V[o] = sr; V[o + 4096] = si;
+            uint32_t const idx = uint32_t(o);
+            T const tr = shadow_t<T>(c.seed, idx), ti = shadow_t<T>(c.seed, idx + 4096u);
+            dr = fma(tr, sr, fma(ti, si, dr)); di = fma(tr, si, fma(-ti, sr, di));
+        }
+        v[0] += double(dr); v[1] += double(di);
+    }
+    double out[2];
+    if (reduce_source<2>(c, blockIdx.x, s, v, out)) step_alpha(c, s, out);
 }
 
-__global__ void k_max_ratio(double const *colnorm, uint32_t ncol, double *out) {
-    __shared__ double r[256];
-    double v = 0;
-    for (uint32_t c = threadIdx.x; c < ncol; c += blockDim.x) v = fmax(v, sqrt(colnorm[c]));
-    r[threadIdx.x] = v;
-    __syncthreads();
-    for (int k = 128; k > 0; k >>= 1) { if (threadIdx.x < k) r[threadIdx.x] = fmax(r[threadIdx.x], r[threadIdx.x + k]); __syncthreads(); }
-    if (0 == threadIdx.x) *out = r[0];
+// ------------------------------------------------------------------ residual replacement
+// (FP32 recurrences; the units of sources without a replacement in this iteration return at once)
+
+// X64 += X32, X32 = 0
+__global__ void __launch_bounds__(256) k_flush(double *X64, float *X32, Ctx const c, uint8_t const *sel) {
+    uint32_t s, lo, hi;
+    if (!unit_range(c, sel, blockIdx.x, s, lo, hi)) return;
+    for (uint32_t k = lo; k < hi; ++k) {
+        size_t const b = c.src_blocks[k];
+        for (int t = threadIdx.x; t < kBlk/4; t += blockDim.x) {
+            float4 const x = ld4(X32 + b*kBlk + 4*t);
+            double2 *p = reinterpret_cast<double2*>(X64 + b*kBlk + 4*t);
+            double2 a = p[0], d = p[1];
+            a.x += x.x; a.y += x.y; d.x += x.z; d.y += x.w;
+            p[0] = a; p[1] = d;
+            st4(X32 + b*kBlk + 4*t, make_float4(0.f, 0.f, 0.f, 0.f));
+        }
+    }
+}
+
+// R = B - AX64 (B: unit diagonal block of the source); W = R - cup AD; |R|^2 and rt^H W
+__global__ void __launch_bounds__(256) k_replace(float *W, double const *AX64, float const *AD, Ctx const c) {
+    uint32_t s, lo, hi;
+    if (!unit_range(c, c.upd, blockIdx.x, s, lo, hi)) return;
+    if (c.active && !c.active[s]) return;
+    int const j = threadIdx.x & 63, q = threadIdx.x >> 6;
+    uint32_t const col = s*64 + j;
+    double const pr = c.cs[col].cup_re, pi = c.cs[col].cup_im;
+    uint32_t const diag = c.subset[s];
+    double v[3] = {0, 0, 0};
+    for (uint32_t k = lo; k < hi; ++k) {
+        size_t const b = c.src_blocks[k];
+        bool const isdiag = (b == diag);
+#pragma unroll 4
+        for (int i = q*16; i < q*16 + 16; ++i) {
+            size_t const o = b*kBlk + i*64 + j;
+            double const rr = ((isdiag && i == j) ? 1.0 : 0.0) - AX64[o], ri = -AX64[o + 4096];
+            double const dr = AD[o], di = AD[o + 4096];
+            float const wr = float(rr - (pr*dr - pi*di)), wi = float(ri - (pr*di + pi*dr));
+            W[o] = wr; W[o + 4096] = wi;
+            uint32_t const idx = uint32_t(o);
+            double const tr = shadow32(c.seed, idx), ti = shadow32(c.seed, idx + 4096u);
+            v[0] += rr*rr + ri*ri;
+            v[1] += tr*double(wr) + ti*double(wi); v[2] += tr*double(wi) - ti*double(wr);
+        }
+    }
+    double out[3];
+    if (reduce_source<3>(c, blockIdx.x, s, v, out)) step_replace(c, s, out);
+}
+
+// U1 = W + beta U2 after a replacement (the new beta)
+__global__ void __launch_bounds__(256) k_U1(float *U1, float const *W, float const *U2, Ctx const c) {
+    uint32_t s, lo, hi;
+    if (!unit_range(c, c.upd, blockIdx.x, s, lo, hi)) return;
+    if (c.active && !c.active[s]) return;
+    int const cg = threadIdx.x & 15, rg = threadIdx.x >> 4;
+    uint32_t const col = s*64 + cg*4;
+    float4 const g_r = ldc4(c, 2, col), g_i = ldc4(c, 3, col);
+    for (uint32_t k = lo; k < hi; ++k) {
+        size_t const b = c.src_blocks[k];
+        for (int i = rg*4; i < rg*4 + 4; ++i) {
+            size_t const o = b*kBlk + i*64 + cg*4;
+            float4 const u2r = ld4(U2 + o), u2i = ld4(U2 + o + 4096), wr = ld4(W + o), wi = ld4(W + o + 4096);
+            float4 nr, ni;
+#define A43G_U1_LANE(f) nr.f = fmaf(g_r.f, u2r.f, fmaf(-g_i.f, u2i.f, wr.f)); ni.f = fmaf(g_r.f, u2i.f, fmaf(g_i.f, u2r.f, wi.f));
+            A43G_U1_LANE(x) A43G_U1_LANE(y) A43G_U1_LANE(z) A43G_U1_LANE(w)
+#undef A43G_U1_LANE
+            st4(U1 + o, nr); st4(U1 + o + 4096, ni);
+        }
+    }
+}
+
+// |B - AX|^2 per column of every source (final residuals; AX in FP64)
+__global__ void __launch_bounds__(256) k_final(double const *AX, Ctx const c) {
+    uint32_t s, lo, hi;
+    if (!unit_range(c, nullptr, blockIdx.x, s, lo, hi)) return;
+    int const j = threadIdx.x & 63, q = threadIdx.x >> 6;
+    uint32_t const diag = c.subset[s];
+    double v[1] = {0};
+    for (uint32_t k = lo; k < hi; ++k) {
+        size_t const b = c.src_blocks[k];
+        bool const isdiag = (b == diag);
+        for (int i = q*16; i < q*16 + 16; ++i) {
+            size_t const o = b*kBlk + i*64 + j;
+            double const rr = ((isdiag && i == j) ? 1.0 : 0.0) - AX[o], ri = -AX[o + 4096];
+            v[0] += rr*rr + ri*ri;
+        }
+    }
+    double out[1];
+    if (reduce_source<1>(c, blockIdx.x, s, v, out)) step_final(c, s, out);
+}
+
+// FP64 continuation of the sources flagged in sel: W = U1 = B - AX, with a source whose FP64
+// solution is not finite restarted from zero (W = U1 = B, X = 0)
+__global__ void __launch_bounds__(256) k_start64(double *W, double *U1, double *X, double const *AX, Ctx const c,
+                                                 uint8_t const *sel) {
+    uint32_t s, lo, hi;
+    if (!unit_range(c, sel, blockIdx.x, s, lo, hi)) return;
+    uint32_t const diag = c.subset[s];
+    int const bad = c.ss[s].nonfinite;               // the FP32 phase's record, uniform
+    for (uint32_t k = lo; k < hi; ++k) {
+        size_t const b = c.src_blocks[k];
+        bool const isdiag = (b == diag);
+        for (int t = threadIdx.x; t < kBlk; t += blockDim.x) {
+            int const reim = t >> 12, i = (t >> 6) & 63, j = t & 63;
+            double const one = (isdiag && 0 == reim && i == j) ? 1.0 : 0.0;
+            double const r = bad ? one : one - AX[b*kBlk + t];
+            W[b*kBlk + t] = r; U1[b*kBlk + t] = r;
+            if (bad) X[b*kBlk + t] = 0.0;
+        }
+    }
 }
 
 // rho[c][i] = X[subset[c]][re, im][i][i] / pi
@@ -565,7 +775,12 @@ __global__ void k_export_rho(double *rho, T const *X, uint32_t const *subset, ui
     rho[2*(size_t(c)*64 + i) + 1] = double(X[o + 4096])*f;
 }
 
-unsigned grid_for(uint32_t nnzb) { return std::max(1u, std::min<uint32_t>(nnzb, 148u*8)); }
+// chunks per source: at least one CTA per SM for a lone source, about eight per SM in total
+uint32_t chunks_for(DevicePlan const &dp) {
+    uint32_t const n = std::max(1u, dp.nCols);
+    uint32_t const want = std::max<uint32_t>(148u, (148u*8u + n - 1)/n);
+    return std::max(1u, std::min(want, std::max(1u, dp.max_src_blocks)));
+}
 
 } // namespace
 
@@ -579,75 +794,154 @@ bool TfqmrVectors::alloc(size_t nreals, size_t elem_bytes) {
 
 void TfqmrVectors::release() {
     X.release(); W.release(); U1.release(); U2.release(); V.release(); D.release();
-    AU1.release(); AU2.release(); Rt.release(); n = 0; elem = 0;
+    AU1.release(); AU2.release(); n = 0; elem = 0;
 }
 
 SolverWorkspace::~SolverWorkspace() {
-    if (host_counters) cudaFreeHost(host_counters);
+    if (host_ctl) cudaFreeHost(host_ctl);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
 }
 
 namespace {
 
-// half steps without a halving of tau after which a column of an FP32 sweep counts as stalled
-constexpr int kStallWindow = 60;
+// restores the plan's retirement state (all sources active, retirement off) on every exit
+struct RetireGuard {
+    DevicePlan &dp;
+    cudaStream_t st;
+    ~RetireGuard() {
+        dp.retire = false;
+        if (dp.src_active.ptr) cudaMemsetAsync(dp.src_active.ptr, 1, std::max<uint32_t>(dp.nCols, 1), st);
+    }
+};
 
-struct InnerResult { int iterations = 0; int converged = 0; int breakdowns = 0; double estimate = 0; double applications = 0; };
+struct Prepared {
+    Ctx c;
+    uint32_t units = 0;
+};
 
-// tfQMR on the vectors of precision T whose W, U1 hold the right-hand side and D is zero;
-// the solution is accumulated into Xs (precision TX), which holds the starting guess of the
-// correction (zero for a plain solve)
-template <typename T, typename TX>
-bool tfqmr_inner(DevicePlan &dp, SolverWorkspace &ws, TfqmrVectors &v, TX *Xs, double tol, int maxit, int check_every,
-                 uint32_t seed, cudaStream_t st, InnerResult &res, int echo, double stall_level = 0) {
-    uint32_t const nnzb = dp.nnzb, ncol = dp.nCols*64;
-    uint16_t const *ci = dptr<uint16_t>(dp.colindx);
-    auto *cs = dptr<ColState>(ws.colstate);
-    Acc *accA = (Acc*)(cs + ncol);     // two accumulator banks after the states
-    auto *accB = accA + ncol;
-    float *cf = reinterpret_cast<float*>(accB + ncol);   // kCoef float columns for the FP32 kernels
-    int32_t *cnt = dptr<int32_t>(ws.counters);
-    unsigned const g = grid_for(nnzb), gs = (ncol + 255)/256;
-    TX *X = Xs;
+bool prepare(DevicePlan &dp, SolverWorkspace &ws, a43g_solve_options_t const &opt, bool mixed, bool retire,
+             Prepared &p) {
+    uint32_t const nsrc = dp.nCols, ncol = nsrc*64;
+    uint32_t const nch = chunks_for(dp);
+    uint32_t const units = nsrc*nch;
+    auto r256 = [](size_t n) { return (n + 255) & ~size_t(255); };
+    size_t const bytes = r256(size_t(ncol)*sizeof(ColState)) + r256(size_t(ncol)*kCoef*sizeof(double)) +
+                         r256(size_t(ncol)*kCoef*sizeof(float)) + r256(size_t(nsrc)*sizeof(SrcState)) +
+                         r256(nsrc) + r256(sizeof(Ctl));
+    if (!ws.state.alloc(bytes)) return false;
+    if (!ws.part.alloc(std::max<size_t>(16, size_t(units)*kSlots*64*sizeof(double)))) return false;
+    if (!ws.tickets.alloc(std::max<size_t>(16, size_t(nsrc)*sizeof(uint32_t)))) return false;
+    if (!ws.host_ctl) A43G_CUDA_TRY(cudaMallocHost(&ws.host_ctl, 64));
+    if (!ws.ev0) { A43G_CUDA_TRY(cudaEventCreate(&ws.ev0)); A43G_CUDA_TRY(cudaEventCreate(&ws.ev1)); }
+    char *q = static_cast<char*>(ws.state.ptr);
+    auto take = [&](size_t n) { char *r = q; q += (n + 255) & ~size_t(255); return r; };
+    Ctx &c = p.c;
+    c = Ctx{};
+    c.cs = reinterpret_cast<ColState*>(take(size_t(ncol)*sizeof(ColState)));
+    c.cd = reinterpret_cast<double*>(take(size_t(ncol)*kCoef*sizeof(double)));
+    c.cf = reinterpret_cast<float*>(take(size_t(ncol)*kCoef*sizeof(float)));
+    c.ss = reinterpret_cast<SrcState*>(take(size_t(nsrc)*sizeof(SrcState)));
+    c.upd = reinterpret_cast<uint8_t*>(take(nsrc));
+    c.ctl = reinterpret_cast<Ctl*>(take(sizeof(Ctl)));
+    c.src_start = dptr<uint32_t>(dp.src_start);
+    c.src_blocks = dptr<uint32_t>(dp.src_blocks);
+    c.subset = dptr<uint32_t>(dp.subset_dev);
+    c.src_active = dptr<uint8_t>(dp.src_active);
+    c.active = retire ? c.src_active : nullptr;
+    c.nch = nch; c.ncol = ncol;
+    c.part = dptr<double>(ws.part);
+    c.tickets = dptr<uint32_t>(ws.tickets);
+    c.seed = uint32_t(opt.seed*2654435761ull + 12345u);
+    c.tol = opt.tolerance;
+    c.delta = (opt.update_factor > 0 && opt.update_factor < 1) ? opt.update_factor : 0.1;
+    c.gap = (opt.update_gap > 0) ? opt.update_gap : 10;
+    c.mixed = mixed ? 1 : 0;
+    c.retire = retire ? 1 : 0;
+    c.stall_limit = 8;
+    c.abs_tol = 0;
+    p.units = units;
+    return true;
+}
+
+// the operator on the solver's vectors with the source selection `sel` (nullptr: all sources)
+template <typename T>
+bool apply(DevicePlan &dp, T *y, T const *x, uint8_t const *sel, bool retire, cudaStream_t st) {
+    // the action's kernels read DevicePlan::src_active when retire is set; a replacement runs the
+    // action on the sources flagged in upd instead, through a temporary swap of the buffer pointer
+    void *const keep = dp.src_active.ptr;
+    bool const keep_retire = dp.retire;
+    if (sel) { dp.src_active.ptr = const_cast<uint8_t*>(sel); dp.retire = true; }
+    else dp.retire = retire;
+    bool const ok = launch_action<T>(dp, y, x, dptr<uint16_t>(dp.colindx), st);
+    dp.src_active.ptr = keep;
+    dp.retire = keep_retire;
+    return ok;
+}
+
+struct Result { int iterations = 0; double applications = 0; };
+
+// tfQMR on vectors of precision T whose W, U1 hold B and D, X are zero; mixed: X is X32 and the
+// solution accumulates in X64 (with AX64 the FP64 scratch of the replacements)
+// mask: the sources that take part (the others are padding of a batch, or sources an earlier
+// phase has finished), retired before the first kernel
+template <typename T>
+bool run(DevicePlan &dp, SolverWorkspace &ws, TfqmrVectors &v, Prepared &p, T *X, int maxit, int check_every,
+         double *X64, double *AX64, cudaStream_t st, Result &res, int echo, std::vector<uint8_t> const &mask) {
+    Ctx const &c = p.c;
+    uint32_t const nsrc = dp.nCols;
+    bool const mixed = c.mixed != 0;
+    bool const retire = c.retire != 0;
     T *W = dptr<T>(v.W), *U1 = dptr<T>(v.U1), *U2 = dptr<T>(v.U2), *V = dptr<T>(v.V);
     T *D = dptr<T>(v.D), *AU1 = dptr<T>(v.AU1), *AU2 = dptr<T>(v.AU2);
-    A43G_CUDA_TRY(cudaMemsetAsync(accA, 0, 2*size_t(ncol)*sizeof(Acc), st));
-    A43G_CUDA_TRY(cudaMemsetAsync(cnt, 0, 4*sizeof(int32_t), st));
+    uint32_t live = 0;
+    for (auto f : mask) live += f ? 1u : 0u;
+    bool const partial = live < nsrc;
+    Ctl init{}; init.n_active = int32_t(live);
+    A43G_CUDA_TRY(cudaMemsetAsync(ws.state.ptr, 0, ws.state.bytes, st));
+    A43G_CUDA_TRY(cudaMemcpyAsync(c.ctl, &init, sizeof(Ctl), cudaMemcpyHostToDevice, st));
+    A43G_CUDA_TRY(cudaMemsetAsync(ws.tickets.ptr, 0, size_t(nsrc)*sizeof(uint32_t), st));
+    A43G_CUDA_TRY(cudaMemcpyAsync(dp.src_active.ptr, mask.data(), nsrc, cudaMemcpyHostToDevice, st));
     // V = A U1
-    if (!launch_action<T>(dp, AU1, U1, ci, st)) return false;
+    if (!apply<T>(dp, AU1, U1, nullptr, retire, st)) return false;
     A43G_CUDA_TRY(cudaMemcpyAsync(V, AU1, v.n*sizeof(T), cudaMemcpyDeviceToDevice, st));
     res.applications += 1;
-    k_init_dots<T><<<g, 256, 0, st>>>(W, V, nnzb, ci, accA, accB, seed);
+    {   // the sources outside the mask are skipped by the initial reductions too
+        Ctx ci = c;
+        if (partial) ci.active = c.src_active;
+        k_init_dots<T><<<p.units, 256, 0, st>>>(W, V, ci);
+    }
     count_launch();
-    s_init<<<gs, 256, 0, st>>>(cs, accA, accB, ncol, cnt, cf);
-    count_launch();
-    // one iteration; counters[0] counts the columns still active after it
     auto iteration = [&]() -> bool {
-        A43G_CUDA_TRY(cudaMemsetAsync(cnt, 0, sizeof(int32_t), st));
-        k_A<T><<<g, 256, 0, st>>>(U2, U1, V, W, AU1, nnzb, ci, cs, accA, cf, ncol);
+        k_A<T><<<p.units, 256, 0, st>>>(U2, U1, V, W, AU1, c);
         count_launch();
-        s_half1<<<gs, 256, 0, st>>>(cs, accA, ncol, cnt, tol);
+        if (!apply<T>(dp, AU2, U2, nullptr, retire, st)) return false;
+        k_C<T><<<p.units, 256, 0, st>>>(W, AU1, AU2, c);
         count_launch();
-        if (!launch_action<T>(dp, AU2, U2, ci, st)) return false;
-        k_C<T><<<g, 256, 0, st>>>(W, AU1, AU2, nnzb, ci, cs, accA, seed, cf, ncol);
+        if constexpr (sizeof(T) == 4) k_DX32<<<p.units, 256, 0, st>>>(X, D, U1, U2, W, c);
+        else k_DX<T><<<p.units, 256, 0, st>>>(X, D, U1, U2, W, c);
         count_launch();
-        s_half2<<<gs, 256, 0, st>>>(cs, accA, ncol, tol, cnt, stall_level, kStallWindow, cf);
-        count_launch();
-        if constexpr (sizeof(T) == 4 && sizeof(TX) == 4)
-            k_DX32<<<g, 256, 0, st>>>(X, D, U1, U2, W, nnzb, ci, cf, ncol);
-        else
-            k_DX<T, TX><<<g, 256, 0, st>>>(X, D, U1, U2, W, nnzb, ci, cs, cf, ncol);
-        count_launch();
-        if (!launch_action<T>(dp, AU1, U1, ci, st)) return false;
-        k_E<T><<<g, 256, 0, st>>>(V, AU1, AU2, nnzb, ci, cs, accA, seed, cf, ncol);
-        count_launch();
-        s_alpha<<<gs, 256, 0, st>>>(cs, accA, ncol, cnt, cf);
+        if constexpr (sizeof(T) == 4) {
+            if (mixed) {
+                // residual replacement of the sources flagged in upd (the launches of the other
+                // sources' units return at once)
+                k_flush<<<p.units, 256, 0, st>>>(X64, X, c, c.upd);
+                count_launch();
+                if (!apply<double>(dp, AX64, X64, c.upd, retire, st)) return false;
+                if (!apply<float>(dp, AU1, D, c.upd, retire, st)) return false;    // A d (AU1 is free here)
+                k_replace<<<p.units, 256, 0, st>>>(W, AX64, AU1, c);
+                count_launch();
+                k_U1<<<p.units, 256, 0, st>>>(U1, W, U2, c);
+                count_launch();
+            }
+        }
+        if (!apply<T>(dp, AU1, U1, nullptr, retire, st)) return false;
+        k_E<T><<<p.units, 256, 0, st>>>(V, AU1, AU2, c);
         count_launch();
         return true;
     };
-    // the iteration is captured once into a CUDA graph and replayed (one launch instead of
-    // about 25 per iteration); not on the legacy default stream, which cannot be captured
+    // one iteration captured as a CUDA graph and replayed (not on the legacy default stream,
+    // which cannot be captured)
     cudaGraphExec_t exec = nullptr;
     uint64_t per_iteration = 0;
     if (st != nullptr && !std::getenv("A43G_NO_GRAPH")) {
@@ -668,195 +962,269 @@ bool tfqmr_inner(DevicePlan &dp, SolverWorkspace &ws, TfqmrVectors &v, TX *Xs, d
         count_launches(uint64_t(0) - per_iteration);   // captured, not launched: counted per replay
     }
     struct GraphGuard { cudaGraphExec_t &e; ~GraphGuard() { if (e) cudaGraphExecDestroy(e); } } guard{exec};
-    uint64_t const captured = per_iteration;
     int it = 0;
+    int const every = std::max(1, check_every);
     for (it = 1; it <= maxit; ++it) {
-        bool const check = (0 == it % check_every) || (it == maxit);
         if (exec) {
             A43G_CUDA_TRY(cudaGraphLaunch(exec, st));
-            count_launches(captured);
+            count_launches(per_iteration);
         } else if (!iteration()) {
             return false;
         }
         res.applications += 2;
-        if (check) {
-            A43G_CUDA_TRY(cudaMemcpyAsync(ws.host_counters, cnt, 4*sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+        if (0 == it % every || it == maxit) {
+            A43G_CUDA_TRY(cudaMemcpyAsync(ws.host_ctl, c.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, st));
             A43G_CUDA_TRY(cudaStreamSynchronize(st));
+            Ctl const *h = reinterpret_cast<Ctl const*>(ws.host_ctl);
             if (echo > 1) {
-                double *est = dptr<double>(ws.colnorm) + ncol;
-                s_estimate<<<1, 256, 0, st>>>(cs, ncol, 2*it, est);
-                count_launch();
-                double e = 0;
-                A43G_CUDA_TRY(cudaMemcpyAsync(&e, est, sizeof(double), cudaMemcpyDeviceToHost, st));
-                A43G_CUDA_TRY(cudaStreamSynchronize(st));
-                std::printf("# tfqmr<%s> iteration %d: %d of %u columns active, %d breakdowns, estimate %.3e\n",
-                            sizeof(T) == 8 ? "f64" : "f32", it, ws.host_counters[0], ncol, ws.host_counters[1], e);
+                std::printf("# tfqmr<%s> iteration %d: %d of %u sources active, %d breakdowns\n",
+                            mixed ? "f32+f64" : "f64", it, h->n_active, nsrc, h->breakdowns);
                 std::fflush(stdout);
             }
-            if (0 == ws.host_counters[0]) break;
+            if (0 == h->n_active) break;
         }
     }
     res.iterations += std::min(it, maxit);
     A43G_CUDA_TRY(cudaGetLastError());
-    double *est = dptr<double>(ws.colnorm) + ncol;     // one spare double after the column norms
-    s_estimate<<<1, 256, 0, st>>>(cs, ncol, 2*std::min(it, maxit), est);
-    count_launch();
-    A43G_CUDA_TRY(cudaMemcpyAsync(ws.host_counters, cnt, 4*sizeof(int32_t), cudaMemcpyDeviceToHost, st));
-    double e = 0;
-    A43G_CUDA_TRY(cudaMemcpyAsync(&e, est, sizeof(double), cudaMemcpyDeviceToHost, st));
+    // the host copy of the mask must outlive the asynchronous copy above
     A43G_CUDA_TRY(cudaStreamSynchronize(st));
-    res.estimate = e;
-    res.breakdowns += ws.host_counters[1];
-    res.converged = (e <= tol) ? 1 : 0;
-    if (echo > 0) std::printf("# tfqmr<%s> %d iterations, residual estimate %.3e (tolerance %.1e)\n",
-                              sizeof(T) == 8 ? "f64" : "f32", std::min(it, maxit), e, tol);
     return true;
 }
 
-bool workspace_common(DevicePlan &dp, SolverWorkspace &ws) {
-    size_t const ncol = size_t(dp.nCols)*64;
-    if (!ws.colstate.alloc(ncol*(sizeof(ColState) + 2*sizeof(Acc) + kCoef*sizeof(float)))) return false;
-    if (!ws.counters.alloc(64)) return false;
-    if (!ws.colnorm.alloc((ncol + 8)*sizeof(double))) return false;
-    if (!ws.host_counters) A43G_CUDA_TRY(cudaMallocHost(&ws.host_counters, 64));
-    if (!ws.ev0) { A43G_CUDA_TRY(cudaEventCreate(&ws.ev0)); A43G_CUDA_TRY(cudaEventCreate(&ws.ev1)); }
-    return true;
-}
-
-// true relative residual max_col |B - A X| / |B| for an FP64 solution X64 (|B col| = 1); R64 receives B - AX
-bool residual64(DevicePlan &dp, SolverWorkspace &ws, double const *X64, double *R64, double *AX64, cudaStream_t st,
-                double &rmax, double &applications) {
-    uint32_t const ncol = dp.nCols*64;
-    if (!launch_action<double>(dp, AX64, X64, dptr<uint16_t>(dp.colindx), st)) return false;
-    applications += 1;
-    double *cn = dptr<double>(ws.colnorm);
-    A43G_CUDA_TRY(cudaMemsetAsync(cn, 0, (ncol + 8)*sizeof(double), st));
-    k_residual<<<grid_for(dp.nnzb), 256, 0, st>>>(R64, AX64, dp.nnzb, dptr<uint16_t>(dp.colindx),
-                                                  dptr<uint32_t>(dp.subset_dev), cn);
-                                                  count_launch();
-    k_max_ratio<<<1, 256, 0, st>>>(cn, ncol, cn + ncol);
-    count_launch();
-    A43G_CUDA_TRY(cudaMemcpyAsync(&rmax, cn + ncol, sizeof(double), cudaMemcpyDeviceToHost, st));
-    A43G_CUDA_TRY(cudaStreamSynchronize(st));
-    return true;
+// FP64 solution X64 and operator scratch AX64, and the recurrence vectors of the precision
+// (the FP64 tfQMR keeps its solution in X64; its vector set's X is not used)
+bool ensure_vectors(SolverWorkspace &ws, DevicePlan &dp, bool mixed) {
+    size_t const n = size_t(dp.nnzb)*kBlk;
+    if (!ws.X64.alloc(n*8) || !ws.AX64.alloc(n*8)) return false;
+    return mixed ? ws.v32.alloc(n, 4) : ws.v64.alloc(n, 8);
 }
 
 } // namespace
 
+size_t solve_bytes(DevicePlan const &dp, int precision) {
+    size_t const n = size_t(dp.nnzb)*kBlk;
+    return (A43G_F32 == precision) ? n*(8*4 + 2*8) : n*(9*8);
+}
+
 int solve(GreenPlan &hp, DevicePlan &dp, SolverWorkspace &ws, a43g_solve_options_t const &opt,
-          void *Xout, double *rho, a43g_solve_stats_t *stats, cudaStream_t st) {
+          void *Xout, double *rho, a43g_solve_stats_t *stats, cudaStream_t st, SourceStats *per_source) {
     *stats = a43g_solve_stats_t{};
     if (0 == dp.nnzb) { stats->converged = 1; return A43G_OK; }
     if (!(opt.tolerance > 0) || opt.max_iterations < 1) { set_error("tolerance must be > 0 and max_iterations >= 1"); return A43G_ERR_ARGUMENT; }
-    if (!dp.subset_dev.ptr) {
-        std::vector<uint32_t> sub(hp.subset.begin(), hp.subset.end());
-        if (!dp.subset_dev.alloc(std::max<size_t>(16, sub.size()*4))) return A43G_ERR_MEMORY;
-        if (cudaSuccess != cudaMemcpy(dp.subset_dev.ptr, sub.data(), sub.size()*4, cudaMemcpyHostToDevice)) { set_error("copy of subset"); return A43G_ERR_CUDA; }
-    }
-    if (!workspace_common(dp, ws)) return A43G_ERR_MEMORY;
+    if (A43G_F64 != opt.precision && A43G_F32 != opt.precision) { set_error("precision must be A43G_F64 or A43G_F32"); return A43G_ERR_ARGUMENT; }
+    (void)hp;
+    bool const mixed = (A43G_F32 == opt.precision);
+    bool const retire = 0 == (opt.flags & A43G_SOLVE_NO_RETIRE);
+    uint32_t const nsrc = dp.nCols;
+    uint32_t const live = (per_source && per_source->live_sources) ? std::min(per_source->live_sources, nsrc) : nsrc;
+    std::vector<uint8_t> mask(nsrc, 0);
+    std::fill(mask.begin(), mask.begin() + live, uint8_t(1));
+    if (!ensure_vectors(ws, dp, mixed)) return A43G_ERR_MEMORY;
+    // projector scratch for both precisions before the iteration is captured (no allocation
+    // may happen inside a stream capture)
+    if (!ensure_dyadic_scratch(dp, 8) || !ensure_prj_part(dp, 8)) return A43G_ERR_MEMORY;
+    Prepared p;
+    if (!prepare(dp, ws, opt, mixed, retire || live < nsrc, p)) return A43G_ERR_MEMORY;
+    RetireGuard rg{dp, st};
     size_t const n = size_t(dp.nnzb)*kBlk;
-    int const check = std::max(1, opt.check_every);
-    uint32_t const seed = uint32_t(opt.seed*2654435761ull + 12345u);
-    cudaEventRecord(ws.ev0, st);
-    InnerResult res;
-    unsigned const g = grid_for(dp.nnzb);
-    if (A43G_F64 == opt.precision) {
-        if (!ws.v64.alloc(n, 8)) return A43G_ERR_MEMORY;
-        auto &v = ws.v64;
-        // W = U1 = B (unit diagonal blocks), D = X = 0
-        for (DeviceBuffer *b : {&v.W, &v.U1, &v.D, &v.X})
-            if (cudaSuccess != cudaMemsetAsync(b->ptr, 0, n*8, st)) { set_error("memset"); return A43G_ERR_CUDA; }
-        k_set_diag<double><<<dp.nCols, 64, 0, st>>>(dptr<double>(v.W), dptr<double>(v.U1), dptr<uint32_t>(dp.subset_dev), dp.nCols);
-        count_launch();
-        if (!tfqmr_inner<double, double>(dp, ws, v, dptr<double>(v.X), opt.tolerance, opt.max_iterations, check, seed, st, res, opt.echo)) return A43G_ERR_CUDA;
-        // true residual of the FP64 solution (uses U2/AU1 as scratch)
-        double rmax = 0;
-        if (!residual64(dp, ws, dptr<double>(v.X), dptr<double>(v.U2), dptr<double>(v.AU1), st, rmax, res.applications)) return A43G_ERR_CUDA;
-        stats->residual_max = rmax;
-        stats->refinements = 0;
-        if (Xout) cudaMemcpyAsync(Xout, v.X.ptr, n*8, cudaMemcpyDeviceToDevice, st);
-        if (rho) {
-            DeviceBuffer rb; if (!rb.alloc(size_t(dp.nCols)*128*8)) return A43G_ERR_MEMORY;
-            k_export_rho<double><<<dp.nCols, 64, 0, st>>>(dptr<double>(rb), dptr<double>(v.X), dptr<uint32_t>(dp.subset_dev), dp.nCols);
-            count_launch();
-            cudaMemcpyAsync(rho, rb.ptr, size_t(dp.nCols)*128*8, cudaMemcpyDeviceToHost, st);
-            cudaStreamSynchronize(st);
-        }
-    } else if (A43G_F32 == opt.precision) {
-        // mixed precision: X64 = 0, R64 = B; repeat: solve A dX = R in FP32, X64 += dX, R64 = B - A X64
-        if (!ws.v32.alloc(n, 4)) return A43G_ERR_MEMORY;
-        if (!ws.X64.alloc(n*8) || !ws.R64.alloc(n*8) || !ws.AX64.alloc(n*8)) return A43G_ERR_MEMORY;
-        double *X64 = dptr<double>(ws.X64), *R64 = dptr<double>(ws.R64), *AX64 = dptr<double>(ws.AX64);
-        if (cudaSuccess != cudaMemsetAsync(X64, 0, n*8, st)) { set_error("memset"); return A43G_ERR_CUDA; }
+    A43G_CUDA_TRY_RC(cudaEventRecord(ws.ev0, st));
+    Result res;
+    double *X64 = dptr<double>(ws.X64);
+    std::vector<SrcState> ss1;                  // the FP32 phase's per-source results
+    std::vector<int> it1(nsrc, 0);
+    if (mixed) {
         auto &v = ws.v32;
-        double rmax = 1.0;
-        // R64 = B - A*0 = B
-        if (!residual64(dp, ws, X64, R64, AX64, st, rmax, res.applications)) return A43G_ERR_CUDA;
-        int const maxref = std::max(1, opt.max_refinements);
-        double const inner_tol = (opt.inner_tolerance > 0) ? opt.inner_tolerance : 1e-4;
-        int ref = 0, first_sweep = 0;
-        for (ref = 0; ref < maxref && rmax > opt.tolerance; ++ref) {
-            k_set_from<float><<<g*8, 256, 0, st>>>(dptr<float>(v.W), dptr<float>(v.U1), dptr<float>(v.D), R64, n);
-            count_launch();
-            if (cudaSuccess != cudaMemsetAsync(v.X.ptr, 0, n*4, st)) { set_error("memset"); return A43G_ERR_CUDA; }
-            int left = opt.max_iterations - res.iterations;
-            if (left < 1) break;
-            // a correction sweep that needs far more iterations than the first one has stagnated
-            // at the FP32 rounding floor: end it, recompute the true residual and restart (with a
-            // new shadow vector), which is cheaper than letting it run
-            if (ref > 0) left = std::min(left, std::max(2*first_sweep, 100));
-            // relative inner tolerance, not tighter than needed for the outer target
-            double const itol = std::max(inner_tol, 0.5*opt.tolerance/rmax);
-            // FP32 correction sweep (keeping its solution in FP64 does not lower the FP32 residual
-            // floor, measured, so the correction is accumulated once per sweep)
-            // columns stalled below 10x the sweep tolerance end the sweep (FP32 rounding floor)
-            if (!tfqmr_inner<float, float>(dp, ws, v, dptr<float>(v.X), itol, left, check, seed + 7919u*uint32_t(ref + 1), st, res,
-                                           opt.echo, 10*itol)) return A43G_ERR_CUDA;
-            if (0 == ref) first_sweep = res.iterations;
-            k_accumulate<float><<<g*8, 256, 0, st>>>(X64, dptr<float>(v.X), n);
-            count_launch();
-            if (!residual64(dp, ws, X64, R64, AX64, st, rmax, res.applications)) return A43G_ERR_CUDA;
-            if (opt.echo > 0) std::printf("# refinement %d: FP64 residual %.3e after %d iterations in total\n",
-                                          ref + 1, rmax, res.iterations);
+        for (DeviceBuffer *b : {&v.W, &v.U1, &v.D, &v.X}) A43G_CUDA_TRY_RC(cudaMemsetAsync(b->ptr, 0, n*4, st));
+        A43G_CUDA_TRY_RC(cudaMemsetAsync(X64, 0, n*8, st));
+        k_set_diag<float><<<nsrc, 64, 0, st>>>(dptr<float>(v.W), dptr<float>(v.U1), dptr<uint32_t>(dp.subset_dev), nsrc);
+        count_launch();
+        if (!run<float>(dp, ws, v, p, dptr<float>(v.X), opt.max_iterations, opt.check_every, X64,
+                        dptr<double>(ws.AX64), st, res, opt.echo, mask))
+            return A43G_ERR_CUDA;
+        // the rest of every column's FP32 correction into the FP64 solution
+        k_flush<<<p.units, 256, 0, st>>>(X64, dptr<float>(v.X), p.c, nullptr);
+        count_launch();
+        ss1.resize(nsrc);
+        A43G_CUDA_TRY_RC(cudaMemcpyAsync(ss1.data(), p.c.ss, nsrc*sizeof(SrcState), cudaMemcpyDeviceToHost, st));
+        A43G_CUDA_TRY_RC(cudaStreamSynchronize(st));
+        // sources whose FP32 recurrences stalled, or that ran out of iterations, continue in FP64
+        // from their FP64 solution: tfQMR on (H - E S) X = B with the initial guess X64
+        std::vector<uint8_t> fb(nsrc, 0);
+        uint32_t nfb = 0;
+        for (uint32_t k = 0; k < live; ++k) {
+            it1[k] = ss1[k].done ? ss1[k].it : res.iterations;
+            if (ss1[k].fallback) { fb[k] = 1; ++nfb; }
         }
-        stats->refinements = ref;
-        stats->residual_max = rmax;
-        if (Xout) cudaMemcpyAsync(Xout, X64, n*8, cudaMemcpyDeviceToDevice, st);
-        if (rho) {
-            DeviceBuffer rb; if (!rb.alloc(size_t(dp.nCols)*128*8)) return A43G_ERR_MEMORY;
-            k_export_rho<double><<<dp.nCols, 64, 0, st>>>(dptr<double>(rb), X64, dptr<uint32_t>(dp.subset_dev), dp.nCols);
+        int const left = opt.max_iterations - res.iterations;
+        if (nfb && left > 0) {
+            if (!ws.v64.alloc(n, 8)) return A43G_ERR_MEMORY;
+            auto &w = ws.v64;
+            Prepared p2;
+            a43g_solve_options_t o2 = opt;
+            if (!prepare(dp, ws, o2, false, true, p2)) return A43G_ERR_MEMORY;
+            p2.c.abs_tol = 1;
+            // R = B - A X64 of the continuing sources into W and U1; D = 0
+            if (!apply<double>(dp, dptr<double>(ws.AX64), X64, nullptr, false, st)) return A43G_ERR_CUDA;
+            A43G_CUDA_TRY_RC(cudaMemsetAsync(w.D.ptr, 0, n*8, st));
+            A43G_CUDA_TRY_RC(cudaMemcpyAsync(dp.src_active.ptr, fb.data(), nsrc, cudaMemcpyHostToDevice, st));
+            k_start64<<<p2.units, 256, 0, st>>>(dptr<double>(w.W), dptr<double>(w.U1), X64, dptr<double>(ws.AX64),
+                                               p2.c, dptr<uint8_t>(dp.src_active));
             count_launch();
-            cudaMemcpyAsync(rho, rb.ptr, size_t(dp.nCols)*128*8, cudaMemcpyDeviceToHost, st);
-            cudaStreamSynchronize(st);
+            if (!run<double>(dp, ws, w, p2, X64, left, opt.check_every, nullptr, nullptr, st, res, opt.echo, fb))
+                return A43G_ERR_CUDA;
+            std::vector<SrcState> ss2(nsrc);
+            A43G_CUDA_TRY_RC(cudaMemcpyAsync(ss2.data(), p2.c.ss, nsrc*sizeof(SrcState), cudaMemcpyDeviceToHost, st));
+            A43G_CUDA_TRY_RC(cudaStreamSynchronize(st));
+            for (uint32_t k = 0; k < live; ++k) if (fb[k]) it1[k] += ss2[k].done ? ss2[k].it : left;
         }
     } else {
-        set_error("precision must be A43G_F64 or A43G_F32");
-        return A43G_ERR_ARGUMENT;
+        auto &v = ws.v64;
+        for (DeviceBuffer *b : {&v.W, &v.U1, &v.D}) A43G_CUDA_TRY_RC(cudaMemsetAsync(b->ptr, 0, n*8, st));
+        A43G_CUDA_TRY_RC(cudaMemsetAsync(X64, 0, n*8, st));
+        k_set_diag<double><<<nsrc, 64, 0, st>>>(dptr<double>(v.W), dptr<double>(v.U1), dptr<uint32_t>(dp.subset_dev), nsrc);
+        count_launch();
+        if (!run<double>(dp, ws, v, p, X64, opt.max_iterations, opt.check_every, nullptr, nullptr, st, res, opt.echo, mask))
+            return A43G_ERR_CUDA;
     }
-    cudaEventRecord(ws.ev1, st);
-    if (cudaSuccess != cudaEventSynchronize(ws.ev1)) { set_error("event synchronize"); return A43G_ERR_CUDA; }
+    // true residual of every column's FP64 solution (the whole operator, no source skipped)
+    dp.retire = false;
+    if (!launch_action<double>(dp, dptr<double>(ws.AX64), X64, dptr<uint16_t>(dp.colindx), st)) return A43G_ERR_CUDA;
+    res.applications += 1;
+    k_final<<<p.units, 256, 0, st>>>(dptr<double>(ws.AX64), p.c);
+    count_launch();
+    if (Xout) A43G_CUDA_TRY_RC(cudaMemcpyAsync(Xout, X64, n*8, cudaMemcpyDeviceToDevice, st));
+    if (rho) {
+        double *rb = dptr<double>(ws.AX64);      // the residual scratch is free again
+        k_export_rho<double><<<nsrc, 64, 0, st>>>(rb, X64, dptr<uint32_t>(dp.subset_dev), nsrc);
+        count_launch();
+        A43G_CUDA_TRY_RC(cudaMemcpyAsync(rho, rb, size_t(nsrc)*128*8, cudaMemcpyDeviceToHost, st));
+    }
+    A43G_CUDA_TRY_RC(cudaEventRecord(ws.ev1, st));
+    // per-column and per-source results
+    std::vector<ColState> cs(size_t(nsrc)*64);
+    std::vector<SrcState> ss(nsrc);
+    Ctl ctl{};
+    A43G_CUDA_TRY_RC(cudaMemcpyAsync(cs.data(), p.c.cs, cs.size()*sizeof(ColState), cudaMemcpyDeviceToHost, st));
+    A43G_CUDA_TRY_RC(cudaMemcpyAsync(ss.data(), p.c.ss, ss.size()*sizeof(SrcState), cudaMemcpyDeviceToHost, st));
+    A43G_CUDA_TRY_RC(cudaMemcpyAsync(&ctl, p.c.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, st));
+    if (cudaSuccess != cudaEventSynchronize(ws.ev1) || cudaSuccess != cudaStreamSynchronize(st)) {
+        set_error(std::string("solve: ") + cudaGetErrorString(cudaGetLastError()));
+        return A43G_ERR_CUDA;
+    }
     float ms = 0; cudaEventElapsedTime(&ms, ws.ev0, ws.ev1);
+    if (!mixed) for (uint32_t k = 0; k < live; ++k) it1[k] = ss[k].done ? ss[k].it : res.iterations;
+    double rmax = 0;
+    int updates = 0;
+    for (size_t k = 0; k < size_t(live)*64; ++k) rmax = std::max(rmax, std::isfinite(cs[k].res) ? cs[k].res : 1e300);
+    if (mixed) for (uint32_t k = 0; k < live; ++k) updates = std::max(updates, ss1[k].updates);
+    int fallbacks = 0;
+    if (mixed) for (uint32_t k = 0; k < live; ++k) fallbacks += ss1[k].fallback;
     stats->seconds = ms*1e-3;
     stats->iterations = res.iterations;
-    stats->breakdowns = res.breakdowns;
-    stats->residual_estimate = res.estimate;
+    stats->refinements = updates;
+    stats->breakdowns = ctl.breakdowns;
+    stats->residual_max = rmax;
     stats->operator_applications = res.applications;
-    stats->converged = (stats->residual_max <= opt.tolerance) ? 1 : 0;
+    stats->converged = (rmax <= opt.tolerance) ? 1 : 0;
+    stats->fp64_sources = fallbacks;
+    double est = 0;
+    for (size_t k = 0; k < size_t(live)*64; ++k)
+        if (cs[k].bnorm > 0) est = std::max(est, cs[k].tau*std::sqrt(double(cs[k].m) + 1.0)/cs[k].bnorm);
+    stats->residual_estimate = est;
+    if (per_source) {
+        per_source->iterations.assign(it1.begin(), it1.end());
+        per_source->residual.assign(nsrc, 0.0);
+        per_source->updates.assign(nsrc, 0);
+        per_source->fallback.assign(nsrc, 0);
+        for (uint32_t k = 0; k < nsrc; ++k) {
+            if (mixed) { per_source->updates[k] = ss1[k].updates; per_source->fallback[k] = ss1[k].fallback; }
+            for (int j = 0; j < 64; ++j) {
+                double const r = cs[size_t(k)*64 + j].res;
+                per_source->residual[k] = std::max(per_source->residual[k], std::isfinite(r) ? r : 1e300);
+            }
+        }
+    }
+    if (opt.echo > 0)
+        std::printf("# tfqmr<%s> %d iterations, %d replacements, %d sources continued in FP64, true residual %.3e (tolerance %.1e)\n",
+                    mixed ? "f32+f64" : "f64", res.iterations, updates, fallbacks, rmax, opt.tolerance);
     cudaError_t const e = cudaGetLastError();
     if (cudaSuccess != e) { set_error(std::string("solve: ") + cudaGetErrorString(e)); return A43G_ERR_CUDA; }
     return A43G_OK;
 }
 
-int solve_batched(GreenPlan &hp, DevicePlan &dp, SolverWorkspace &ws, a43g_solve_options_t const &opt,
+} // namespace a43g
+
+namespace a43g {
+
+// Solves of many (energy, k-point) pairs on the geometry of the one-pair plan hp, in waves of
+// up to `wave` pairs: each wave is one block-sparse system (GreenPlan::replicate) whose sources
+// retire as they finish.  The last wave is filled up with copies of its last pair whose sources
+// are retired from the start.
+int solve_batched(GreenPlan &hp, DevicePlan &dp, BatchCache &bc, a43g_solve_options_t const &opt,
                   int32_t n, double const *energies, double const *kpoints, double dVol,
                   double *rho, a43g_solve_stats_t *stats, cudaStream_t st) {
-    for (int32_t i = 0; i < n; ++i) {
-        hp.set_energy(energies[2*i], energies[2*i + 1], dVol);
-        auto const err = hp.set_kpoint(kpoints + 3*i);
+    if (n <= 0) return A43G_OK;
+    if (hp.npairs != 1) { set_error("solve_batched needs a one-pair plan"); return A43G_ERR_ARGUMENT; }
+    for (int32_t i = 0; i < n; ++i)
+        for (int d = 0; d < 3; ++d)
+            if (!(std::abs(kpoints[3*i + d]) < 0.503)) { set_error("k-point components must be below 0.503 (units of 2 pi / cell)"); return A43G_ERR_ARGUMENT; }
+    uint32_t const nsrc = hp.nCols;
+    uint32_t wave = opt.batch > 0 ? uint32_t(opt.batch) : 0;
+    if (0 == wave) {
+        // as many pairs as fit 85 % of the free memory next to what the batch plan holds already
+        size_t freeb = 0, total = 0;
+        if (cudaSuccess != cudaMemGetInfo(&freeb, &total)) { set_error("cudaMemGetInfo"); return A43G_ERR_CUDA; }
+        size_t const held = bc.npairs ? solve_bytes(*bc.dev, opt.precision) : 0;
+        size_t const per = solve_bytes(dp, opt.precision) + size_t(dp.nnzb)*kBlk*2 + (size_t(64) << 20);
+        wave = uint32_t(std::max<size_t>(1, (size_t(0.85*double(freeb + held)))/per));
+    }
+    wave = std::min<uint32_t>(wave, uint32_t(n));
+    wave = std::min<uint32_t>(wave, 65535u/std::max(1u, nsrc));
+    if (wave < 1) { set_error("a pair has more sources than a batch holds"); return A43G_ERR_UNSUPPORTED; }
+    if (bc.npairs != wave) {
+        bc.ws.reset(); bc.dev.reset(); bc.npairs = 0;    // release the old batch first
+        auto const err = bc.host.replicate(hp, wave);
         if (!err.empty()) { set_error(err); return A43G_ERR_ARGUMENT; }
-        if (!upload_values(hp, dp)) return A43G_ERR_CUDA;
-        int const rc = solve(hp, dp, ws, opt, nullptr, rho ? rho + size_t(i)*dp.nCols*128 : nullptr, &stats[i], st);
+        bc.dev.reset(new DevicePlan());
+        bc.ws.reset(new SolverWorkspace());
+        bc.dev->prj_chunk = dp.prj_chunk; bc.dev->add_blocks = dp.add_blocks;
+        if (!upload_plan(bc.host, *bc.dev)) return A43G_ERR_CUDA;
+        bc.dev->local_variant = dp.local_variant; bc.dev->use_tc = dp.use_tc;
+        bc.npairs = wave;
+    }
+    // the caller's potential and atom matrices as they are now
+    bc.host.Vcell = hp.Vcell;
+    bc.host.AtomMatricesIn = hp.AtomMatricesIn;
+    for (int32_t w0 = 0; w0 < n; w0 += int32_t(wave)) {
+        uint32_t const live = std::min<uint32_t>(wave, uint32_t(n - w0));
+        for (uint32_t p = 0; p < wave; ++p) {
+            uint32_t const i = w0 + std::min(p, live - 1);
+            auto const err = bc.host.set_pair(p, energies[2*i], energies[2*i + 1], dVol, kpoints + 3*size_t(i));
+            if (!err.empty()) { set_error(err); return A43G_ERR_ARGUMENT; }
+        }
+        if (!upload_values(bc.host, *bc.dev)) return A43G_ERR_CUDA;
+        a43g_solve_stats_t ws_stats{};
+        SourceStats per;
+        per.live_sources = live*nsrc;
+        std::vector<double> rb(rho ? size_t(wave)*nsrc*128 : 0);
+        a43g_solve_options_t o = opt;
+        o.flags &= ~A43G_SOLVE_NO_RETIRE;            // padding sources are retired from the start
+        int const rc = solve(bc.host, *bc.dev, *bc.ws, o, nullptr, rho ? rb.data() : nullptr, &ws_stats, st, &per);
         if (rc) return rc;
+        for (uint32_t p = 0; p < live; ++p) {
+            a43g_solve_stats_t &s = stats[w0 + p];
+            s = ws_stats;
+            int it = 0, upd = 0, fb = 0; double r = 0;
+            for (uint32_t k = 0; k < nsrc; ++k) {
+                it = std::max(it, per.iterations[p*nsrc + k]);
+                upd = std::max(upd, per.updates[p*nsrc + k]);
+                fb += per.fallback[p*nsrc + k];
+                r = std::max(r, per.residual[p*nsrc + k]);
+            }
+            s.iterations = it; s.refinements = upd; s.residual_max = r; s.fp64_sources = fb;
+            s.converged = (r <= opt.tolerance) ? 1 : 0;
+            if (rho) std::memcpy(rho + (size_t(w0) + p)*nsrc*128, rb.data() + size_t(p)*nsrc*128, size_t(nsrc)*128*8);
+        }
     }
     return A43G_OK;
 }

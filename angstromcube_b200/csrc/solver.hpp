@@ -4,32 +4,51 @@
 #include "device.cuh"
 #include "../../include/a43g.h"
 
+#include <memory>
+
 namespace a43g {
 
 // device vectors of one precision for the tfQMR recurrences
 struct TfqmrVectors {
     size_t elem = 0;             // bytes per real
     size_t n = 0;                // reals per vector (nnzb * 8192)
-    DeviceBuffer X, W, U1, U2, V, D, AU1, AU2, Rt;
+    DeviceBuffer X, W, U1, U2, V, D, AU1, AU2;
     bool alloc(size_t nreals, size_t elem_bytes);
     void release();
 };
 
 struct SolverWorkspace {
     TfqmrVectors v64, v32;
-    DeviceBuffer X64, R64, AX64;     // refinement vectors (FP64)
-    DeviceBuffer colstate;           // per-column scalars (double), see solver.cu
-    DeviceBuffer counters;           // int32 [4]
-    DeviceBuffer colnorm;            // double [nCols*64]
-    int32_t *host_counters = nullptr; // pinned
+    DeviceBuffer X64, AX64;          // FP64 solution of the FP32 recurrences, FP64 operator scratch
+    DeviceBuffer state;              // per-column and per-source scalars, control block (solver.cu)
+    DeviceBuffer part, tickets;      // fixed-order column reductions
+    void *host_ctl = nullptr;        // pinned copy of the control block
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     ~SolverWorkspace();
 };
 
-int solve(GreenPlan &hp, DevicePlan &dp, SolverWorkspace &ws, a43g_solve_options_t const &opt,
-          void *X, double *rho, a43g_solve_stats_t *stats, cudaStream_t st);
+// per-source results of a solve (batches report them per pair)
+struct SourceStats {
+    uint32_t live_sources = 0;       // sources beyond this are padding of a batch, retired at the start
+    std::vector<int> iterations, updates, fallback;
+    std::vector<double> residual;
+};
 
-int solve_batched(GreenPlan &hp, DevicePlan &dp, SolverWorkspace &ws, a43g_solve_options_t const &opt,
+// the batch plan and workspace of solve_batched, kept between calls
+struct BatchCache {
+    GreenPlan host;
+    std::unique_ptr<DevicePlan> dev;
+    std::unique_ptr<SolverWorkspace> ws;
+    uint32_t npairs = 0;
+};
+
+// device bytes of the solver vectors of one solve of this plan in the given precision
+size_t solve_bytes(DevicePlan const &dp, int precision);
+
+int solve(GreenPlan &hp, DevicePlan &dp, SolverWorkspace &ws, a43g_solve_options_t const &opt,
+          void *X, double *rho, a43g_solve_stats_t *stats, cudaStream_t st, SourceStats *per_source = nullptr);
+
+int solve_batched(GreenPlan &hp, DevicePlan &dp, BatchCache &bc, a43g_solve_options_t const &opt,
                   int32_t n, double const *energies, double const *kpoints, double dVol,
                   double *rho, a43g_solve_stats_t *stats, cudaStream_t st);
 

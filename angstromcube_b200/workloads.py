@@ -165,3 +165,47 @@ def make(name, seed=0):
 def random_blocks(nnzb, rng, dtype=np.float64):
     """Random block vector [nnzb, 2, 64, 64]."""
     return rng.standard_normal((nnzb, 2, 64, 64)).astype(dtype)
+
+
+def contour_semicircle(n=32, e_bottom=-1.0, e_top=0.0):
+    """Energy points and complex weights of a semicircular contour from e_bottom to e_top in the
+    upper half plane, Gauss-Legendre in the angle: E(theta) = c + R exp(i theta), theta from pi
+    to 0 (c the midpoint, R the radius).  With 32 points the imaginary parts run from about
+    1.1e-3 to 0.5 Ha for the interval [-1, 0]."""
+    x, wx = np.polynomial.legendre.leggauss(n)
+    c, R = 0.5 * (e_bottom + e_top), 0.5 * (e_top - e_bottom)
+    theta = 0.5 * np.pi * (1.0 - x)                     # x = -1 -> pi (bottom), x = 1 -> 0 (top)
+    E = c + R * np.exp(1j * theta)
+    # dE = i R exp(i theta) dtheta, dtheta = -pi/2 dx
+    w = 1j * R * np.exp(1j * theta) * (-0.5 * np.pi) * wx
+    return E, w
+
+
+def truncation_radius(E, scale=8.0, lo=8.0, hi=16.0):
+    """r_trunc = clamp(8 / sqrt(Im E / 0.5), 8, 16) Bohr: longer-ranged Green functions close to
+    the real axis."""
+    return float(np.clip(scale / np.sqrt(np.imag(E) / 0.5), lo, hi))
+
+
+def contour_kpoints(n=4, seed=7):
+    """Gamma and n-1 seeded points in the irreducible wedge of the cubic Brillouin zone
+    (0 <= k_z <= k_y <= k_x < 0.5, units of 2 pi / cell), equal weights."""
+    rng = np.random.default_rng(seed)
+    ks = [np.zeros(3)]
+    while len(ks) < n:
+        k = np.sort(rng.uniform(0.0, 0.5, size=3))[::-1]
+        ks.append(k)
+    return np.array(ks), np.full(n, 1.0 / n)
+
+
+def batched_contour(name="periodic16_64atoms_s2x2x2", nE=32, nk=4):
+    """The batched contour workload: the 16^3-cube cell with 64 atoms and 8 source cubes, nE
+    energy points on the semicircle from -1 to 0 Ha, nk k-points.  Returns the workload, the
+    (E, k) pairs in the reference's loop order (energies outer), their weights and truncation
+    radii."""
+    w = make(name)
+    E, wE = contour_semicircle(nE)
+    K, wK = contour_kpoints(nk)
+    pairs = [(complex(e), k.copy(), complex(we) * wk, truncation_radius(e))
+             for e, we in zip(E, wE) for k, wk in zip(K, wK)]
+    return w, pairs

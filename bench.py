@@ -1,21 +1,29 @@
 """Benchmark of the Green-function solver: solves/s at 1e-8 relative residual.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--wave P]
+    python bench.py --full-contour [--nk K]     (every pair of the contour; a long run)
 
-A step is one solve of the periodic 16^3-cube cell with 64 atoms (numax 5), 16 source cubes
-(1024 right-hand-side columns), truncation radius 12 Bohr, to 1e-8 relative residual per
-column, with the mixed-precision solver: FP32 tfQMR sweeps (FP32 finite-difference stencil,
-potential and projectors) inside FP64 residual refinement.  The energy is E = -0.2 + 0.5i Ha,
-the largest imaginary part of the energy contour over this cell: at E = -0.2 + 0.02i tfQMR
-stagnates (4000 FP32 iterations leave a relative residual of 0.33, 700 FP64 iterations 0.07),
-so no solver reaches 1e-8 there in a bounded time.  Each rank solves its own energy point
-(weak scaling); the complex densities of all ranks are summed with one NCCL all-reduce per
-step, as the energy-contour integration does.
+Workload (the batched contour): the periodic 16^3-cube cell (h = 0.25 Bohr) with 64 atoms
+(numax 5, sigma 0.6) on a jittered 4^3 lattice and 64 Gaussian wells, 8 source cubes (512
+right-hand-side columns), 32 energies on a semicircular Gauss-Legendre contour from -1 to 0 Ha
+(imaginary parts 2.1e-3 to 0.5 Ha), each with its truncation radius clamp(8/sqrt(Im E/0.5), 8,
+16) Bohr, times 4 k-points (Gamma and 3 seeded points of the irreducible wedge): 128 (E, k)
+solves.  Every radius above 8 Bohr leaves the 16 Bohr cell untruncated, so all 128 share one
+plan of 32,768 blocks (checked at set-up).  A solve is one (E, k) pair with all 512 columns at a
+true FP64 relative residual below 1e-8.
 
-Reported beside the solver throughput: the fused local-action kernel against the measured HBM
-peak, the tensor-core projector, the plain FP64 solver on the same point, and the reference's
-CPU action (oracle/_ref) timed on the host cores on a bounded sample and extrapolated to a
-solve.  --impl reference prints the reference CPU arm only.
+A step solves one wave of --wave pairs (default 2) with a43g_solve_batched: FP32 recurrences and
+operator, FP64 solution and residual replacement, finished source cubes retired, sources whose
+FP32 recurrences stall continued in FP64.  The steps walk through the 128 pairs in a fixed order
+that spreads them over the contour (pair 37*i mod 128 for the i-th solve), so a run of K steps
+times a sample of 2K pairs of the whole contour; `value` counts the converged solves per second
+of device time.  Reported beside it on the same pairs: the plain FP64 solver (the reference's
+algorithm: FP64 tfQMR, no retirement, one pair at a time) on the first pairs of the sample, per
+pair status and iterations, the fused local kernel and the projector against their rooflines,
+and the reference's CPU action (oracle/_ref) timed on the host cores on a bounded sample and
+extrapolated to a solve.  Each rank of a multi-GPU run solves its own pairs (weak scaling) and
+the weighted densities of all ranks are summed with one NCCL all-reduce per step, as the
+contour integration does.  --impl reference prints the reference CPU arm only.
 """
 import argparse
 import json
@@ -28,14 +36,17 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-WORKLOAD = "periodic16_64atoms"
-ENERGY = complex(-0.2, 0.5)
+WORKLOAD = "periodic16_64atoms_s2x2x2"
 TOLERANCE = 1e-8
-# tfQMR iterations of the plain FP64 solver at this workload, energy and tolerance (measured
-# with this code on a B200); the reference arm, which runs without a GPU, extrapolates its
-# action time to a solve with it.  The main arm uses the count of its own FP64 solve.
-FP64_ITERATIONS = 240
+MAX_ITERATIONS = 1500
+STRIDE = 37            # walk of the 128 pairs: 37*i mod 128 (37 is coprime with 128)
 METRIC = "Solves/s at 1e-8 resid (mixed+batched vs plain FP64); action % HBM peak"
+# plain FP64 tfQMR iterations to 1e-8 of the 32 contour energies at Gamma, one source cube of this
+# cell, measured with this repository's FP64 solver on a B200 (1500 = no convergence within 1500
+# iterations); the reference arm, which runs without a GPU, extrapolates its action time to solves
+# with them
+FP64_ITERATIONS_GAMMA = [430, 387, 379, 361, 343, 300, 284, 242, 221, 209, 199, 195, 191, 184, 194, 198,
+                         205, 211, 217, 242, 267, 292, 353, 408, 505, 646, 876, 1247, 1500, 1500, 1500, 1500]
 
 
 def _json_default(o):
@@ -53,13 +64,15 @@ def emit(obj):
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=2)
+    ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default=WORKLOAD)
-    ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 comparison solve")
+    ap.add_argument("--wave", type=int, default=2, help="(E, k) pairs per step")
+    ap.add_argument("--fp64-pairs", type=int, default=4, help="pairs of the sample also solved in plain FP64")
+    ap.add_argument("--full-contour", action="store_true", help="solve all pairs (mixed+batched and plain FP64)")
+    ap.add_argument("--nk", type=int, default=4, help="k-points of the contour")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
-    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
     return ap.parse_args()
 
 
@@ -119,12 +132,20 @@ class ClockSampler:
                 "samples": len(self.rows)}
 
 
+def pair_order(npairs):
+    """The fixed walk through the pairs: 37 i mod npairs (a permutation when npairs is a power of
+    two), spreading consecutive solves over the contour."""
+    from math import gcd
+    stride = STRIDE if gcd(STRIDE, npairs) == 1 else 1
+    return [(stride * i) % npairs for i in range(npairs)]
+
+
 # ------------------------------------------------------------------ reference CPU leg
 
 def _ref_worker(args):
     """One process: the reference's action_t<double,2,1>::multiply (its CPU build in
-    oracle/_ref) on the benchmark cell with ONE source cube; returns seconds per action."""
-    workload, seed, reps = args
+    oracle/_ref) on the contour cell with ONE source cube; returns seconds per action."""
+    workload, seed, reps, E = args
     # the reference's plan builder prints warnings on stdout: keep the JSON line alone there
     devnull = os.open(os.devnull, os.O_WRONLY)
     os.dup2(devnull, 1)
@@ -140,7 +161,7 @@ def _ref_worker(args):
     r = oracle.RefGreen(g)
     r.set_potential(w.Vcell)
     r.set_atom_matrices(w.mats, w.offsets)
-    r.set_energy(ENERGY, w.dVol)
+    r.set_energy(E, w.dVol)
     x = np.random.default_rng(seed).standard_normal((r.sizes["nnzb"], 2, 64, 64))
     best = None
     for _ in range(reps):
@@ -151,18 +172,38 @@ def _ref_worker(args):
     return best
 
 
-def cpu_reference_sample(workload, nsources, procs=None, reps=1, iterations=FP64_ITERATIONS):
-    """Reference CPU action on a bounded sample: one single-source action per process, all host
-    cores in parallel.  Returns (solves/s extrapolated, cores, seconds per single-source action)."""
+def cpu_action_seconds(workload, E, procs=None, reps=1):
+    """Reference CPU action of one source cube, one process per host core in parallel; returns
+    (seconds per single-source action (slowest process), processes)."""
     import multiprocessing as mp
     procs = procs or min(os.cpu_count() or 1, 32)
     ctx = mp.get_context("spawn")
     with ctx.Pool(procs) as pool:
-        times = pool.map(_ref_worker, [(workload, i, reps) for i in range(procs)])
-    t1 = max(times)
-    # a solve applies the full operator (all sources) twice per iteration
-    solves_per_s = procs / (t1 * nsources * 2 * iterations)
-    return solves_per_s, procs, t1
+        times = pool.map(_ref_worker, [(workload, i, reps, E) for i in range(procs)])
+    return max(times), procs
+
+
+def _ref_configs0_solve(_):
+    """The CPU-runnable configuration solved for real: the reference's CPU action inside the
+    numpy restatement of tfQMR (oracle/tfqmr.py), FP64 to 1e-9.  Returns (iterations, seconds)."""
+    devnull = os.open(os.devnull, os.O_WRONLY)
+    os.dup2(devnull, 1)
+    import tempfile
+    os.chdir(tempfile.mkdtemp())
+    sys.path.insert(0, ROOT)
+    import oracle
+    from oracle import tfqmr
+    from angstromcube_b200 import workloads
+    w = workloads.make("periodic4_1atom")
+    r = oracle.RefGreen(w.geometry)
+    r.set_potential(w.Vcell)
+    r.set_atom_matrices(w.mats, w.offsets)
+    r.set_energy(w.E, w.dVol)
+    e = r.export()
+    t = time.perf_counter()
+    X, info = tfqmr.solve_blocks(r.action, e["subset"], e["colindx"], r.sizes["nnzb"], r.sizes["nCols"],
+                                 tol=w.tolerance, maxiter=w.max_iterations)
+    return info["iterations"], time.perf_counter() - t, bool(info["converged"])
 
 
 def reference_arm(a):
@@ -173,27 +214,47 @@ def reference_arm(a):
     if not ref_available():
         emit({"impl": "reference", "unavailable": "reference CPU build oracle/_ref not built"})
         return
-    nsrc = 16
-    for _ in range(a.warmup):
-        pass  # the warm-up of the CPU arm is the first (untimed) sample below
-    cpu_reference_sample(a.workload, nsrc, procs=2)            # warm-up: page in, build plans
+    import multiprocessing as mp
+    import numpy as np
+    from angstromcube_b200 import workloads
+    w, pairs = workloads.batched_contour(WORKLOAD, nk=a.nk)
+    nsrc = 8
+    order = pair_order(len(pairs))
+    nE = len(pairs) // a.nk
+    # a step is one wave of the same pairs as our arm; a pair's solve = 8 sources x 2 actions x its
+    # FP64 iteration count (measured at Gamma on the GPU, the table above) x the action time
+    E_mid = pairs[order[0]][0]
+    cpu_action_seconds(WORKLOAD, E_mid, procs=2)              # warm-up: page in, build plans
     vals, t_all = [], time.perf_counter()
-    for _ in range(a.steps):
-        v, cores, t1 = cpu_reference_sample(a.workload, nsrc)
-        vals.append(v)
+    t1, cores = 0.0, 1
+    for step in range(a.steps):
+        t1, cores = cpu_action_seconds(WORKLOAD, pairs[order[(step * a.wave) % len(pairs)]][0])
+        its = [FP64_ITERATIONS_GAMMA[order[(step * a.wave + i) % len(pairs)] // a.nk * 32 // nE]
+               for i in range(a.wave)]
+        seconds = sum(t1 * nsrc * 2 * n for n in its) / cores
+        vals.append(a.wave / seconds)
     elapsed = time.perf_counter() - t_all
     value = sum(vals) / len(vals)
-    sample = ("reference action_t<double,2,1>::multiply (oracle/_ref CPU build) of the %s cell with one source "
-              "cube per process, %d processes, %.2f s per action; solve = 16 sources x 2 x %d FP64 tfQMR "
-              "iterations (extrapolated)" % (a.workload, cores, t1, FP64_ITERATIONS))
+    # the CPU-runnable configuration solved for real on every core
+    with mp.get_context("spawn").Pool(min(cores, 8)) as pool:
+        sol = pool.map(_ref_configs0_solve, range(min(cores, 8)))
+    it0, s0, ok0 = sol[0]
+    sample = ("reference action_t<double,2,1>::multiply (oracle/_ref CPU build, -O3 x86-64-v3) of the contour "
+              "cell with one source cube per process, %d processes, %.2f s per action; a solve = 8 sources x 2 x "
+              "FP64 tfQMR iterations of its energy (GPU-measured table), extrapolated" % (cores, t1))
     emit({
         "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": a.gpus, "steps": a.steps,
         "warmup": a.warmup, "ms_per_step": 1e3 * elapsed / max(a.steps, 1), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
-        "config": {"workload": a.workload, "tolerance": TOLERANCE, "sources": nsrc, "E": [ENERGY.real, ENERGY.imag]},
+        "config": {"workload": "batched contour: %s, %d energies x %d k-points, tolerance %g" % (
+            WORKLOAD, nE, a.nk, TOLERANCE), "wave": a.wave},
         "impl": "reference",
         "cpu_baseline": {"value": value, "unit": "solves/s", "cores": cores, "kind": "reference", "sample": sample},
         "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "configs0_cpu_solve": {"iterations": it0, "seconds": s0, "converged": ok0, "processes": len(sol),
+                               "solves_per_s": len(sol) / max(s[1] for s in sol),
+                               "what": "periodic 4^3-cube cell, one atom: reference CPU action inside the numpy "
+                                       "tfQMR restatement, FP64 to 1e-9, one solve per process"},
     })
 
 
@@ -241,6 +302,22 @@ def local_kernel_of(tune_lines):
     return "local_fused_pf_kernel<float,16> (potential + 8th-order kinetic, one pass)", "local_fused_pf_kernel_f32"
 
 
+def check_one_plan(w, pairs):
+    """Every truncation radius of the contour gives the same plan (the dense one): the plans of
+    the smallest and the largest radius have identical arrays."""
+    import copy
+    import numpy as np
+    from angstromcube_b200 import green_function as gf
+    rs = [p[3] for p in pairs]
+    exports = []
+    for r in (min(rs), max(rs)):
+        g = copy.copy(w.geometry)
+        g.r_trunc = r
+        exports.append(gf.construct_Green_function(g).export())
+    a, b = exports
+    return all(np.array_equal(a[k], b[k]) for k in a if k not in ("AtomMatrices", "phase"))
+
+
 def our_arm(a):
     import numpy as np
     import torch
@@ -253,43 +330,50 @@ def our_arm(a):
     torch.cuda.set_device(local)
     if world > 1:
         from datetime import timedelta
-        dist.init_process_group("nccl", init_method="env://", timeout=timedelta(seconds=600),
+        dist.init_process_group("nccl", init_method="env://", timeout=timedelta(seconds=900),
                                 device_id=torch.device("cuda", local))
     hbm, bf16, peak_kind = peaks()
-    w = workloads.make(a.workload)
-    # every rank solves its own energy point of the contour (weak scaling)
-    E = complex(ENERGY.real - 0.01*rank, ENERGY.imag)
-    plan = gf.construct_Green_function(w.geometry)
+    w, pairs = workloads.batched_contour(WORKLOAD, nk=a.nk)
+    one_plan = check_one_plan(w, pairs)
+    g = w.geometry
+    g.r_trunc = pairs[0][3]
+    plan = gf.construct_Green_function(g)
     gf.update_potential(plan, w.Vcell, w.mats, w.offsets, layout="cells")
-    gf.update_energy_parameter(plan, E, w.dVol)
+    gf.update_energy_parameter(plan, pairs[0][0], w.dVol)
     plan.upload()
     stream = torch.cuda.Stream()
     # schedule of the FP32 action chosen by timing, outside the timed region
     tune_report = green_action.autotune(plan, "float32", stream)
-    # convergence read back after every iteration: a check costs one host round trip (tens of us)
-    # against about 23 ms per FP32 iteration, and ends each sweep on the iteration it converges
-    # inner tolerance 1e-4 (the library default): sweeps then end near the FP32 floor (about 1e-3
-    # of their right-hand side) by convergence or by the short stall rule; a tighter one leaves
-    # columns above the stall level, where they wait four times as long (measured: 430-450
-    # iterations at 1e-4, 480-630 at 1e-5)
-    opts = dict(tolerance=TOLERANCE, max_iterations=3000, precision="float32", inner_tolerance=1e-4,
-                max_refinements=8, check_every=1)
+    opts = dict(tolerance=TOLERANCE, max_iterations=MAX_ITERATIONS, precision="float32", check_every=1)
+    order = pair_order(len(pairs))
+    nsteps_total = a.warmup + a.steps
+
+    def wave_of(step):
+        # rank r takes the waves r, r + world, ... of the walk (distinct pairs on every rank)
+        base = (step * world + rank) * a.wave
+        return [order[(base + i) % len(pairs)] for i in range(a.wave)]
+
     rho_all = torch.zeros((plan.nCols, 64, 2), dtype=torch.float64, device="cuda")
 
-    def step():
-        stats, rho = green_action.solve(plan, stream=stream, **opts)
+    def step(idx):
+        sel = wave_of(idx)
+        Es = [pairs[i][0] for i in sel]
+        Ks = [pairs[i][1] for i in sel]
+        stats, rho = green_action.solve_batched(plan, Es, Ks, w.dVol, want_rho=True, stream=stream,
+                                                batch=a.wave, **opts)
+        acc = sum(pairs[i][2] * rho[n] for n, i in enumerate(sel))
+        rho_all.copy_(torch.from_numpy(np.stack([acc.real, acc.imag], axis=-1)))
         if world > 1:
-            rho_all.copy_(torch.from_numpy(np.stack([rho.real, rho.imag], axis=-1)))
             dist.all_reduce(rho_all)
-        return stats
+        return sel, stats
 
-    for _ in range(a.warmup):
-        st = step()
+    for i in range(a.warmup):
+        step(i)
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
     launches0 = _lib.lib().a43g_kernel_launches()
-    stats = []
+    records = []
     with ClockSampler(local) as clocks:
         if world > 1:
             dist.barrier()
@@ -297,125 +381,228 @@ def our_arm(a):
         t0 = time.perf_counter()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        for _ in range(a.steps):
-            stats.append(step())
+        for i in range(a.warmup, nsteps_total):
+            records.append(step(i))
         e1.record(stream)
         torch.cuda.synchronize()
         if world > 1:
             dist.barrier()
         wall = time.perf_counter() - t0
     launches = _lib.lib().a43g_kernel_launches() - launches0
-    # device-side time of the steps: the solver records its own events per solve
-    dev = sum(s["seconds"] for s in stats)
+    dev = e0.elapsed_time(e1) * 1e-3
     t = torch.tensor([max(dev, 1e-9)], dtype=torch.float64, device="cuda")
+    conv = torch.tensor([sum(s["converged"] for _, st in records for s in st)], dtype=torch.float64, device="cuda")
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.all_reduce(conv)
     tmax = float(t.item())
-    value = world*a.steps/tmax
-    converged = all(s["converged"] for s in stats)
-    iters = [s["iterations"] for s in stats]
-    refs = [s["refinements"] for s in stats]
-    res = max(s["residual_max"] for s in stats)
+    value = float(conv.item()) / tmax
+    per_pair = []
+    for sel, st in records:
+        for i, s in zip(sel, st):
+            E, k = pairs[i][0], pairs[i][1]
+            per_pair.append({"pair": i, "E": [E.real, E.imag], "k": list(np.round(k, 4)),
+                             "converged": bool(s["converged"]), "iterations": s["iterations"],
+                             "fp64_sources": s["fp64_sources"], "replacements": s["refinements"],
+                             "residual": s["residual_max"]})
 
-    # end to end through the public API: host potential, matrices and energy in, density out
+    # end to end through the public API: host potential and matrices in (pinned), host energies and
+    # k-points in, the pairs' densities out; one wave per step, timed on the host around synchronized work
     Vpin = torch.from_numpy(w.Vcell).pin_memory().numpy()
     Mpin = torch.from_numpy(w.mats).pin_memory().numpy()
-    ke2e = 0 if a.no_e2e else max(1, a.steps//2)
+    ke2e = 0 if a.no_e2e else max(1, a.steps // 2)
     torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for _ in range(ke2e):
+    te = time.perf_counter()
+    conv_e2e = 0
+    for i in range(ke2e):
         gf.update_potential(plan, Vpin, Mpin, w.offsets, layout="cells")
-        gf.update_energy_parameter(plan, E, w.dVol)
-        s_e2e, rho = green_action.solve(plan, stream=stream, **opts)
+        sel = wave_of(a.warmup + i)
+        st_e, rho_e = green_action.solve_batched(plan, [pairs[j][0] for j in sel], [pairs[j][1] for j in sel],
+                                                 w.dVol, want_rho=True, stream=stream, batch=a.wave, **opts)
+        conv_e2e += sum(s["converged"] for s in st_e)
     torch.cuda.synchronize()
-    e2e_s = (time.perf_counter() - t0)/max(ke2e, 1)
-    h2d = w.Vcell.nbytes + w.mats.nbytes
-    d2h = plan.nCols*64*16
+    e2e_s = time.perf_counter() - te
+    h2d = w.Vcell.nbytes + w.mats.nbytes + a.wave * 5 * 8
+    d2h = a.wave * plan.nCols * 64 * 16
 
     out = None
     if rank == 0:
         out = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": a.steps,
-               "warmup": a.warmup, "ms_per_step": 1e3*tmax/a.steps, "higher_is_better": True, "scaling": "weak",
-               "vs_baseline": None, "dtype": "f32+3xtf32 (fp64 refinement)", "data": "synthetic (seeded)",
-               "config": {"workload": a.workload, "cell_cubes": list(np.array(w.geometry.ng)//4),
-                          "sources": plan.nCols, "rhs_columns": plan.nCols*64, "atoms": w.natoms, "numax": 5,
-                          "nnzb": plan.nnzb, "tolerance": TOLERANCE, "E": [E.real, E.imag],
-                          "parallelism": "dp%d (energy points)" % world,
-                          "l2": "inputs larger than L2 (%.1f GB per FP32 vector)" % (plan.nnzb*32768/1e9)},
-               "solve": {"iterations": iters, "refinements": refs, "residual_max": res, "converged": converged,
-                         "wall_s_per_step": wall/a.steps},
-               "e2e": None if 0 == ke2e else {"value": 1.0/e2e_s*world, "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
-                       "d2h_bytes_per_step": int(d2h)},
+               "warmup": a.warmup, "ms_per_step": 1e3 * tmax / a.steps, "higher_is_better": True, "scaling": "weak",
+               "vs_baseline": None, "dtype": "f32 recurrences and operator, f64 solution and residual replacement",
+               "data": "synthetic (seeded)",
+               "config": {"workload": "batched contour (configs 3): %s, 32 Gauss-Legendre energies on the semicircle "
+                                      "-1..0 Ha x %d k-points, 8 source cubes, tolerance %g" % (WORKLOAD, a.nk, TOLERANCE),
+                          "cell_cubes": [16, 16, 16], "sources": plan.nCols, "rhs_columns": plan.nCols * 64,
+                          "atoms": w.natoms, "numax": 5, "nnzb_per_pair": plan.nnzb, "one_plan_for_all_radii": one_plan,
+                          "wave": a.wave, "pairs_timed": len(per_pair), "max_iterations": MAX_ITERATIONS,
+                          "parallelism": "dp%d ((E, k) pairs per rank)" % world,
+                          "l2": "inputs larger than L2 (%.2f GB per FP32 vector and pair)" % (plan.nnzb * 32768 / 1e9)},
+               "solve": {"converged": int(conv.item()), "pairs": len(per_pair) * world, "wall_s_per_step": wall / a.steps,
+                         "per_pair": per_pair},
+               "e2e": None if 0 == ke2e else {"value": conv_e2e * world / e2e_s, "unit": "solves/s",
+                                               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
                "gpu_launches": int(launches), "clocks": clocks.summary(),
                "autotune": [l for l in tune_report.splitlines() if l.startswith("chosen")]}
-    return plan, w, E, stream, opts, out, hbm, bf16, peak_kind, world, rank
+    return plan, w, pairs, stream, opts, out, hbm, bf16, peak_kind, world, rank, records
 
 
-def measure_kernels(a, plan, w, stream, out, hbm, bf16, peak_kind):
-    """Rooflines of the fused local kernel (HBM) and of the tensor-core projector (TF32)."""
+def measure_kernels(plan, stream, out, hbm, bf16, peak_kind):
+    """Rooflines of the fused local kernel (HBM) and of the projector (TF32 tensor peak)."""
     import torch
     from angstromcube_b200 import _lib
     nnzb = plan.nnzb
     x = torch.randn((nnzb, 2, 64, 64), device="cuda", dtype=torch.float32)
     y = torch.empty_like(x)
     t_local = time_part(_lib, plan, 0, _lib.A43G_F32, x, y, 20, stream)
-    bytes_local = 2*nnzb*8192*4 + plan.sizes["ncells"]*64*4 + nnzb*(7*4) + plan.sizes["lists_nnz2"]*4
-    ach = bytes_local/t_local/1e9
+    bytes_local = 2 * nnzb * 8192 * 4 + plan.sizes["ncells"] * 64 * 4 + nnzb * (7 * 4) + plan.sizes["lists_nnz2"] * 4
+    ach = bytes_local / t_local / 1e9
     kname, tkey = local_kernel_of(out.get("autotune", []))
     traffic = read_traffic(tkey) if tkey else None
     out["roofline"] = {"kernel": kname,
-                       "bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach/hbm,
+                       "bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
                        "peak_kind": peak_kind, "algorithmic_bytes_per_launch": bytes_local,
-                       "ms_per_launch": t_local*1e3,
-                       "traffic": traffic*nnzb if traffic is not None else None}
+                       "ms_per_launch": t_local * 1e3,
+                       "traffic": traffic * nnzb if traffic is not None else None}
     t_dyadic = time_part(_lib, plan, 1, _lib.A43G_F32, x, y, 10, stream)
     nsho = 56
-    flops = 4.0*nsho*64*128*plan.sizes["SHOadd_nnz"]
-    tf32_peak = bf16/2
+    flops = 4.0 * nsho * 64 * 128 * plan.sizes["SHOadd_nnz"]
+    tf32_peak = bf16 / 2
     tc = os.environ.get("A43G_PROJECTOR", "") == "tc"
     out["roofline_projector"] = {"kernel": ("sho_project_tc + sho_add_tc (tcgen05 kind::tf32, 3xTF32)" if tc else
-                                            "sho_project_kernel + sho_add_kernel (SIMT FP32, sum-factorized)")
+                                            "sho_project_simt + sho_add_simt (FP32 CUDA cores, sum-factorized)")
                                  + " + atom matrices",
-                                 "bound": "tensor", "achieved": flops/t_dyadic/1e12, "peak": tf32_peak,
-                                 "unit": "TFLOP/s", "frac": flops/t_dyadic/1e12/tf32_peak,
+                                 "bound": "tensor", "achieved": flops / t_dyadic / 1e12, "peak": tf32_peak,
+                                 "unit": "TFLOP/s", "frac": flops / t_dyadic / 1e12 / tf32_peak,
                                  "peak_kind": "dense TF32 = half of the %s bf16 peak" % peak_kind,
-                                 "algorithmic_flops_per_launch": flops, "ms_per_launch": t_dyadic*1e3,
+                                 "algorithmic_flops_per_launch": flops, "ms_per_launch": t_dyadic * 1e3,
                                  "note": "flops of the dense contraction P (64 x 64 per block and image) x X (64 x 128)"}
     x64 = torch.randn((nnzb, 2, 64, 64), device="cuda", dtype=torch.float64)
     y64 = torch.empty_like(x64)
     del x, y
-    out["action_ms"] = {"fp32_local": t_local*1e3, "fp32_projector": t_dyadic*1e3,
-                        "fp64_local": time_part(_lib, plan, 0, _lib.A43G_F64, x64, y64, 10, stream)*1e3,
-                        "fp64_projector": time_part(_lib, plan, 1, _lib.A43G_F64, x64, y64, 3, stream)*1e3}
+    out["action_ms"] = {"fp32_local": t_local * 1e3, "fp32_projector": t_dyadic * 1e3,
+                        "fp64_local": time_part(_lib, plan, 0, _lib.A43G_F64, x64, y64, 10, stream) * 1e3,
+                        "fp64_projector": time_part(_lib, plan, 1, _lib.A43G_F64, x64, y64, 3, stream) * 1e3}
     del x64, y64
     torch.cuda.empty_cache()
 
 
+def fp64_plain(plan, w, pairs, sel, stream, opts):
+    """The plain FP64 solver on the given pairs one after the other: FP64 tfQMR without
+    retirement (the reference's algorithm).  Returns per-pair (converged, iterations, seconds)."""
+    from angstromcube_b200 import green_action, green_function as gf
+    o64 = dict(opts)
+    o64["precision"] = "float64"
+    res = []
+    for i in sel:
+        E, k = pairs[i][0], pairs[i][1]
+        gf.update_energy_parameter(plan, E, w.dVol)
+        gf.update_phases(plan, k)
+        s, _ = green_action.solve(plan, stream=stream, want_rho=False, retire=False, **o64)
+        res.append((bool(s["converged"]), s["iterations"], s["seconds"]))
+    return res
+
+
+def mixed_single(plan, w, pairs, sel, stream, opts):
+    """The same pairs with the mixed solver, one pair per wave (a43g_solve_batched with batch 1)."""
+    from angstromcube_b200 import green_action
+    res = []
+    for i in sel:
+        st, _ = green_action.solve_batched(plan, [pairs[i][0]], [pairs[i][1]], w.dVol, stream=stream,
+                                           batch=1, **opts)
+        res.append((bool(st[0]["converged"]), st[0]["iterations"], st[0]["seconds"]))
+    return res
+
+
+def full_contour(a):
+    """Every pair of the contour with the mixed batched solver (waves as large as memory allows)
+    and with the plain FP64 solver; prints one JSON line per solver and a summary."""
+    import numpy as np
+    import torch
+    from angstromcube_b200 import green_action, green_function as gf, workloads
+    torch.cuda.set_device(0)
+    w, pairs = workloads.batched_contour(WORKLOAD, nk=a.nk)
+    g = w.geometry
+    g.r_trunc = pairs[0][3]
+    plan = gf.construct_Green_function(g)
+    gf.update_potential(plan, w.Vcell, w.mats, w.offsets, layout="cells")
+    gf.update_energy_parameter(plan, pairs[0][0], w.dVol)
+    plan.upload()
+    stream = torch.cuda.Stream()
+    green_action.autotune(plan, "float32", stream)
+    opts = dict(tolerance=TOLERANCE, max_iterations=MAX_ITERATIONS, precision="float32", check_every=1)
+    Es = [p[0] for p in pairs]
+    Ks = [p[1] for p in pairs]
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    st, rho = green_action.solve_batched(plan, Es, Ks, w.dVol, want_rho=True, stream=stream, batch=a.wave, **opts)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t_mixed = e0.elapsed_time(e1) * 1e-3
+    emit({"solver": "mixed+batched", "pairs": len(pairs), "wave": a.wave, "seconds": t_mixed,
+          "converged": sum(s["converged"] for s in st),
+          "per_pair": [[i, pairs[i][0].real, pairs[i][0].imag, s["converged"], s["iterations"], s["fp64_sources"],
+                        s["residual_max"]] for i, s in enumerate(st)]})
+    res64 = fp64_plain(plan, w, pairs, range(len(pairs)), stream, opts)
+    t64 = sum(r[2] for r in res64)
+    emit({"solver": "plain fp64", "pairs": len(pairs), "seconds": t64, "converged": sum(r[0] for r in res64),
+          "per_pair": [[i, pairs[i][0].real, pairs[i][0].imag, r[0], r[1]] for i, r in enumerate(res64)]})
+    cm, c64 = sum(s["converged"] for s in st), sum(r[0] for r in res64)
+    emit({"summary": {"mixed_batched_solves_per_s": cm / t_mixed, "fp64_plain_solves_per_s": c64 / t64,
+                      "speedup": (cm / t_mixed) / (c64 / t64) if c64 else None,
+                      "seconds": [t_mixed, t64], "converged": [cm, c64], "pairs": len(pairs)}})
+
+
+def launch_ranks(a):
+    """--gpus N without a launcher: start N ranks with torch.distributed.run (one process per GPU,
+    NCCL over 127.0.0.1) and return its exit code."""
+    import socket
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", str(a.gpus),
+           "--master-addr", "127.0.0.1", "--master-port", str(port), os.path.abspath(__file__)] + sys.argv[1:]
+    return subprocess.call(cmd)
+
+
 def main():
     a = parse()
+    if a.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        sys.exit(launch_ranks(a))
     if a.impl == "reference":
         reference_arm(a)
         return
-    plan, w, E, stream, opts, out, hbm, bf16, peak_kind, world, rank = our_arm(a)
+    if a.full_contour:
+        full_contour(a)
+        return
+    plan, w, pairs, stream, opts, out, hbm, bf16, peak_kind, world, rank, records = our_arm(a)
     if rank == 0:
-        measure_kernels(a, plan, w, stream, out, hbm, bf16, peak_kind)
-        if not a.no_fp64:
-            from angstromcube_b200 import green_action
-            o64 = dict(opts); o64["precision"] = "float64"
-            s64, _ = green_action.solve(plan, stream=stream, want_rho=False, **o64)
-            out["fp64_plain"] = {"solves_per_s": 1.0/s64["seconds"], "iterations": s64["iterations"],
-                                 "residual_max": s64["residual_max"], "converged": s64["converged"],
-                                 "speedup_mixed_vs_fp64": out["value"]/world*s64["seconds"]}
+        measure_kernels(plan, stream, out, hbm, bf16, peak_kind)
+        # plain FP64 on the first pairs of the timed sample, and the mixed solver on the same
+        # pairs one at a time: the metric's comparison on matched solves
+        sel = [i for s, _ in records for i in s][:max(1, a.fp64_pairs)]
+        r64 = fp64_plain(plan, w, pairs, sel, stream, opts)
+        rmx = mixed_single(plan, w, pairs, sel, stream, opts)
+        t64, tmx = sum(r[2] for r in r64), sum(r[2] for r in rmx)
+        c64, cmx = sum(r[0] for r in r64), sum(r[0] for r in rmx)
+        out["fp64_plain"] = {"pairs": sel, "solves_per_s": c64 / t64, "seconds": t64, "converged": c64,
+                             "iterations": [r[1] for r in r64],
+                             "mixed_same_pairs": {"solves_per_s": cmx / tmx, "seconds": tmx, "converged": cmx,
+                                                  "iterations": [r[1] for r in rmx]},
+                             "speedup_mixed_vs_fp64": (cmx / tmx) / (c64 / t64) if c64 and cmx else None,
+                             "what": "the same (E, k) pairs: plain FP64 tfQMR without retirement, one pair at a "
+                                     "time, against the mixed solver one pair per wave"}
         if world == 1 and not a.no_cpu:
             from oracle import ref_available
             if ref_available():
-                nit = out.get("fp64_plain", {}).get("iterations", FP64_ITERATIONS)
-                v, cores, t1 = cpu_reference_sample(a.workload, plan.nCols, iterations=nit)
-                out["cpu_baseline"] = {"value": v, "unit": "solves/s", "cores": cores, "kind": "reference",
+                t1, cores = cpu_action_seconds(WORKLOAD, pairs[sel[0]][0])
+                its = [r[1] for r in r64]
+                sec = sum(t1 * 8 * 2 * n for n in its) / cores
+                out["cpu_baseline"] = {"value": len(its) / sec, "unit": "solves/s", "cores": cores, "kind": "reference",
                                        "sample": "reference CPU action (oracle/_ref) of the cell with one source cube "
-                                                 "per process, %d processes, %.2f s per action; solve = %d sources x 2 x "
-                                                 "%d FP64 tfQMR iterations (extrapolated)"
-                                                 % (cores, t1, plan.nCols, nit)}
+                                                 "per process, %d processes, %.2f s per action; a solve = 8 sources x 2 x "
+                                                 "the FP64 iteration count this run measured for the pair (%s), "
+                                                 "extrapolated" % (cores, t1, its)}
         emit(out)
     if world > 1:
         import torch.distributed as dist

@@ -74,26 +74,37 @@ typedef struct {
 } a43g_plan_export_t;
 
 /* Solver options and per-solve statistics (tfQMR, Freund 1993, per-column scalars) */
+enum {
+    A43G_SOLVE_NO_RETIRE = 1  /* keep computing on finished source cubes (the reference's tfQMRgpu does) */
+};
+
 typedef struct {
     double   tolerance;       /* relative residual |B - A X| / |B| per column */
     int32_t  max_iterations;  /* tfQMR iterations (two operator applications each) */
-    int32_t  precision;       /* A43G_F64: plain FP64 tfQMR; A43G_F32: FP32 sweeps inside FP64 refinement */
-    double   inner_tolerance; /* FP32 inner solve tolerance per refinement step (mixed precision) */
-    int32_t  max_refinements; /* FP64 refinement steps (mixed precision) */
+    int32_t  precision;       /* A43G_F64: plain FP64 tfQMR; A43G_F32: FP32 recurrences and operator, FP64
+                                 solution, convergence checked on the FP64 residual (residual replacement) */
+    double   update_factor;   /* A43G_F32: a source cube replaces its residual when its largest estimate has
+                                 fallen by this factor since its last replacement (0: default 0.1) */
+    int32_t  update_gap;      /* A43G_F32: at most this many iterations between replacements (0: default 50) */
     int32_t  check_every;     /* iterations between convergence checks on the host */
     uint64_t seed;            /* seed of the random shadow residual */
-    int32_t  echo;            /* log level: > 0 prints one line per refinement / convergence check to stdout */
+    int32_t  echo;            /* log level: > 0 prints one line per solve, > 1 one per convergence check */
+    int32_t  flags;           /* A43G_SOLVE_NO_RETIRE */
+    int32_t  batch;           /* a43g_solve_batched: (energy, k-point) pairs per wave, 0: as many as fit */
+    int32_t  pad;
 } a43g_solve_options_t;
 
 typedef struct {
-    int32_t iterations;       /* tfQMR iterations performed (summed over refinements) */
-    int32_t refinements;      /* FP64 residual recomputations performed */
+    int32_t iterations;       /* tfQMR iterations performed (a batched pair: until its last source finished) */
+    int32_t refinements;      /* residual replacements with the FP64 operator (most of any source cube) */
     int32_t converged;        /* 1 if every column reached the tolerance */
     int32_t breakdowns;       /* columns stopped by a rho or sigma breakdown */
     double  residual_max;     /* max over columns of the true relative residual (FP64) */
     double  residual_estimate;/* tfQMR residual bound at exit */
     double  operator_applications; /* action calls made */
-    double  seconds;          /* device time of the solve */
+    double  seconds;          /* device time of the solve (a batched pair: of its wave) */
+    int32_t fp64_sources;     /* A43G_F32: source cubes whose FP32 recurrences stalled and that continued in FP64 */
+    int32_t pad;
 } a43g_solve_stats_t;
 
 const char *a43g_last_error(void);
@@ -186,7 +197,12 @@ int a43g_solve(a43g_plan_t *plan, const a43g_solve_options_t *opts, void *X, dou
                a43g_solve_stats_t *stats, void *stream);
 
 /* ---- batched solve over (energy, k-point) pairs on one plan geometry: energies[n][2],
- * kpoints[n][3]; rho (optional) host [n][nCols][64][2]; stats[n] */
+ * kpoints[n][3]; rho (optional) host [n][nCols][64][2]; stats[n].  No reference counterpart as
+ * one call (the reference loops over its (E, k) points one solve at a time,
+ * src/energy_contour.cxx:355-386): the pairs are solved in waves, each wave one block-sparse
+ * system of all its pairs' source cubes with their own energies and Bloch phases, whose
+ * finished source cubes stop costing work.  The plan keeps the batch's device arrays and
+ * vectors for later calls (released with the plan). */
 int a43g_solve_batched(a43g_plan_t *plan, const a43g_solve_options_t *opts, int32_t n,
                        const double *energies, const double *kpoints, double dVol,
                        double *rho, a43g_solve_stats_t *stats, void *stream);
