@@ -19,6 +19,8 @@ EXPORTED = [
     "a43g_plan_export", "a43g_plan_set_potential", "a43g_plan_set_atom_matrices", "a43g_plan_set_energy",
     "a43g_plan_set_kpoint", "a43g_plan_upload", "a43g_action_multiply", "a43g_action_part", "a43g_vjp", "a43g_plan_autotune", "a43g_action_multiply_noalloc",
     "a43g_kernel_launches", "a43g_plan_device_status", "a43g_solve", "a43g_solve_batched",
+    "a43g_hamiltonian_load", "a43g_hamiltonian_info", "a43g_hamiltonian_get", "a43g_hamiltonian_create",
+    "a43g_hamiltonian_save", "a43g_hamiltonian_destroy", "a43g_projection_coefficients",
 ]
 
 
@@ -102,6 +104,13 @@ def lib():
         L.a43g_solve.argtypes = [vp, ctypes.POINTER(SolveOptions), vp, vp, ctypes.POINTER(SolveStats), vp]
         L.a43g_solve_batched.argtypes = [vp, ctypes.POINTER(SolveOptions), i32, vp, vp, f64, vp,
                                          ctypes.POINTER(SolveStats), vp]
+        L.a43g_hamiltonian_load.argtypes = [ctypes.c_char_p, ctypes.POINTER(vp)]
+        L.a43g_hamiltonian_info.argtypes = [vp, vp, vp, vp, vp, vp]
+        L.a43g_hamiltonian_get.argtypes = [vp, vp, vp, vp, vp]
+        L.a43g_hamiltonian_create.argtypes = [vp, vp, vp, vp, i32, vp, vp, vp, ctypes.POINTER(vp)]
+        L.a43g_hamiltonian_save.argtypes = [vp, ctypes.c_char_p, i32, vp]
+        L.a43g_hamiltonian_destroy.argtypes = [vp]
+        L.a43g_projection_coefficients.argtypes = [vp, vp, vp, vp]
         for name in EXPORTED:
             if name not in ("a43g_last_error", "a43g_version", "a43g_kernel_launches"):
                 getattr(L, name).restype = ctypes.c_int

@@ -596,6 +596,218 @@ local_pencil_kernel(float *__restrict__ y, float const *__restrict__ x,
     }
 }
 
+// Pencils with staged lateral cubes (FP32): the thread mapping and arithmetic of
+// local_pencil_kernel, but the four x- and y-neighbour cubes of step k + 1 are copied into shared
+// memory with 16-byte cp.async while step k is computed, so the stencil reads only shared memory
+// and registers and the neighbour rows' L2 latency is hidden behind a whole step.  The lateral
+// stage holds [2 steps][x-, x+, y-, y+][re, im][64 rows][32 columns]; one CTA per SM.
+constexpr int kStageLat = 4*2*64*kPencilS;                       // floats of one step's laterals
+constexpr int kStageSmem = kPencilSmem + 2*kStageLat*4;          // bytes: z-slots + two lateral steps
+
+__device__ __forceinline__ uint32_t smem_addr_u32(void const *p) { return uint32_t(__cvta_generic_to_shared(p)); }
+__device__ __forceinline__ void cp_async16_cg(void *dst, void const *src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" :: "r"(smem_addr_u32(dst)), "l"(src) : "memory");
+}
+
+__global__ void __launch_bounds__(4*kPencilS, 1)
+local_stage_kernel(float *__restrict__ y, float const *__restrict__ x,
+                   uint32_t const *__restrict__ zstart, int32_t const *__restrict__ zlist,
+                   int32_t const *__restrict__ nbr, int32_t const *__restrict__ veff,
+                   float const *__restrict__ Vcell, LocalArgs<float> a)
+{
+    constexpr int S = kPencilS, NSL = 64/S;
+    extern __shared__ __align__(16) float4 slot4[];   // [3][2][16][S] float4, then the lateral stages
+    float *lat = reinterpret_cast<float*>(slot4 + 3*2*16*S);
+    __shared__ int32_t code[kMaxLine][8];              // per step: block, x-, x+, y-, y+, veff, z-next
+    __shared__ int32_t zleft, nline;
+    int const line = blockIdx.x/NSL, slice = blockIdx.x % NSL;
+    int const tid = threadIdx.x, j = tid % S, zq = tid/S, col = slice*S + j;
+    int32_t const *L = zlist + zstart[line];
+    if (0 == tid) {
+        int n = 0;
+        while (L[4 + n] > 0) ++n;                   // lists end with 4 non-positive entries
+        nline = n; zleft = list_code(L[3]);
+    }
+    __syncthreads();
+    int const n = nline;
+    if (0 == n || !line_args(a, L[4] - 1)) return;  // uniform: nothing on this line, or retired
+    for (int k = tid; k < n; k += 4*S) {
+        int32_t const b = L[4 + k] - 1;
+        int32_t const *nb = nbr + 6*size_t(b);
+        code[k][0] = b; code[k][1] = nb[0]; code[k][2] = nb[1]; code[k][3] = nb[2]; code[k][4] = nb[3];
+        code[k][5] = veff[b]; code[k][6] = list_code(L[5 + k]);
+    }
+    __syncthreads();                                // code[] complete
+    // the four lateral cubes of step k into stage st: 1024 16-byte pieces each, 8 per thread
+    auto issue = [&](int k, int st) {
+#pragma unroll
+        for (int l = 0; l < 4; ++l) {
+            int32_t const e = code[k][1 + l];
+            if (-1 == e) continue;                  // no cube: read as zeros, nothing to copy
+            float const *src = x + size_t(nbr_block(e))*kBlockReals + slice*S;
+            float *dst = lat + (st*4 + l)*2*64*S;
+#pragma unroll
+            for (int q = 0; q < 2*64*(S/4)/(4*S); ++q) {
+                int const c = q*4*S + tid;          // piece: (plane*64 + row)*(S/4) + quad
+                int const pr = c/(S/4), qd = c % (S/4);
+                cp_async16_cg(dst + pr*S + qd*4, src + pr*64 + qd*4);
+            }
+        }
+    };
+    auto srow = [&](int slot, int pl, int row) -> float4 & { return slot4[((slot*2 + pl)*16 + row)*S + j]; };
+    auto put = [&](int slot, Quad const &q) {
+#pragma unroll
+        for (int yy = 0; yy < 4; ++yy)
+#pragma unroll
+            for (int pl = 0; pl < 2; ++pl)
+                srow(slot, pl, zq*4 + yy) = make_float4(q.v[pl][yy*4], q.v[pl][yy*4 + 1], q.v[pl][yy*4 + 2], q.v[pl][yy*4 + 3]);
+    };
+    // row (zq, r4) of lateral l of stage st: 4 x-points, re and im, with the Bloch phase of its code
+    auto lrow = [&](int st, int l, int r4, int32_t e, float pr, float pi, Rows<float> &o) {
+        if (-1 == e) {
+#pragma unroll
+            for (int i = 0; i < 4; ++i) { o.re[i] = 0.f; o.im[i] = 0.f; }
+            return;
+        }
+        float const *b = lat + (st*4 + l)*2*64*S + (zq*16 + r4*4)*S + j;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) { o.re[i] = b[i*S]; o.im[i] = b[64*S + i*S]; }
+        row_phase(e, pr, pi, o);
+    };
+    float const (&cx)[5] = a.st.c[0];
+    float const (&cy)[5] = a.st.c[1];
+    float const (&cz)[5] = a.st.c[2];
+    float const c0 = cx[0] + cy[0] + cz[0];
+    issue(0, 0);
+    asm volatile("cp.async.commit_group;" ::: "memory");
+    {
+        Quad h;
+        quad_raw(x, zleft, zq, col, h);
+        quad_phase(zleft, a.ph[2][0][0], a.ph[2][0][1], h);
+        put(0, h);
+        quad_raw(x, code[0][0], zq, col, h);
+        put(1, h);
+    }
+    Quad nx;                                        // rows of the z-successor, one step ahead
+    quad_raw(x, code[0][6], zq, col, nx);
+    int sp = 0, sc = 1, sn = 2;
+    for (int k = 0; k < n; ++k) {
+        int32_t const b = code[k][0];
+        int const st = k & 1;
+        quad_phase(code[k][6], a.ph[2][1][0], a.ph[2][1][1], nx);   // only the line end has a phase
+        __syncthreads();                            // step k-1 finished reading slot sn and stage st^1
+        if (k + 1 < n) issue(k + 1, st ^ 1);
+        asm volatile("cp.async.commit_group;" ::: "memory");
+        put(sn, nx);
+        asm volatile("cp.async.wait_group 1;" ::: "memory");   // this thread's copies of step k landed
+        __syncthreads();                            // ... and everybody else's; slot sn written
+        if (k + 1 < n) quad_raw(x, code[k + 1][6], zq, col, nx);   // arrives during this step
+        Quad cur;
+#pragma unroll
+        for (int yy = 0; yy < 4; ++yy)
+#pragma unroll
+            for (int pl = 0; pl < 2; ++pl) {
+                float4 const v = srow(sc, pl, zq*4 + yy);
+                cur.v[pl][yy*4] = v.x; cur.v[pl][yy*4 + 1] = v.y; cur.v[pl][yy*4 + 2] = v.z; cur.v[pl][yy*4 + 3] = v.w;
+            }
+        float acc[2][16];
+        int32_t const iloc = code[k][5];
+        float V[16];
+        if (iloc < 0) {
+#pragma unroll
+            for (int i = 0; i < 16; ++i) V[i] = 0.f;
+        } else {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                float4 const v = __ldg(reinterpret_cast<float4 const*>(Vcell + size_t(iloc)*64 + zq*16 + q*4));
+                V[q*4] = v.x; V[q*4 + 1] = v.y; V[q*4 + 2] = v.z; V[q*4 + 3] = v.w;
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+            float const Vt = V[i] - a.E_re;
+            acc[0][i] = Vt*cur.v[0][i] + a.E_im*cur.v[1][i] + c0*cur.v[0][i];
+            acc[1][i] = Vt*cur.v[1][i] - a.E_im*cur.v[0][i] + c0*cur.v[1][i];
+        }
+#pragma unroll
+        for (int pl = 0; pl < 2; ++pl)
+#pragma unroll
+            for (int yy = 0; yy < 4; ++yy)
+#pragma unroll
+                for (int yo = 0; yo < 4; ++yo) {
+                    if (yo == yy) continue;
+                    int const d = (yo > yy) ? yo - yy : yy - yo;
+#pragma unroll
+                    for (int i = 0; i < 4; ++i) acc[pl][yy*4 + i] += cy[d]*cur.v[pl][yo*4 + i];
+                }
+        int32_t const exm = code[k][1], exp_ = code[k][2], eym = code[k][3], eyp = code[k][4];
+#pragma unroll
+        for (int yy = 0; yy < 4; ++yy) {
+            Rows<float> xm, xp;
+            lrow(st, 0, yy, exm, a.ph[0][0][0], a.ph[0][0][1], xm);
+            lrow(st, 1, yy, exp_, a.ph[0][1][0], a.ph[0][1][1], xp);
+            float lr[12], li[12];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                lr[i] = xm.re[i]; li[i] = xm.im[i];
+                lr[4 + i] = cur.v[0][yy*4 + i]; li[4 + i] = cur.v[1][yy*4 + i];
+                lr[8 + i] = xp.re[i]; li[8 + i] = xp.im[i];
+            }
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int d = 1; d <= 4; ++d) {
+                    acc[0][yy*4 + i] += cx[d]*(lr[4 + i - d] + lr[4 + i + d]);
+                    acc[1][yy*4 + i] += cx[d]*(li[4 + i - d] + li[4 + i + d]);
+                }
+        }
+#pragma unroll
+        for (int yo = 0; yo < 4; ++yo) {
+            Rows<float> ym, yp;
+            lrow(st, 2, yo, eym, a.ph[1][0][0], a.ph[1][0][1], ym);
+            lrow(st, 3, yo, eyp, a.ph[1][1][0], a.ph[1][1][1], yp);
+#pragma unroll
+            for (int yy = 0; yy < 4; ++yy) {
+                if (yy <= yo) {
+#pragma unroll
+                    for (int i = 0; i < 4; ++i) {
+                        acc[0][yy*4 + i] += cy[yy - yo + 4]*ym.re[i];
+                        acc[1][yy*4 + i] += cy[yy - yo + 4]*ym.im[i];
+                    }
+                }
+                if (yy >= yo) {
+#pragma unroll
+                    for (int i = 0; i < 4; ++i) {
+                        acc[0][yy*4 + i] += cy[yo + 4 - yy]*yp.re[i];
+                        acc[1][yy*4 + i] += cy[yo + 4 - yy]*yp.im[i];
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int yy = 0; yy < 4; ++yy)
+#pragma unroll
+            for (int d = 1; d <= 4; ++d) {
+                int const zm = zq - d, zp = zq + d;
+                int const s_m = (zm < 0) ? sp : sc, s_p = (zp > 3) ? sn : sc;
+                int const r_m = (zm & 3)*4 + yy, r_p = (zp & 3)*4 + yy;
+#pragma unroll
+                for (int pl = 0; pl < 2; ++pl) {
+                    float4 const m = srow(s_m, pl, r_m), p = srow(s_p, pl, r_p);
+                    acc[pl][yy*4 + 0] += cz[d]*(m.x + p.x);
+                    acc[pl][yy*4 + 1] += cz[d]*(m.y + p.y);
+                    acc[pl][yy*4 + 2] += cz[d]*(m.z + p.z);
+                    acc[pl][yy*4 + 3] += cz[d]*(m.w + p.w);
+                }
+            }
+        float *yb = y + size_t(b)*kBlockReals + (zq*16)*64 + col;
+#pragma unroll
+        for (int i = 0; i < 16; ++i) { yb[i*64] = acc[0][i]; yb[4096 + i*64] = acc[1][i]; }
+        int const t = sp; sp = sc; sc = sn; sn = t;  // rotate the z-slots
+    }
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+}
+
 // ---------------------------------------------------------------- generic local path
 
 // y = (V - E) x for every block (include/green_potential.hxx:15-139, collinear)
@@ -983,6 +1195,7 @@ void launch_project_L(DevicePlan &dp, T const *x, cudaStream_t st) {
 bool prepare_local_kernels() {
     // the pencil kernel's three z-slots are 48 KB of dynamic shared memory beside its static part
     A43G_CUDA_TRY(cudaFuncSetAttribute(local_pencil_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kPencilSmem));
+    A43G_CUDA_TRY(cudaFuncSetAttribute(local_stage_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kStageSmem));
     return true;
 }
 
@@ -1010,7 +1223,16 @@ bool launch_local(DevicePlan &dp, T *y, T const *x, cudaStream_t st) {
         constexpr int S = (sizeof(T) == 8) ? 8 : 16;
         unsigned const nblk = dp.nlists[2]*(64/S);
         if constexpr (sizeof(T) == 4) {
-            if (dp.nlists[2] && dp.max_zline <= kMaxLine && 2 == dp.local_variant) {
+            if (dp.nlists[2] && dp.max_zline <= kMaxLine && 3 == dp.local_variant &&
+                0 == (reinterpret_cast<uintptr_t>(x) & 15u)) {
+                local_stage_kernel<<<dp.nlists[2]*(64/kPencilS), 4*kPencilS, kStageSmem, st>>>(y, x,
+                    dptr<uint32_t>(dp.lists_start[2]), dptr<int32_t>(dp.lists[2]), dptr<int32_t>(dp.nbr),
+                    dptr<int32_t>(dp.veff_index), vcell<T>(dp), a);
+                count_launch();
+                A43G_CUDA_TRY(cudaGetLastError());
+                return true;
+            }
+            if (dp.nlists[2] && dp.max_zline <= kMaxLine && (2 == dp.local_variant || 3 == dp.local_variant)) {
                 local_pencil_kernel<<<dp.nlists[2]*(64/kPencilS), 4*kPencilS, kPencilSmem, st>>>(y, x,
                     dptr<uint32_t>(dp.lists_start[2]), dptr<int32_t>(dp.lists[2]), dptr<int32_t>(dp.nbr),
                     dptr<int32_t>(dp.veff_index), vcell<T>(dp), a);

@@ -6,8 +6,8 @@
 //                   schedule of the projection: longer chunks amortize the pipeline start and
 //                   the coefficient atomics, shorter ones balance the load)   {8, 16, 32}
 //   * add_blocks  : consecutive blocks per CTA of the FP32 addition        {8, 16, 32}
-//   * local_variant: FP32 local kernel on rows with one-step-ahead loads, on plain rows, or on
-//                   y-pencils                                                  {0, 1, 2}
+//   * local_variant: FP32 local kernel on rows with one-step-ahead loads, on plain rows, on
+//                   y-pencils, or on y-pencils with staged neighbour cubes     {0, 1, 2, 3}
 //   * use_tc      : FP32 projector on the tensor cores (3xTF32) or on the CUDA cores
 // Each parameter is tuned in turn (coordinate descent), every candidate timed with CUDA events
 // on the caller's stream: two untimed applications, then the mean of three.  Scratch vectors
@@ -96,11 +96,11 @@ bool autotune(GreenPlan const &hp, DevicePlan &dp, cudaStream_t st, std::string 
             }
         }
     }
-    char const *const local_name[3] = {"rows with loads ahead", "plain rows", "pencils"};
+    char const *const local_name[4] = {"rows with loads ahead", "plain rows", "pencils", "staged pencils"};
     if (sizeof(T) == 4 && dp.fused_local) {
-        float t[3] = {0, 0, 0};
+        float t[4] = {0, 0, 0, 0};
         int best = 0;
-        for (int v = 0; v < 3; ++v) {
+        for (int v = 0; v < 4; ++v) {
             dp.local_variant = v;
             if (!time_part<T>(dp, 0, y, x, ci, st, t[v])) return false;
             std::snprintf(line, sizeof(line), "local kernel, %s: %.3f ms\n", local_name[v], t[v]);

@@ -4,6 +4,8 @@
 #include "solver.hpp"
 #include "vjp.hpp"
 #include "noalloc.hpp"
+#include "hamiltonian_io.hpp"
+#include "density_matrix.hpp"
 
 #include <algorithm>
 #include <atomic>
@@ -16,6 +18,7 @@ struct a43g_plan {
     a43g::DevicePlan dev;
     a43g::SolverWorkspace solver;
     a43g::BatchCache batch;          // batch plan and vectors of a43g_solve_batched
+    a43g::DensityWorkspace density;  // tables and scratch of a43g_projection_coefficients
     a43g::VjpWorkspace vjpws;
     bool energy_set = false;
     bool matrices_set = false;
@@ -334,6 +337,87 @@ int a43g_solve_batched(a43g_plan_t *plan, const a43g_solve_options_t *opts, int3
     if (rc) return rc;
     return a43g::solve_batched(plan->host, plan->dev, plan->batch, *opts, n, energies, kpoints, dVol,
                                rho, stats, (cudaStream_t)stream);
+}
+
+int a43g_projection_coefficients(a43g_plan_t *plan, const void *G, double *out, void *stream) {
+    if (!plan || !G || !out) return fail(A43G_ERR_ARGUMENT, "null argument");
+    std::lock_guard<std::mutex> lock(plan->mtx);
+    if (!plan->energy_set) return fail(A43G_ERR_STATE, "energy parameter not set (a43g_plan_set_energy)");
+    int const rc = ensure_device(plan);
+    if (rc) return rc;
+    return a43g::projection_coefficients(plan->host, plan->dev, plan->density, (double const*)G, out,
+                                         (cudaStream_t)stream);
+}
+
+struct a43g_hamiltonian { a43g::Hamiltonian h; };
+
+int a43g_hamiltonian_load(const char *filename, a43g_hamiltonian_t **h) {
+    if (!filename || !h) return fail(A43G_ERR_ARGUMENT, "null argument");
+    auto *p = new (std::nothrow) a43g_hamiltonian();
+    if (!p) return fail(A43G_ERR_MEMORY, "host allocation failed");
+    std::string err;
+    try { err = p->h.load(filename); } catch (std::bad_alloc const &) { err = "host memory exhausted"; }
+    if (!err.empty()) { delete p; return fail(A43G_ERR_ARGUMENT, err); }
+    *h = p;
+    return A43G_OK;
+}
+
+int a43g_hamiltonian_info(const a43g_hamiltonian_t *h, uint32_t ng[3], int32_t bc[3], double hg[3],
+                          int32_t *natoms, int64_t *nmat) {
+    if (!h) return fail(A43G_ERR_ARGUMENT, "null argument");
+    for (int d = 0; d < 3; ++d) {
+        if (ng) ng[d] = h->h.ng[d];
+        if (bc) bc[d] = h->h.bc[d];
+        if (hg) hg[d] = h->h.hg[d];
+    }
+    if (natoms) *natoms = int32_t(h->h.atom_mat.size());
+    if (nmat) { int64_t n = 0; for (auto const &m : h->h.atom_mat) n += int64_t(m.size()); *nmat = n; }
+    return A43G_OK;
+}
+
+int a43g_hamiltonian_get(const a43g_hamiltonian_t *h, double *Veff, double *xyzZinso, double *mats, int64_t *offsets) {
+    if (!h) return fail(A43G_ERR_ARGUMENT, "null argument");
+    if (Veff) std::memcpy(Veff, h->h.Veff.data(), h->h.Veff.size()*sizeof(double));
+    if (xyzZinso) std::memcpy(xyzZinso, h->h.xyzZinso.data(), h->h.xyzZinso.size()*sizeof(double));
+    int64_t o = 0;
+    for (size_t a = 0; a < h->h.atom_mat.size(); ++a) {
+        if (offsets) offsets[a] = o;
+        if (mats) std::memcpy(mats + o, h->h.atom_mat[a].data(), h->h.atom_mat[a].size()*sizeof(double));
+        o += int64_t(h->h.atom_mat[a].size());
+    }
+    return A43G_OK;
+}
+
+int a43g_hamiltonian_create(const uint32_t ng[3], const int32_t bc[3], const double hg[3], const double *Veff,
+                            int32_t natoms, const double *xyzZinso, const double *mats, const int64_t *offsets,
+                            a43g_hamiltonian_t **h) {
+    if (!ng || !bc || !hg || !Veff || !h || natoms < 0 || (natoms > 0 && (!xyzZinso || !mats || !offsets)))
+        return fail(A43G_ERR_ARGUMENT, "null argument");
+    auto *p = new (std::nothrow) a43g_hamiltonian();
+    if (!p) return fail(A43G_ERR_MEMORY, "host allocation failed");
+    for (int d = 0; d < 3; ++d) { p->h.ng[d] = ng[d]; p->h.bc[d] = bc[d]; p->h.hg[d] = hg[d]; }
+    p->h.Veff.assign(Veff, Veff + size_t(ng[0])*ng[1]*ng[2]);
+    p->h.xyzZinso.assign(xyzZinso, xyzZinso + 8*size_t(natoms));
+    for (int32_t a = 0; a < natoms; ++a) {
+        int const numax = int(xyzZinso[8*a + 5]);
+        if (numax < 0 || numax > 15) { delete p; return fail(A43G_ERR_ARGUMENT, "numax out of range"); }
+        int const nc = ((1 + numax)*(2 + numax)*(3 + numax))/6;
+        p->h.atom_mat.emplace_back(mats + offsets[a], mats + offsets[a] + 2*size_t(nc)*nc);
+    }
+    *h = p;
+    return A43G_OK;
+}
+
+int a43g_hamiltonian_save(const a43g_hamiltonian_t *h, const char *filename, int format, const double *spectrum) {
+    if (!h || !filename) return fail(A43G_ERR_ARGUMENT, "null argument");
+    if (0 != format && 1 != format) return fail(A43G_ERR_ARGUMENT, "format must be 0 (XML) or 1 (JSON)");
+    auto const err = h->h.save(filename, 1 == format, spectrum);
+    return err.empty() ? A43G_OK : fail(A43G_ERR_ARGUMENT, err);
+}
+
+int a43g_hamiltonian_destroy(a43g_hamiltonian_t *h) {
+    delete h;
+    return A43G_OK;
 }
 
 } // extern "C"

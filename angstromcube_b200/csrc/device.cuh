@@ -47,7 +47,7 @@ struct DevicePlan {
     // schedule parameters, set by the autotuner (autotune.cu) or left at these defaults
     uint32_t prj_chunk = 16;         // blocks per projection work item
     uint32_t add_blocks = 16;        // blocks per CTA of the FP32 addition
-    int local_variant = 2;           // FP32: 0 rows with one-step-ahead loads, 1 plain rows, 2 pencils
+    int local_variant = 2;           // FP32: 0 rows with one-step-ahead loads, 1 plain rows, 2 pencils, 3 staged pencils
     uint32_t nlists[3] = {0, 0, 0};
 
     DeviceBuffer veff_index;     // int32 [nnzb]

@@ -161,9 +161,11 @@ bool upload_plan(GreenPlan const &hp, DevicePlan &dp) {
         // FP32 projector: SIMT (default) or the tensor cores ("tc"); the FP64 path is always SIMT
         char const *e = std::getenv("A43G_PROJECTOR");
         dp.use_tc = (e && 0 == std::strcmp(e, "tc"));
-        // FP32 local kernel: y-"pencils" (default), "rows" with loads ahead or "plain" rows
+        // FP32 local kernel: y-"pencils" (default), pencils with "staged" neighbour cubes, "rows"
+        // with loads ahead or "plain" rows
         char const *l = std::getenv("A43G_LOCAL");
-        dp.local_variant = (l && 0 == std::strcmp(l, "plain")) ? 1 : ((l && 0 == std::strcmp(l, "rows")) ? 0 : 2);
+        dp.local_variant = (l && 0 == std::strcmp(l, "plain")) ? 1 : ((l && 0 == std::strcmp(l, "rows")) ? 0 :
+                           ((l && 0 == std::strcmp(l, "staged")) ? 3 : 2));
     }
     if (!dp.aac.alloc(std::max<size_t>(16, size_t(dp.ncoeffA)*dp.nCols*128*sizeof(double)))) return false;
     if (!dp.cadd.alloc(std::max<size_t>(16, size_t(dp.ncoeffA)*dp.nCols*128*sizeof(double)))) return false;

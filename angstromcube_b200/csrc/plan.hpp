@@ -134,6 +134,10 @@ struct GreenPlan {
     // slot_H with the functions of direction dir replaced by their derivative with respect to
     // the atom position (vector-Jacobian products; the reference has no derivatives)
     std::vector<double> position_derivative_tables(int dir) const;
+    // projector tables of every (atom image, source cube) pair, in the layout of slot_H and
+    // slot_mask (the functions evaluated at the points of the source cube instead of a target
+    // cube; green_dyadic::SHOprj_right, include/green_dyadic.hxx:925-1060)
+    void source_tables(std::vector<double> &H, std::vector<uint64_t> &mask) const;
     // this plan as npairs copies of the one-pair plan `one` (same geometry, potential and atom
     // matrices; no reference counterpart: the reference solves its (E, k) points one by one)
     std::string replicate(GreenPlan const &one, uint32_t npairs);

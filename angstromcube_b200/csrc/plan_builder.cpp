@@ -731,3 +731,53 @@ std::string GreenPlan::set_pair(uint32_t p, double Er, double Ei, double dVol, d
 }
 
 } // namespace a43g
+
+namespace a43g {
+
+// The 1D Hermite-Gauss functions and the spherical mask of every (image, source cube) pair,
+// evaluated as the slot tables are (the same expressions in the same order) but at the points
+// of the source cube: colCubePos instead of rowCubePos.
+void GreenPlan::source_tables(std::vector<double> &H, std::vector<uint64_t> &mask) const {
+    int const nt = (table_lmax + 1)*12;
+    H.assign(size_t(nAtomImages)*nCols*size_t(std::max(nt, 1)), 0.0);
+    mask.assign(size_t(nAtomImages)*nCols, 0);
+    if (table_lmax < 0) return;
+    double const R2 = geo.proj_radius*geo.proj_radius;
+    float const R2f = float(R2);
+    for (uint32_t a = 0; a < nAtomImages; ++a) {
+        int const lmax = AtomImageLmax[a];
+        double const isq = AtomImagePos[4*size_t(a) + 3];          // 1/sqrt(sigma)
+        double const sinv = isq*isq;
+        double const pos[3] = {AtomImagePos[4*size_t(a)], AtomImagePos[4*size_t(a) + 1], AtomImagePos[4*size_t(a) + 2]};
+        for (uint32_t s = 0; s < nCols; ++s) {
+            float const *tc = &colCubePos[4*size_t(s)];
+            double *h1 = &H[(size_t(a)*nCols + s)*nt];
+            float xi2[3][4];
+            for (int d = 0; d < 3; ++d)
+                for (int i4 = 0; i4 < 4; ++i4) {
+                    double const xi = sinv*((double(tc[d])*4 + i4 + 0.5)*geo.hg[d] - pos[d]);
+                    double const x2 = xi*xi;
+                    xi2[d][i4] = float(x2);
+                    double hm = 0, h = (x2 < R2) ? std::exp(-0.5*x2) : 0.0;
+                    h1[(0*3 + d)*4 + i4] = h;
+                    for (int nu = 0; nu < lmax; ++nu) {
+                        double const hp = xi*h - 0.5*nu*hm;
+                        h1[((nu + 1)*3 + d)*4 + i4] = hp;
+                        hm = h; h = hp;
+                    }
+                }
+            uint64_t m = 0;
+            for (int z = 0; z < 4; ++z) {
+                float const d2z = xi2[2][z] - R2f;
+                for (int y = 0; y < 4; ++y) {
+                    float const d2yz = xi2[1][y] + d2z;
+                    for (int x = 0; x < 4; ++x)
+                        if (xi2[0][x] + d2yz < 0.f) m |= 1ull << ((z*4 + y)*4 + x);
+                }
+            }
+            mask[size_t(a)*nCols + s] = m;
+        }
+    }
+}
+
+} // namespace a43g

@@ -19,7 +19,7 @@
 //    has fallen by update_factor since its last one, when all of them are below the tolerance,
 //    or after update_gap iterations.  The CGS-type recurrences of tfQMR amplify the FP32
 //    rounding strongly where the energy lies close to the spectrum: a source cube whose largest
-//    true residual has not fallen by 10 % over stall_limit replacements (or is not finite) leaves the FP32
+//    true residual has not halved over stall_limit replacements (or is not finite) leaves the FP32
 //    recurrences, and all such sources then continue as FP64 tfQMR from their FP64 solution.
 //
 // One iteration = two operator applications.  The BLAS-1 work is fused so that every vector
@@ -90,7 +90,7 @@ struct SrcState {
     int32_t upd;                 // replacement in this iteration
     int32_t updates;             // replacements done
     int32_t done;                // no active column left
-    int32_t stall;               // replacements since its largest true residual last fell by 10 %
+    int32_t stall;               // replacements since its largest true residual last halved
     int32_t fallback;            // left the FP32 recurrences for FP64
     int32_t nonfinite;           // ... with a residual that was not finite
     double est_ref;              // largest true residual of its active columns at the last replacement
@@ -424,8 +424,9 @@ __device__ void step_replace(Ctx const &c, uint32_t s, double const (&r)[3]) {
         SrcState &src = c.ss[s];
         src.est_ref = e;
         src.updates += 1;
-        // progress: the largest true residual fell by 10 % since the best one so far
-        if (e < 0.9*src.best) { src.best = e; src.stall = 0; } else src.stall += 1;
+        // progress: the largest true residual halved since the best one so far (slower progress
+        // is slower than the FP64 recurrences, whose iterations cost 2.7 times as much)
+        if (e < 0.5*src.best) { src.best = e; src.stall = 0; } else src.stall += 1;
         fb = any && (!finite || src.stall >= c.stall_limit);
         if (fb) { src.fallback = 1; src.nonfinite = !finite; }
     }
@@ -784,11 +785,12 @@ uint32_t chunks_for(DevicePlan const &dp) {
 
 } // namespace
 
-bool TfqmrVectors::alloc(size_t nreals, size_t elem_bytes) {
-    if (n == nreals && elem == elem_bytes && X.ptr) return true;
+bool TfqmrVectors::alloc(size_t nreals, size_t elem_bytes, bool with_x) {
+    if (n == nreals && elem == elem_bytes && W.ptr && (!with_x || X.ptr)) return true;
     n = nreals; elem = elem_bytes;
     size_t const b = std::max<size_t>(16, nreals*elem_bytes);
-    return X.alloc(b) && W.alloc(b) && U1.alloc(b) && U2.alloc(b) && V.alloc(b) && D.alloc(b) &&
+    if (!with_x) X.release();
+    return (!with_x || X.alloc(b)) && W.alloc(b) && U1.alloc(b) && U2.alloc(b) && V.alloc(b) && D.alloc(b) &&
            AU1.alloc(b) && AU2.alloc(b);
 }
 
@@ -858,7 +860,7 @@ bool prepare(DevicePlan &dp, SolverWorkspace &ws, a43g_solve_options_t const &op
     c.gap = (opt.update_gap > 0) ? opt.update_gap : 10;
     c.mixed = mixed ? 1 : 0;
     c.retire = retire ? 1 : 0;
-    c.stall_limit = 8;
+    c.stall_limit = 3;
     c.abs_tol = 0;
     p.units = units;
     return true;
@@ -991,19 +993,37 @@ bool run(DevicePlan &dp, SolverWorkspace &ws, TfqmrVectors &v, Prepared &p, T *X
     return true;
 }
 
-// FP64 solution X64 and operator scratch AX64, and the recurrence vectors of the precision
-// (the FP64 tfQMR keeps its solution in X64; its vector set's X is not used)
+// The FP64 solution X64 and the recurrence vectors of the precision: FP64 tfQMR keeps its
+// solution in X64 and uses AU1 as the scratch of its final residual (8 FP64 vectors); the FP32
+// recurrences have their own X (X32) and the FP64 scratch AX64 of the replacements (8 FP32 and
+// 2 FP64 vectors).  Vectors of the other precision are released first when the free memory does
+// not hold both (large plans: 9 FP64 vectors of the 300,960-block cell fill 178 GB).
 bool ensure_vectors(SolverWorkspace &ws, DevicePlan &dp, bool mixed) {
     size_t const n = size_t(dp.nnzb)*kBlk;
-    if (!ws.X64.alloc(n*8) || !ws.AX64.alloc(n*8)) return false;
-    return mixed ? ws.v32.alloc(n, 4) : ws.v64.alloc(n, 8);
+    size_t need = 0;
+    if (ws.X64.bytes < n*8) need += n*8;
+    if (mixed) {
+        if (ws.AX64.bytes < n*8) need += n*8;
+        if (!ws.v32.W.ptr || ws.v32.n != n) need += 8*n*4;
+    } else if (!ws.v64.W.ptr || ws.v64.n != n) {
+        need += 7*n*8;
+    }
+    size_t freeb = 0, total = 0;
+    if (need && cudaSuccess == cudaMemGetInfo(&freeb, &total) && freeb < need + (size_t(512) << 20)) {
+        if (mixed) ws.v64.release(); else { ws.v32.release(); ws.AX64.release(); }
+    }
+    if (!ws.X64.alloc(n*8)) return false;
+    if (mixed) return ws.AX64.alloc(n*8) && ws.v32.alloc(n, 4, true);
+    return ws.v64.alloc(n, 8, false);
 }
 
 } // namespace
 
 size_t solve_bytes(DevicePlan const &dp, int precision) {
+    // FP64: X64 and 7 recurrence vectors; FP32: 8 FP32 vectors, X64 and AX64, or, for sources
+    // continued in FP64, X64 and 7 FP64 vectors (the larger of the two)
     size_t const n = size_t(dp.nnzb)*kBlk;
-    return (A43G_F32 == precision) ? n*(8*4 + 2*8) : n*(9*8);
+    return (A43G_F32 == precision) ? n*std::max(8*4 + 2*8, 8 + 7*8) : n*(8*8);
 }
 
 int solve(GreenPlan &hp, DevicePlan &dp, SolverWorkspace &ws, a43g_solve_options_t const &opt,
@@ -1014,7 +1034,9 @@ int solve(GreenPlan &hp, DevicePlan &dp, SolverWorkspace &ws, a43g_solve_options
     if (A43G_F64 != opt.precision && A43G_F32 != opt.precision) { set_error("precision must be A43G_F64 or A43G_F32"); return A43G_ERR_ARGUMENT; }
     (void)hp;
     bool const mixed = (A43G_F32 == opt.precision);
-    bool const retire = 0 == (opt.flags & A43G_SOLVE_NO_RETIRE);
+    // the FP32 recurrences always retire finished sources (stalled sources leave them retired and
+    // continue in FP64 on their own); A43G_SOLVE_NO_RETIRE applies to FP64 solves
+    bool const retire = mixed || 0 == (opt.flags & A43G_SOLVE_NO_RETIRE);
     uint32_t const nsrc = dp.nCols;
     uint32_t const live = (per_source && per_source->live_sources) ? std::min(per_source->live_sources, nsrc) : nsrc;
     std::vector<uint8_t> mask(nsrc, 0);
@@ -1057,17 +1079,28 @@ int solve(GreenPlan &hp, DevicePlan &dp, SolverWorkspace &ws, a43g_solve_options
         }
         int const left = opt.max_iterations - res.iterations;
         if (nfb && left > 0) {
-            if (!ws.v64.alloc(n, 8)) return A43G_ERR_MEMORY;
+            // the FP32 set is done with: released first where both sets do not fit
+            size_t freeb = 0, total = 0;
+            if ((!ws.v64.W.ptr || ws.v64.n != n) && cudaSuccess == cudaMemGetInfo(&freeb, &total) &&
+                freeb < 7*n*8 + (size_t(512) << 20)) {
+                A43G_CUDA_TRY_RC(cudaStreamSynchronize(st));
+                v.release();
+                ws.AX64.release();
+            }
+            if (!ws.v64.alloc(n, 8, false)) return A43G_ERR_MEMORY;
             auto &w = ws.v64;
             Prepared p2;
             a43g_solve_options_t o2 = opt;
             if (!prepare(dp, ws, o2, false, true, p2)) return A43G_ERR_MEMORY;
             p2.c.abs_tol = 1;
+            // the QMR bound decides FP64 convergence; aiming at half the tolerance keeps the true
+            // residual, which the solve reports, below the tolerance
+            p2.c.tol = 0.5*opt.tolerance;
             // R = B - A X64 of the continuing sources into W and U1; D = 0
-            if (!apply<double>(dp, dptr<double>(ws.AX64), X64, nullptr, false, st)) return A43G_ERR_CUDA;
+            if (!apply<double>(dp, dptr<double>(w.AU1), X64, nullptr, false, st)) return A43G_ERR_CUDA;
             A43G_CUDA_TRY_RC(cudaMemsetAsync(w.D.ptr, 0, n*8, st));
             A43G_CUDA_TRY_RC(cudaMemcpyAsync(dp.src_active.ptr, fb.data(), nsrc, cudaMemcpyHostToDevice, st));
-            k_start64<<<p2.units, 256, 0, st>>>(dptr<double>(w.W), dptr<double>(w.U1), X64, dptr<double>(ws.AX64),
+            k_start64<<<p2.units, 256, 0, st>>>(dptr<double>(w.W), dptr<double>(w.U1), X64, dptr<double>(w.AU1),
                                                p2.c, dptr<uint8_t>(dp.src_active));
             count_launch();
             if (!run<double>(dp, ws, w, p2, X64, left, opt.check_every, nullptr, nullptr, st, res, opt.echo, fb))
@@ -1086,15 +1119,17 @@ int solve(GreenPlan &hp, DevicePlan &dp, SolverWorkspace &ws, a43g_solve_options
         if (!run<double>(dp, ws, v, p, X64, opt.max_iterations, opt.check_every, nullptr, nullptr, st, res, opt.echo, mask))
             return A43G_ERR_CUDA;
     }
-    // true residual of every column's FP64 solution (the whole operator, no source skipped)
+    // true residual of every column's FP64 solution (the whole operator, no source skipped), in
+    // whichever FP64 scratch the solve holds
+    double *AXs = ws.AX64.ptr ? dptr<double>(ws.AX64) : dptr<double>(ws.v64.AU1);
     dp.retire = false;
-    if (!launch_action<double>(dp, dptr<double>(ws.AX64), X64, dptr<uint16_t>(dp.colindx), st)) return A43G_ERR_CUDA;
+    if (!launch_action<double>(dp, AXs, X64, dptr<uint16_t>(dp.colindx), st)) return A43G_ERR_CUDA;
     res.applications += 1;
-    k_final<<<p.units, 256, 0, st>>>(dptr<double>(ws.AX64), p.c);
+    k_final<<<p.units, 256, 0, st>>>(AXs, p.c);
     count_launch();
     if (Xout) A43G_CUDA_TRY_RC(cudaMemcpyAsync(Xout, X64, n*8, cudaMemcpyDeviceToDevice, st));
     if (rho) {
-        double *rb = dptr<double>(ws.AX64);      // the residual scratch is free again
+        double *rb = AXs;                        // the residual scratch is free again
         k_export_rho<double><<<nsrc, 64, 0, st>>>(rb, X64, dptr<uint32_t>(dp.subset_dev), nsrc);
         count_launch();
         A43G_CUDA_TRY_RC(cudaMemcpyAsync(rho, rb, size_t(nsrc)*128*8, cudaMemcpyDeviceToHost, st));

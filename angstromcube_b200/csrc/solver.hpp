@@ -13,13 +13,13 @@ struct TfqmrVectors {
     size_t elem = 0;             // bytes per real
     size_t n = 0;                // reals per vector (nnzb * 8192)
     DeviceBuffer X, W, U1, U2, V, D, AU1, AU2;
-    bool alloc(size_t nreals, size_t elem_bytes);
+    bool alloc(size_t nreals, size_t elem_bytes, bool with_x);
     void release();
 };
 
 struct SolverWorkspace {
     TfqmrVectors v64, v32;
-    DeviceBuffer X64, AX64;          // FP64 solution of the FP32 recurrences, FP64 operator scratch
+    DeviceBuffer X64, AX64;          // FP64 solution, FP64 operator scratch of the FP32 recurrences
     DeviceBuffer state;              // per-column and per-source scalars, control block (solver.cu)
     DeviceBuffer part, tickets;      // fixed-order column reductions
     void *host_ctl = nullptr;        // pinned copy of the control block
@@ -42,7 +42,7 @@ struct BatchCache {
     uint32_t npairs = 0;
 };
 
-// device bytes of the solver vectors of one solve of this plan in the given precision
+// peak device bytes of the solver vectors of one solve of this plan in the given precision
 size_t solve_bytes(DevicePlan const &dp, int precision);
 
 int solve(GreenPlan &hp, DevicePlan &dp, SolverWorkspace &ws, a43g_solve_options_t const &opt,

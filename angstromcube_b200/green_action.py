@@ -123,6 +123,22 @@ def vjp(plan, L, G, potential=True, matrices=True, positions=True, stream=0):
     return out
 
 
+def get_projection_coefficients(plan, G, stream=0):
+    """Atomic density matrices Im <p_i|G|p_j> (green_dyadic::get_projection_coefficients) of a
+    CUDA float64 Green function G [nnzb, 2, 64, 64]: a list of [nSHO, nSHO] arrays in the order of
+    export()["global_atom_ids"]."""
+    e = plan.export()
+    ns = [((int(l) + 1) * (int(l) + 2) * (int(l) + 3)) // 6 for l in e["AtomLmax"]]
+    out = np.zeros(max(1, sum(n * n for n in ns)))
+    st = ctypes.c_void_p(stream if isinstance(stream, int) else stream.cuda_stream)
+    check(_lib.lib().a43g_projection_coefficients(plan.handle, ptr(G), ptr(out), st), "a43g_projection_coefficients")
+    res, o = [], 0
+    for n in ns:
+        res.append(out[o:o + n * n].reshape(n, n).copy())
+        o += n * n
+    return res
+
+
 def autotune(plan, precision="float32", stream=0):
     """Chooses the action's schedule for this plan by timing (a43g_plan_autotune); returns the
     report text."""

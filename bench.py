@@ -12,11 +12,11 @@ solves.  Every radius above 8 Bohr leaves the 16 Bohr cell untruncated, so all 1
 plan of 32,768 blocks (checked at set-up).  A solve is one (E, k) pair with all 512 columns at a
 true FP64 relative residual below 1e-8.
 
-A step solves one wave of --wave pairs (default 2) with a43g_solve_batched: FP32 recurrences and
+A step solves one wave of --wave pairs (default 1) with a43g_solve_batched: FP32 recurrences and
 operator, FP64 solution and residual replacement, finished source cubes retired, sources whose
 FP32 recurrences stall continued in FP64.  The steps walk through the 128 pairs in a fixed order
 that spreads them over the contour (pair 37*i mod 128 for the i-th solve), so a run of K steps
-times a sample of 2K pairs of the whole contour; `value` counts the converged solves per second
+times a sample of K*P pairs of the whole contour; `value` counts the converged solves per second
 of device time.  Reported beside it on the same pairs: the plain FP64 solver (the reference's
 algorithm: FP64 tfQMR, no retirement, one pair at a time) on the first pairs of the sample, per
 pair status and iterations, the fused local kernel and the projector against their rooflines,
@@ -67,9 +67,11 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--wave", type=int, default=2, help="(E, k) pairs per step")
-    ap.add_argument("--fp64-pairs", type=int, default=4, help="pairs of the sample also solved in plain FP64")
+    ap.add_argument("--wave", type=int, default=1, help="(E, k) pairs per step")
+    ap.add_argument("--fp64-pairs", type=int, default=2, help="pairs of the sample also solved in plain FP64")
     ap.add_argument("--full-contour", action="store_true", help="solve all pairs (mixed+batched and plain FP64)")
+    ap.add_argument("--convergence-scan", action="store_true",
+                    help="FP64 iterations over the contour energies and the residual history at -0.2+0.02i")
     ap.add_argument("--nk", type=int, default=4, help="k-points of the contour")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
@@ -553,6 +555,41 @@ def full_contour(a):
                       "seconds": [t_mixed, t64], "converged": [cm, c64], "pairs": len(pairs)}})
 
 
+def convergence_scan(a):
+    """Convergence of the plain FP64 solver on the one-source version of the contour cell: the
+    iterations to 1e-8 at the 32 contour energies (Gamma, at most 1500 iterations), and the true
+    relative residual at E = -0.2 + 0.02i (the energy of the cell's single-energy configuration)
+    after 100, 200, ... 2000 iterations.  The solver is deterministic, so the solve capped at n
+    iterations is the first n iterations of the uncapped one."""
+    import numpy as np
+    import torch
+    from angstromcube_b200 import green_action, green_function as gf, workloads
+    torch.cuda.set_device(0)
+    w = workloads.make("periodic16_64atoms_s1x1x1")
+    plan = gf.construct_Green_function(w.geometry)
+    gf.update_potential(plan, w.Vcell, w.mats, w.offsets, layout="cells")
+    stream = torch.cuda.Stream()
+    E, _ = workloads.contour_semicircle(32)
+    scan = []
+    for e in E:
+        gf.update_energy_parameter(plan, e, w.dVol)
+        st, _ = green_action.solve(plan, stream=stream, want_rho=False, precision="float64", tolerance=1e-8,
+                                   max_iterations=1500, check_every=1, retire=False)
+        scan.append({"E": [e.real, e.imag], "iterations": st["iterations"], "converged": bool(st["converged"]),
+                     "residual": st["residual_max"], "seconds": st["seconds"]})
+        emit({"scan": scan[-1]})
+    gf.update_energy_parameter(plan, complex(-0.2, 0.02), w.dVol)
+    hist = []
+    for n in range(100, 2001, 100):
+        st, _ = green_action.solve(plan, stream=stream, want_rho=False, precision="float64", tolerance=1e-8,
+                                   max_iterations=n, check_every=1, retire=False)
+        hist.append({"iterations": st["iterations"], "residual": st["residual_max"],
+                     "estimate": st["residual_estimate"]})
+        emit({"history": hist[-1]})
+    emit({"convergence_scan": {"cell": "periodic16_64atoms_s1x1x1", "tolerance": 1e-8, "scan": scan,
+                               "history_E": [-0.2, 0.02], "history": hist}})
+
+
 def launch_ranks(a):
     """--gpus N without a launcher: start N ranks with torch.distributed.run (one process per GPU,
     NCCL over 127.0.0.1) and return its exit code."""
@@ -574,6 +611,9 @@ def main():
         return
     if a.full_contour:
         full_contour(a)
+        return
+    if a.convergence_scan:
+        convergence_scan(a)
         return
     plan, w, pairs, stream, opts, out, hbm, bf16, peak_kind, world, rank, records = our_arm(a)
     if rank == 0:

@@ -75,7 +75,8 @@ typedef struct {
 
 /* Solver options and per-solve statistics (tfQMR, Freund 1993, per-column scalars) */
 enum {
-    A43G_SOLVE_NO_RETIRE = 1  /* keep computing on finished source cubes (the reference's tfQMRgpu does) */
+    A43G_SOLVE_NO_RETIRE = 1  /* FP64 solves: keep computing on finished source cubes (the reference's
+                                 tfQMRgpu does); FP32 recurrences always retire them */
 };
 
 typedef struct {
@@ -206,6 +207,40 @@ int a43g_solve(a43g_plan_t *plan, const a43g_solve_options_t *opts, void *X, dou
 int a43g_solve_batched(a43g_plan_t *plan, const a43g_solve_options_t *opts, int32_t n,
                        const double *energies, const double *kpoints, double dVol,
                        double *rho, a43g_solve_stats_t *stats, void *stream);
+
+/* ---- atomic density matrices: replaces green_dyadic::get_projection_coefficients
+ * (include/green_dyadic.hxx:1062-1088, with SHOprj_right, :925-1060).  G: device FP64 block
+ * vector [nnzb][2][64][64] (a Green function of this plan); out: host Im <p_i|G|p_j> of every plan
+ * atom, [nSHO][nSHO] each, concatenated in the order of the export's global_atom_ids.  Plans with
+ * periodic atom images (nAtomImages > nAtoms) are refused with A43G_ERR_UNSUPPORTED, as the
+ * reference refuses them.  Synchronizes the stream. */
+int a43g_projection_coefficients(a43g_plan_t *plan, const void *G, double *out, void *stream);
+
+/* ---- the grid Hamiltonian file that a43 exports (Hmt.xml or Hmt.json): cell, boundary
+ * conditions, spacing, the local potential on the full grid and the SHO atoms with their
+ * Hamiltonian and overlap matrices. */
+typedef struct a43g_hamiltonian a43g_hamiltonian_t;
+/* replaces green_input::load_Hamiltonian (src/green_input.cxx:29-221; a name containing ".json"
+ * is read as JSON, json_reading::load_Hamiltonian, include/json_reading.hxx:61-229, falling back
+ * to XML) */
+int a43g_hamiltonian_load(const char *filename, a43g_hamiltonian_t **h);
+/* grid points, boundary conditions, spacings, number of atoms and of matrix doubles
+ * (sum over atoms of 2 nSHO^2); any output may be NULL */
+int a43g_hamiltonian_info(const a43g_hamiltonian_t *h, uint32_t ng[3], int32_t bc[3], double hg[3],
+                          int32_t *natoms, int64_t *nmat);
+/* copies out Veff [nz][ny][nx], xyzZinso [natoms][8] (x, y, z relative to the cell centre, Z,
+ * global id, numax, sigma, 0), the matrices concatenated per atom [2][nSHO][nSHO] (hamiltonian,
+ * overlap) and their offsets [natoms] in doubles; any output may be NULL */
+int a43g_hamiltonian_get(const a43g_hamiltonian_t *h, double *Veff, double *xyzZinso, double *mats,
+                         int64_t *offsets);
+/* a Hamiltonian from arrays in the layouts of a43g_hamiltonian_get (to write one) */
+int a43g_hamiltonian_create(const uint32_t ng[3], const int32_t bc[3], const double hg[3], const double *Veff,
+                            int32_t natoms, const double *xyzZinso, const double *mats, const int64_t *offsets,
+                            a43g_hamiltonian_t **h);
+/* replaces grid_operators::write_to_file (include/grid_operators.hxx:460-613): format 0 XML,
+ * 1 JSON; spectrum (optional) min, max, Fermi level in Hartree */
+int a43g_hamiltonian_save(const a43g_hamiltonian_t *h, const char *filename, int format, const double *spectrum);
+int a43g_hamiltonian_destroy(a43g_hamiltonian_t *h);
 
 #ifdef __cplusplus
 }

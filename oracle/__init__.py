@@ -69,6 +69,8 @@ def _load_ref():
         lib.ref_set_atom_matrices.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
         lib.ref_set_energy.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double, ctypes.c_double]
         lib.ref_set_kpoint.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        lib.ref_projection_coefficients.restype = ctypes.c_int
+        lib.ref_projection_coefficients.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
         lib.ref_action_f64.restype = ctypes.c_double
         lib.ref_action_f64.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
         lib.ref_action_f32.restype = ctypes.c_double
@@ -172,6 +174,22 @@ class RefGreen:
     def set_kpoint(self, k):
         kk = np.ascontiguousarray(k, dtype=np.float64)
         self.lib.ref_set_kpoint(self.h, _ptr(kk))
+
+    def projection_coefficients(self, G):
+        """green_dyadic::get_projection_coefficients: Im <p_i|G|p_j> of every plan atom for an FP64
+        block vector G [nnzb, 2, 64, 64]; a list of [nSHO, nSHO] arrays, or None where the
+        reference refuses (plans with periodic atom images)."""
+        e = self.export()
+        ns = [((int(l) + 1) * (int(l) + 2) * (int(l) + 3)) // 6 for l in e["AtomLmax"]]
+        out = np.zeros(max(1, sum(n * n for n in ns)))
+        G = np.ascontiguousarray(G, dtype=np.float64)
+        if self.lib.ref_projection_coefficients(self.h, _ptr(G), _ptr(out)) != 0:
+            return None
+        res, o = [], 0
+        for n in ns:
+            res.append(out[o:o + n * n].reshape(n, n).copy())
+            o += n * n
+        return res
 
     def action(self, x):
         """y = (H - E S) x for x of shape [nnzb, 2, 64, 64], float64 or float32."""

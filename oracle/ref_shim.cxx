@@ -272,6 +272,24 @@ double ref_action_f32(void *h, float *y, const float *x) {
                                rp->colIndex.data(), nnzb, p.nCols);
 }
 
+// green_dyadic::get_projection_coefficients (include/green_dyadic.hxx:1062-1088): the atomic
+// density matrices Im <p_i|G|p_j> of every plan atom from an FP64 block vector G, concatenated
+// [nAtoms][nSHO][nSHO]; returns -1 where the reference refuses (atom images beyond the atoms)
+int ref_projection_coefficients(void *h, const double *G, double *out) {
+    auto *rp = (RefPlan*)h;
+    auto &p = rp->p;
+    auto const &dp = p.dyadic_plan;
+    if (dp.nAtomImages != dp.nAtoms) return -1;
+    auto const res = green_dyadic::get_projection_coefficients<double,2,1>(
+        (double const(*)[2][64][64])G, dp, p.rowindx, p.rowCubePos, p.colCubePos, 0);
+    size_t off{0};
+    for (auto const &m : res) {
+        std::memcpy(out + off, m.data(), m.size()*sizeof(double));
+        off += m.size();
+    }
+    return 0;
+}
+
 // kinetic_plan::set_phase (src/kinetic_plan.cxx:214-269): phase[2][2] for one direction
 double ref_set_phase(double *phase4, double angle) {
     return kinetic_plan::set_phase((double(*)[2])phase4, angle, 'x', 0);

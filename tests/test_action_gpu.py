@@ -44,11 +44,12 @@ def test_action_fp64_fp32_vs_oracle(name):
     assert rel_err(y32, y_ref) < FP32_TOL
 
 
-@pytest.mark.parametrize("variant", ["rows", "plain", "pencils"])
+@pytest.mark.parametrize("variant", ["rows", "plain", "pencils", "staged"])
 @pytest.mark.parametrize("name", sorted(GEOMETRIES))
 def test_action_fp32_local_variants_vs_oracle(name, variant, monkeypatch):
-    """Every FP32 local kernel (rows with loads ahead; plain rows; y-pencils, the default)
-    matches the oracle on every boundary condition, with Bloch phases (k != 0)."""
+    """Every FP32 local kernel (rows with loads ahead; plain rows; y-pencils; y-pencils with staged
+    neighbour cubes, the default) matches the oracle on every boundary condition, with Bloch
+    phases (k != 0)."""
     g = GEOMETRIES[name]()
     Vc, mats, offs, E, k, dVol, na = inputs_for(g)
     monkeypatch.setenv("A43G_LOCAL", variant)

@@ -12,7 +12,7 @@ import numpy as np
 import pytest
 
 from helpers import geometry, inputs_for, product_plan
-from angstromcube_b200 import green_action
+from angstromcube_b200 import green_action, workloads
 
 torch = pytest.importorskip("torch")
 pytestmark = pytest.mark.gpu
@@ -159,9 +159,10 @@ def test_vjp_solve_gradient_vs_finite_differences():
     assert abs(fd - gR[2]) <= 1e-6 * max(abs(gR[2]), 1e-3 * np.abs(gR).max()), (fd, gR)
 
 
-def test_vjp_potential_matches_reference_cpu_solves():
-    """dJ/dV assembled on the CPU from solves with the reference's own action (oracle/_ref, its
-    CPU build, driven by the numpy tfQMR restatement) agrees with the GPU adjoint gradient."""
+def test_vjp_matches_reference_cpu_solves():
+    """The gradient from solves with the reference's own action (oracle/_ref, its CPU build,
+    driven by the numpy tfQMR restatement) agrees with the GPU adjoint gradient: dJ/dV and dF/dM
+    assembled on the CPU, dF/dR through the vector-Jacobian products of the CPU solutions."""
     import oracle
     from oracle import tfqmr
     from helpers import reference_plan
@@ -196,5 +197,34 @@ def test_vjp_potential_matches_reference_cpu_solves():
     G, _ = _solve(p)
     Ga, _ = _solve(product_plan(g, Vc, mats, offs, E.conjugate(), k, dVol))
     Lt = torch.stack([Ga[:, 0], -Ga[:, 1]], dim=1) * torch.from_numpy(W).cuda()
-    gV_gpu = np.imag(-w * green_action.vjp(p, Lt, G, matrices=False, positions=False)["V"])
+    out_gpu = green_action.vjp(p, Lt, G)
+    gV_gpu = np.imag(-w * out_gpu["V"])
     assert np.abs(gV_gpu - gV_cpu).max() <= 1e-7 * np.abs(gV_cpu).max()
+    # dF/dM_A = sum over columns of l_A g_A^T with g_A = sum_i ph_i P_i^T G and
+    # l_A = sum_i conj(ph_i) P_i^T Lambda over the images i of atom A, assembled on the CPU from the
+    # reference solves with the oracle's projection (P^T x per image, pinned to the reference)
+    e = p.export()
+    o = oracle.RestatedOracle(e, Vc, E)
+    Gr = np.stack([Gc.real, Gc.imag], axis=1)
+    Lr = np.stack([Lam.real, Lam.imag], axis=1)
+    _, apcG, _ = o.dyadic(Gr, want_coefficients=True)
+    _, apcL, _ = o.dyadic(Lr, want_coefficients=True)
+    aG = apcG[:, 0] + 1j * apcG[:, 1]                  # [coefficients of all images (nCols = 1), 64 columns]
+    aL = apcL[:, 0] + 1j * apcL[:, 1]
+    ph = e["AtomImagePhase"][:, 0] + 1j * e["AtomImagePhase"][:, 1]
+    starts = e["AtomImageStarts"]
+    for slot in range(len(e["AtomLmax"])):
+        nc = workloads.nsho(int(e["AtomLmax"][slot]))
+        gA = np.zeros((nc, 64), complex); lA = np.zeros((nc, 64), complex)
+        for k in range(e["SHOsum_start"][slot], e["SHOsum_start"][slot + 1]):
+            i = e["SHOsum_col"][k]
+            gA += ph[i] * aG[starts[i]:starts[i] + nc]
+            lA += np.conj(ph[i]) * aL[starts[i]:starts[i] + nc]
+        dM_cpu = lA @ gA.T
+        assert np.abs(out_gpu["M"][slot] - dM_cpu).max() <= 1e-7 * np.abs(dM_cpu).max()
+    # positions: the vector-Jacobian products of the reference CPU solutions against those of the
+    # GPU solutions (the same kernels, different solves)
+    Gcu = torch.from_numpy(Gr).cuda()
+    Lcu = torch.from_numpy(Lr).cuda()
+    dR_ref = green_action.vjp(p, Lcu, Gcu, potential=False, matrices=False)["R"]
+    assert np.abs(out_gpu["R"] - dR_ref).max() <= 1e-7 * np.abs(dR_ref).max()
