@@ -15,10 +15,10 @@ A43G_F64, A43G_F32 = 0, 1
 
 # every entry point declared in include/a43g.h
 EXPORTED = [
-    "a43g_last_error", "a43g_version", "a43g_plan_build", "a43g_plan_destroy", "a43g_plan_get_sizes",
+    "a43g_last_error", "a43g_version", "a43g_plan_build", "a43g_plan_build_device", "a43g_plan_destroy", "a43g_plan_get_sizes",
     "a43g_plan_export", "a43g_plan_set_potential", "a43g_plan_set_atom_matrices", "a43g_plan_set_energy",
     "a43g_plan_set_kpoint", "a43g_plan_upload", "a43g_action_multiply", "a43g_action_part", "a43g_vjp", "a43g_plan_autotune", "a43g_action_multiply_noalloc",
-    "a43g_kernel_launches", "a43g_plan_device_status", "a43g_solve", "a43g_solve_batched",
+    "a43g_kernel_launches", "a43g_plan_device_status", "a43g_solve", "a43g_solve_traced", "a43g_solve_batched",
     "a43g_hamiltonian_load", "a43g_hamiltonian_info", "a43g_hamiltonian_get", "a43g_hamiltonian_create",
     "a43g_hamiltonian_save", "a43g_hamiltonian_destroy", "a43g_projection_coefficients",
 ]
@@ -86,6 +86,7 @@ def lib():
         L.a43g_last_error.restype = ctypes.c_char_p
         L.a43g_version.restype = ctypes.c_char_p
         L.a43g_plan_build.argtypes = [ctypes.POINTER(Geometry), ctypes.POINTER(vp)]
+        L.a43g_plan_build_device.argtypes = [ctypes.POINTER(Geometry), ctypes.POINTER(vp)]
         L.a43g_plan_destroy.argtypes = [vp]
         L.a43g_plan_get_sizes.argtypes = [vp, ctypes.POINTER(PlanSizes)]
         L.a43g_plan_export.argtypes = [vp, ctypes.POINTER(PlanExport)]
@@ -102,6 +103,8 @@ def lib():
         L.a43g_kernel_launches.restype = ctypes.c_uint64
         L.a43g_plan_device_status.argtypes = [vp]
         L.a43g_solve.argtypes = [vp, ctypes.POINTER(SolveOptions), vp, vp, ctypes.POINTER(SolveStats), vp]
+        L.a43g_solve_traced.argtypes = [vp, ctypes.POINTER(SolveOptions), vp, vp, ctypes.POINTER(SolveStats), vp,
+                                        vp, i32, vp, i32, ctypes.POINTER(i32)]
         L.a43g_solve_batched.argtypes = [vp, ctypes.POINTER(SolveOptions), i32, vp, vp, f64, vp,
                                          ctypes.POINTER(SolveStats), vp]
         L.a43g_hamiltonian_load.argtypes = [ctypes.c_char_p, ctypes.POINTER(vp)]

@@ -64,7 +64,9 @@ const char *a43g_last_error(void) { return a43g::g_error.c_str(); }
 
 const char *a43g_version(void) { return "a43g 0.1 (sm_100a)"; }
 
-int a43g_plan_build(const a43g_geometry_t *g, a43g_plan_t **plan) {
+namespace {
+
+int build_plan(const a43g_geometry_t *g, a43g_plan_t **plan, a43g::ImageRowsFn image_rows) {
     if (!g || !plan) return fail(A43G_ERR_ARGUMENT, "null argument");
     if (g->natoms < 0 || (g->natoms > 0 && !g->xyzZinso)) return fail(A43G_ERR_ARGUMENT, "atoms missing");
     auto *p = new (std::nothrow) a43g_plan();
@@ -76,10 +78,22 @@ int a43g_plan_build(const a43g_geometry_t *g, a43g_plan_t **plan) {
     geo.r_trunc = g->r_trunc; geo.nFD = g->nFD; geo.proj_radius = g->proj_radius;
     geo.xyzZinso.assign(g->xyzZinso, g->xyzZinso + 8*size_t(g->natoms));
     std::string err;
-    try { err = p->host.build(geo); } catch (std::bad_alloc const &) { err = "host memory exhausted"; }
-    if (!err.empty()) { delete p; return fail(A43G_ERR_ARGUMENT, err); }
+    try { err = p->host.build(geo, image_rows); } catch (std::bad_alloc const &) { err = "host memory exhausted"; }
+    if (!err.empty()) {
+        delete p;
+        bool const device = 0 == err.rfind("device plan construction", 0);
+        return fail(device ? A43G_ERR_CUDA : A43G_ERR_ARGUMENT, err);
+    }
     *plan = p;
     return A43G_OK;
+}
+
+} // namespace
+
+int a43g_plan_build(const a43g_geometry_t *g, a43g_plan_t **plan) { return build_plan(g, plan, nullptr); }
+
+int a43g_plan_build_device(const a43g_geometry_t *g, a43g_plan_t **plan) {
+    return build_plan(g, plan, a43g::image_rows_on_device);
 }
 
 int a43g_plan_destroy(a43g_plan_t *plan) {
@@ -323,6 +337,27 @@ int a43g_solve(a43g_plan_t *plan, const a43g_solve_options_t *opts, void *X, dou
     a43g_solve_stats_t local{};
     int const r = a43g::solve(plan->host, plan->dev, plan->solver, *opts, X, rho, stats ? stats : &local,
                               (cudaStream_t)stream);
+    return r;
+}
+
+int a43g_solve_traced(a43g_plan_t *plan, const a43g_solve_options_t *opts, void *X, double *rho,
+                      a43g_solve_stats_t *stats, void *stream, const void *X_reference, int32_t every,
+                      double *trace, int32_t capacity, int32_t *count) {
+    if (!plan || !opts || !X_reference || (capacity > 0 && !trace)) return fail(A43G_ERR_ARGUMENT, "null argument");
+    std::lock_guard<std::mutex> lock(plan->mtx);
+    if (!plan->energy_set) return fail(A43G_ERR_STATE, "energy parameter not set (a43g_plan_set_energy)");
+    int const rc = ensure_device(plan);
+    if (rc) return rc;
+    a43g_solve_stats_t local{};
+    a43g::SolveTrace tr;
+    tr.Xref = static_cast<double const*>(X_reference);
+    tr.every = std::max<int32_t>(1, every);
+    int const r = a43g::solve(plan->host, plan->dev, plan->solver, *opts, X, rho, stats ? stats : &local,
+                              (cudaStream_t)stream, nullptr, &tr);
+    int32_t const nrow = int32_t(tr.rows.size()/3);
+    int32_t const keep = std::min(nrow, std::max<int32_t>(0, capacity));
+    if (keep > 0) std::copy(tr.rows.begin(), tr.rows.begin() + 3*size_t(keep), trace);
+    if (count) *count = nrow;
     return r;
 }
 

@@ -52,6 +52,22 @@ struct KineticLists {
     uint32_t nlists() const { return start.empty() ? 0u : uint32_t(start.size() - 1); }
 };
 
+// the projection-sphere test of the dyadic plan for every candidate atom image (position, squared
+// projection radius and that radius plus the cube's circumscribing sphere) against every target
+// row: hits[c] receives the rows of candidate c in ascending order
+struct ImageRowsTask {
+    size_t ncand = 0;
+    double const *pos = nullptr;               // [ncand][3]
+    double const *r2p = nullptr, *r2p_plus = nullptr;   // [ncand]
+    uint32_t nRows = 0;
+    float const *rowCubePos = nullptr;         // [nRows][4]
+    double hg[3] = {0, 0, 0};
+};
+using ImageRowsFn = std::string (*)(ImageRowsTask const &task, std::vector<std::vector<uint32_t>> &hits);
+
+// the same test on the current CUDA device (plan_device.cu), bit-identical to the host loop
+std::string image_rows_on_device(ImageRowsTask const &task, std::vector<std::vector<uint32_t>> &hits);
+
 struct GreenPlan {
     Geometry geo;
     uint32_t n_blocks[3] = {0, 0, 0};
@@ -119,8 +135,9 @@ struct GreenPlan {
     size_t ncoeff_images() const { return AtomImageStarts.empty() ? 0 : AtomImageStarts.back(); }
     size_t ncoeff_atoms() const { return AtomStarts.empty() ? 0 : AtomStarts.back(); }
 
-    // returns an empty string on success, else an error message
-    std::string build(Geometry const &g);
+    // returns an empty string on success, else an error message; image_rows (optional) evaluates
+    // the atom-image x target-row test (default: the host loop)
+    std::string build(Geometry const &g, ImageRowsFn image_rows = nullptr);
     // potential on the full grid, natural order V[(iz*ng_y + iy)*ng_x + ix]
     std::string set_potential_grid(double const *V);
     // potential already in cell-cube layout [ncells][64]

@@ -60,7 +60,7 @@ void sho_prefactors(double *out, int numax, double sigma) {
                 out[i++] = f1(nx)*f1(ny)*f1(nz);
 }
 
-std::string GreenPlan::build(Geometry const &g) {
+std::string GreenPlan::build(Geometry const &g, ImageRowsFn image_rows) {
     geo = g;
     constexpr int X = 0, Y = 1, Z = 2;
     for (int d = 0; d < 3; ++d) {
@@ -149,6 +149,31 @@ std::string GreenPlan::build(Geometry const &g) {
     // ---- block sparsity: a target cube belongs to source i if any grid-point pair is closer
     //      than r_trunc, tested at 8 (far) or 27 (near) corner offsets (:580-694)
     double const r2trunc = sq(rtrunc), r2plus = sq(r_plus), r2circ = sq(rbcs*3);
+    // the test depends on the offset (bx, by, bz) from the source only: evaluated once per offset
+    // of the box [-itr, itr]^3 (the reference repeats it for every source)
+    uint32_t const nof[3] = {uint32_t(2*itr[X] + 1), uint32_t(2*itr[Y] + 1), uint32_t(2*itr[Z] + 1)};
+    std::vector<uint8_t> inside(size_t(nof[X])*nof[Y]*nof[Z], 0);
+    for (int32_t bz = -itr[Z]; bz <= itr[Z]; ++bz)
+    for (int32_t by = -itr[Y]; by <= itr[Y]; ++by)
+    for (int32_t bx = -itr[X]; bx <= itr[X]; ++bx) {
+        double const d2 = sq(bx*4*h_trunc[X]) + sq(by*4*h_trunc[Y]) + sq(bz*4*h_trunc[Z]);
+        int nin = 0;
+        if (d2 < r2plus) {
+            int const far = (d2 > r2circ);
+            int const step = 3 + 3*far;
+            for (int iz = -3; iz <= 3; iz += step) {
+                double const d2z = sq((bz*4 + iz)*h_trunc[Z]);
+                for (int iy = -3; iy <= 3; iy += step) {
+                    double const d2yz = sq((by*4 + iy)*h_trunc[Y]) + d2z;
+                    for (int ix = -3; ix <= 3; ix += step) {
+                        double const d2xyz = sq((bx*4 + ix)*h_trunc[X]) + d2yz;
+                        nin += (d2xyz < r2trunc);
+                    }
+                }
+            }
+        }
+        inside[flat3(nof, uint32_t(bx + itr[X]), uint32_t(by + itr[Y]), uint32_t(bz + itr[Z]))] = (nin > 0);
+    }
     std::vector<std::vector<uint16_t>> cols_of(nbox3);
     std::vector<std::vector<bool>> pattern(nrhs, std::vector<bool>(nbox3, false));
     std::vector<int32_t> diag_tag(nbox3, -1);
@@ -167,23 +192,7 @@ std::string GreenPlan::build(Geometry const &g) {
         for (int32_t bz = bfirst[Z]; bz <= blast[Z]; ++bz)
         for (int32_t by = bfirst[Y]; by <= blast[Y]; ++by)
         for (int32_t bx = bfirst[X]; bx <= blast[X]; ++bx) {
-            double const d2 = sq(bx*4*h_trunc[X]) + sq(by*4*h_trunc[Y]) + sq(bz*4*h_trunc[Z]);
-            int nin = 0;
-            if (d2 < r2plus) {
-                int const far = (d2 > r2circ);
-                int const step = 3 + 3*far;
-                for (int iz = -3; iz <= 3; iz += step) {
-                    double const d2z = sq((bz*4 + iz)*h_trunc[Z]);
-                    for (int iy = -3; iy <= 3; iy += step) {
-                        double const d2yz = sq((by*4 + iy)*h_trunc[Y]) + d2z;
-                        for (int ix = -3; ix <= 3; ix += step) {
-                            double const d2xyz = sq((bx*4 + ix)*h_trunc[X]) + d2yz;
-                            nin += (d2xyz < r2trunc);
-                        }
-                    }
-                }
-            }
-            if (nin > 0) {
+            if (inside[flat3(nof, uint32_t(bx + itr[X]), uint32_t(by + itr[Y]), uint32_t(bz + itr[Z]))]) {
                 uint32_t const ix = uint32_t(sc[X] + bx - tmin[X]);
                 uint32_t const iy = uint32_t(sc[Y] + by - tmin[Y]);
                 uint32_t const iz = uint32_t(sc[Z] + bz - tmin[Z]);
@@ -341,18 +350,16 @@ std::string GreenPlan::build(Geometry const &g) {
     }
     size_t const nAtomCopies = size_t(natoms)*ncopies;
 
+    // every atom copy in every periodic image, in the order of the reference's loops
     struct ImageInfo { double pos[3]; size_t iaa; int32_t ia; int8_t shift[3]; };
-    std::vector<ImageInfo> images;
-    std::vector<std::vector<uint32_t>> cubes;   // target rows hit by each contributing image
-    std::vector<bool> copy_contributes(nAtomCopies, false);
-    AtomImageStarts.assign(1, 0);
+    std::vector<ImageInfo> cand;
+    std::vector<double> cand_pos, cand_r2p, cand_r2p_plus;
     for (int zi = -nimg[Z]; zi <= nimg[Z]; ++zi)
     for (int yi = -nimg[Y]; yi <= nimg[Y]; ++yi)
     for (int xi = -nimg[X]; xi <= nimg[X]; ++xi) {
         int const ishift[3] = {xi, yi, zi};
         size_t iaa = 0;
         for (int32_t ia = 0; ia < natoms; ++ia) {
-            int const numax = int(g.xyzZinso[ia*8 + 5]);
             double const sigma = g.xyzZinso[ia*8 + 6];
             double const rp = r_proj*sigma;
             double const r2p = sq(rp), r2p_plus = sq(rp + rbcs);
@@ -360,32 +367,55 @@ std::string GreenPlan::build(Geometry const &g) {
             for (int yc = -ncpy[Y]; yc <= ncpy[Y]; ++yc)
             for (int xc = -ncpy[X]; xc <= ncpy[X]; ++xc, ++iaa) {
                 int const cshift[3] = {xc, yc, zc};
-                double pos[3];
-                for (int d = 0; d < 3; ++d) pos[d] = g.xyzZinso[ia*8 + d] + (ishift[d] + cshift[d])*cell[d];
-                std::vector<uint32_t> hit;
-                for (uint32_t ir = 0; ir < nRows; ++ir) {
-                    float const *tc = &rowCubePos[4*size_t(ir)];
-                    double dc2 = 0;
-                    for (int d = 0; d < 3; ++d) dc2 += sq((tc[d]*4.f + 2.0)*g.hg[d] - pos[d]);
-                    if (dc2 > r2p_plus) continue;
-                    double d2c[3][2];
-                    for (int d = 0; d < 3; ++d)
-                        for (int ii = 0; ii < 2; ++ii) d2c[d][ii] = sq((tc[d]*4.0 + ii*3 + 0.5)*g.hg[d] - pos[d]);
-                    int nin = 0;
-                    for (int i8 = 0; i8 < 8; ++i8)
-                        nin += (d2c[X][i8 & 1] + d2c[Y][(i8 & 2) >> 1] + d2c[Z][i8 >> 2] < r2p);
-                    if (nin > 0) hit.push_back(ir);
-                }
-                if (hit.empty()) continue;
-                copy_contributes[iaa] = true;
                 ImageInfo im;
-                for (int d = 0; d < 3; ++d) { im.pos[d] = pos[d]; im.shift[d] = int8_t(ishift[d]); }
+                for (int d = 0; d < 3; ++d) {
+                    im.pos[d] = g.xyzZinso[ia*8 + d] + (ishift[d] + cshift[d])*cell[d];
+                    im.shift[d] = int8_t(ishift[d]);
+                    cand_pos.push_back(im.pos[d]);
+                }
                 im.iaa = iaa; im.ia = ia;
-                images.push_back(im);
-                cubes.push_back(std::move(hit));
-                AtomImageStarts.push_back(AtomImageStarts.back() + uint32_t(nsho(numax)));
+                cand.push_back(im);
+                cand_r2p.push_back(r2p); cand_r2p_plus.push_back(r2p_plus);
             }
         }
+    }
+    // target rows whose cube has a corner point inside the projection sphere of each candidate
+    std::vector<std::vector<uint32_t>> hits(cand.size());
+    if (image_rows && !cand.empty() && nRows > 0) {
+        ImageRowsTask t;
+        t.ncand = cand.size(); t.pos = cand_pos.data(); t.r2p = cand_r2p.data(); t.r2p_plus = cand_r2p_plus.data();
+        t.nRows = nRows; t.rowCubePos = rowCubePos.data();
+        for (int d = 0; d < 3; ++d) t.hg[d] = g.hg[d];
+        std::string const e = image_rows(t, hits);
+        if (!e.empty()) return e;
+    } else {
+        for (size_t c = 0; c < cand.size(); ++c) {
+            double const *pos = &cand_pos[3*c];
+            for (uint32_t ir = 0; ir < nRows; ++ir) {
+                float const *tc = &rowCubePos[4*size_t(ir)];
+                double dc2 = 0;
+                for (int d = 0; d < 3; ++d) dc2 += sq((tc[d]*4.f + 2.0)*g.hg[d] - pos[d]);
+                if (dc2 > cand_r2p_plus[c]) continue;
+                double d2c[3][2];
+                for (int d = 0; d < 3; ++d)
+                    for (int ii = 0; ii < 2; ++ii) d2c[d][ii] = sq((tc[d]*4.0 + ii*3 + 0.5)*g.hg[d] - pos[d]);
+                int nin = 0;
+                for (int i8 = 0; i8 < 8; ++i8)
+                    nin += (d2c[X][i8 & 1] + d2c[Y][(i8 & 2) >> 1] + d2c[Z][i8 >> 2] < cand_r2p[c]);
+                if (nin > 0) hits[c].push_back(ir);
+            }
+        }
+    }
+    std::vector<ImageInfo> images;
+    std::vector<std::vector<uint32_t>> cubes;   // target rows hit by each contributing image
+    std::vector<bool> copy_contributes(nAtomCopies, false);
+    AtomImageStarts.assign(1, 0);
+    for (size_t c = 0; c < cand.size(); ++c) {
+        if (hits[c].empty()) continue;
+        copy_contributes[cand[c].iaa] = true;
+        images.push_back(cand[c]);
+        cubes.push_back(std::move(hits[c]));
+        AtomImageStarts.push_back(AtomImageStarts.back() + uint32_t(nsho(int(g.xyzZinso[cand[c].ia*8 + 5]))));
     }
     nAtomImages = uint32_t(images.size());
     uint32_t const nAI = nAtomImages;

@@ -60,6 +60,7 @@ namespace {
 constexpr int kBlk = 8192;
 constexpr int kCoef = 14;     // alpha, beta, the five complex K_DX coefficients
 constexpr int kSlots = 8;     // column sums per unit and column (at most 5 are used)
+constexpr int kRestarts = 3;  // FP64 continuation: restarts of sources whose true residual is above the tolerance
 
 struct ColState {
     double rho_re, rho_im;       // rho = rt^H w
@@ -725,9 +726,9 @@ __global__ void __launch_bounds__(256) k_U1(float *U1, float const *W, float con
 }
 
 // |B - AX|^2 per column of every source (final residuals; AX in FP64)
-__global__ void __launch_bounds__(256) k_final(double const *AX, Ctx const c) {
+__global__ void __launch_bounds__(256) k_final(double const *AX, Ctx const c, uint8_t const *sel) {
     uint32_t s, lo, hi;
-    if (!unit_range(c, nullptr, blockIdx.x, s, lo, hi)) return;
+    if (!unit_range(c, sel, blockIdx.x, s, lo, hi)) return;
     int const j = threadIdx.x & 63, q = threadIdx.x >> 6;
     uint32_t const diag = c.subset[s];
     double v[1] = {0};
@@ -762,6 +763,25 @@ __global__ void __launch_bounds__(256) k_start64(double *W, double *U1, double *
             W[b*kBlk + t] = r; U1[b*kBlk + t] = r;
             if (bad) X[b*kBlk + t] = 0.0;
         }
+    }
+}
+
+// sums[0] += |X64 + X32 - Xref|^2, sums[1] += |Xref|^2 over all blocks (X32 may be null)
+__global__ void __launch_bounds__(256) k_trace(double const *X64, float const *X32, double const *Xref, size_t n,
+                                               double *sums) {
+    double e = 0, r = 0;
+    for (size_t i = size_t(blockIdx.x)*blockDim.x + threadIdx.x; i < n; i += size_t(gridDim.x)*blockDim.x) {
+        double const x = X64[i] + (X32 ? double(X32[i]) : 0.0), y = Xref[i];
+        e += (x - y)*(x - y); r += y*y;
+    }
+    __shared__ double se[8], sr[8];
+    for (int o = 16; o > 0; o >>= 1) { e += __shfl_xor_sync(0xffffffffu, e, o); r += __shfl_xor_sync(0xffffffffu, r, o); }
+    if (0 == (threadIdx.x & 31)) { se[threadIdx.x >> 5] = e; sr[threadIdx.x >> 5] = r; }
+    __syncthreads();
+    if (0 == threadIdx.x) {
+        double a = 0, b = 0;
+        for (int w = 0; w < 8; ++w) { a += se[w]; b += sr[w]; }
+        atomicAdd(sums, a); atomicAdd(sums + 1, b);   // a diagnostic: the summation order may vary
     }
 }
 
@@ -889,7 +909,8 @@ struct Result { int iterations = 0; double applications = 0; };
 // phase has finished), retired before the first kernel
 template <typename T>
 bool run(DevicePlan &dp, SolverWorkspace &ws, TfqmrVectors &v, Prepared &p, T *X, int maxit, int check_every,
-         double *X64, double *AX64, cudaStream_t st, Result &res, int echo, std::vector<uint8_t> const &mask) {
+         double *X64, double *AX64, cudaStream_t st, Result &res, int echo, std::vector<uint8_t> const &mask,
+         SolveTrace *trace = nullptr) {
     Ctx const &c = p.c;
     uint32_t const nsrc = dp.nCols;
     bool const mixed = c.mixed != 0;
@@ -966,6 +987,7 @@ bool run(DevicePlan &dp, SolverWorkspace &ws, TfqmrVectors &v, Prepared &p, T *X
     struct GraphGuard { cudaGraphExec_t &e; ~GraphGuard() { if (e) cudaGraphExecDestroy(e); } } guard{exec};
     int it = 0;
     int const every = std::max(1, check_every);
+    int const tevery = trace ? std::max(1, trace->every) : 0;
     for (it = 1; it <= maxit; ++it) {
         if (exec) {
             A43G_CUDA_TRY(cudaGraphLaunch(exec, st));
@@ -974,10 +996,27 @@ bool run(DevicePlan &dp, SolverWorkspace &ws, TfqmrVectors &v, Prepared &p, T *X
             return false;
         }
         res.applications += 2;
-        if (0 == it % every || it == maxit) {
+        bool const sample = trace && (0 == (res.iterations + it) % tevery);
+        if (sample) {
+            // the current solution: X64 plus the FP32 correction of the recurrences
+            double const *x64 = X64 ? X64 : reinterpret_cast<double const*>(X);
+            float const *x32 = (sizeof(T) == 4) ? reinterpret_cast<float const*>(X) : nullptr;
+            A43G_CUDA_TRY(cudaMemsetAsync(ws.trace_sums.ptr, 0, 16, st));
+            k_trace<<<148*8, 256, 0, st>>>(x64, x32, trace->Xref, v.n, dptr<double>(ws.trace_sums));
+            count_launch();
+            A43G_CUDA_TRY(cudaMemcpyAsync(reinterpret_cast<char*>(ws.host_ctl) + 32, ws.trace_sums.ptr, 16,
+                                          cudaMemcpyDeviceToHost, st));
+        }
+        if (sample || 0 == it % every || it == maxit) {
             A43G_CUDA_TRY(cudaMemcpyAsync(ws.host_ctl, c.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, st));
             A43G_CUDA_TRY(cudaStreamSynchronize(st));
             Ctl const *h = reinterpret_cast<Ctl const*>(ws.host_ctl);
+            if (sample) {
+                double const *q = reinterpret_cast<double const*>(reinterpret_cast<char const*>(ws.host_ctl) + 32);
+                trace->rows.push_back(double(res.iterations + it));
+                trace->rows.push_back(q[1] > 0 ? std::sqrt(q[0]/q[1]) : 0.0);
+                trace->rows.push_back(double(h->n_active));
+            }
             if (echo > 1) {
                 std::printf("# tfqmr<%s> iteration %d: %d of %u sources active, %d breakdowns\n",
                             mixed ? "f32+f64" : "f64", it, h->n_active, nsrc, h->breakdowns);
@@ -1027,7 +1066,8 @@ size_t solve_bytes(DevicePlan const &dp, int precision) {
 }
 
 int solve(GreenPlan &hp, DevicePlan &dp, SolverWorkspace &ws, a43g_solve_options_t const &opt,
-          void *Xout, double *rho, a43g_solve_stats_t *stats, cudaStream_t st, SourceStats *per_source) {
+          void *Xout, double *rho, a43g_solve_stats_t *stats, cudaStream_t st, SourceStats *per_source,
+          SolveTrace *trace) {
     *stats = a43g_solve_stats_t{};
     if (0 == dp.nnzb) { stats->converged = 1; return A43G_OK; }
     if (!(opt.tolerance > 0) || opt.max_iterations < 1) { set_error("tolerance must be > 0 and max_iterations >= 1"); return A43G_ERR_ARGUMENT; }
@@ -1042,6 +1082,7 @@ int solve(GreenPlan &hp, DevicePlan &dp, SolverWorkspace &ws, a43g_solve_options
     std::vector<uint8_t> mask(nsrc, 0);
     std::fill(mask.begin(), mask.begin() + live, uint8_t(1));
     if (!ensure_vectors(ws, dp, mixed)) return A43G_ERR_MEMORY;
+    if (trace && (!trace->Xref || !ws.trace_sums.alloc(16))) return trace->Xref ? A43G_ERR_MEMORY : A43G_ERR_ARGUMENT;
     // projector scratch for both precisions before the iteration is captured (no allocation
     // may happen inside a stream capture)
     if (!ensure_dyadic_scratch(dp, 8) || !ensure_prj_part(dp, 8)) return A43G_ERR_MEMORY;
@@ -1061,7 +1102,7 @@ int solve(GreenPlan &hp, DevicePlan &dp, SolverWorkspace &ws, a43g_solve_options
         k_set_diag<float><<<nsrc, 64, 0, st>>>(dptr<float>(v.W), dptr<float>(v.U1), dptr<uint32_t>(dp.subset_dev), nsrc);
         count_launch();
         if (!run<float>(dp, ws, v, p, dptr<float>(v.X), opt.max_iterations, opt.check_every, X64,
-                        dptr<double>(ws.AX64), st, res, opt.echo, mask))
+                        dptr<double>(ws.AX64), st, res, opt.echo, mask, trace))
             return A43G_ERR_CUDA;
         // the rest of every column's FP32 correction into the FP64 solution
         k_flush<<<p.units, 256, 0, st>>>(X64, dptr<float>(v.X), p.c, nullptr);
@@ -1077,7 +1118,7 @@ int solve(GreenPlan &hp, DevicePlan &dp, SolverWorkspace &ws, a43g_solve_options
             it1[k] = ss1[k].done ? ss1[k].it : res.iterations;
             if (ss1[k].fallback) { fb[k] = 1; ++nfb; }
         }
-        int const left = opt.max_iterations - res.iterations;
+        int left = opt.max_iterations - res.iterations;
         if (nfb && left > 0) {
             // the FP32 set is done with: released first where both sets do not fit
             size_t freeb = 0, total = 0;
@@ -1093,22 +1134,52 @@ int solve(GreenPlan &hp, DevicePlan &dp, SolverWorkspace &ws, a43g_solve_options
             a43g_solve_options_t o2 = opt;
             if (!prepare(dp, ws, o2, false, true, p2)) return A43G_ERR_MEMORY;
             p2.c.abs_tol = 1;
-            // the QMR bound decides FP64 convergence; aiming at half the tolerance keeps the true
-            // residual, which the solve reports, below the tolerance
+            // the QMR bound decides when an FP64 run stops; aiming at half the tolerance leaves
+            // room for the gap between the bound and the true residual
             p2.c.tol = 0.5*opt.tolerance;
-            // R = B - A X64 of the continuing sources into W and U1; D = 0
-            if (!apply<double>(dp, dptr<double>(w.AU1), X64, nullptr, false, st)) return A43G_ERR_CUDA;
-            A43G_CUDA_TRY_RC(cudaMemsetAsync(w.D.ptr, 0, n*8, st));
-            A43G_CUDA_TRY_RC(cudaMemcpyAsync(dp.src_active.ptr, fb.data(), nsrc, cudaMemcpyHostToDevice, st));
-            k_start64<<<p2.units, 256, 0, st>>>(dptr<double>(w.W), dptr<double>(w.U1), X64, dptr<double>(w.AU1),
-                                               p2.c, dptr<uint8_t>(dp.src_active));
-            count_launch();
-            if (!run<double>(dp, ws, w, p2, X64, left, opt.check_every, nullptr, nullptr, st, res, opt.echo, fb))
-                return A43G_ERR_CUDA;
-            std::vector<SrcState> ss2(nsrc);
-            A43G_CUDA_TRY_RC(cudaMemcpyAsync(ss2.data(), p2.c.ss, nsrc*sizeof(SrcState), cudaMemcpyDeviceToHost, st));
-            A43G_CUDA_TRY_RC(cudaStreamSynchronize(st));
-            for (uint32_t k = 0; k < live; ++k) if (fb[k]) it1[k] += ss2[k].done ? ss2[k].it : left;
+            std::vector<uint8_t> cont = fb;
+            std::vector<ColState> cs2;
+            for (int restart = 0; ; ++restart) {
+                // A X64 of the continuing sources (their blocks only) into AU1
+                A43G_CUDA_TRY_RC(cudaMemcpyAsync(dp.src_active.ptr, cont.data(), nsrc, cudaMemcpyHostToDevice, st));
+                if (!apply<double>(dp, dptr<double>(w.AU1), X64, nullptr, true, st)) return A43G_ERR_CUDA;
+                res.applications += 1;
+                if (restart > 0) {
+                    // the true residual of each source the last run finished: sources still above
+                    // the tolerance (rounding in the recurrences can hold the true residual above
+                    // the bound) restart from their solution, at most kRestarts times
+                    k_final<<<p2.units, 256, 0, st>>>(dptr<double>(w.AU1), p2.c, dptr<uint8_t>(dp.src_active));
+                    count_launch();
+                    cs2.resize(size_t(nsrc)*64);
+                    A43G_CUDA_TRY_RC(cudaMemcpyAsync(cs2.data(), p2.c.cs, cs2.size()*sizeof(ColState),
+                                                     cudaMemcpyDeviceToHost, st));
+                    A43G_CUDA_TRY_RC(cudaStreamSynchronize(st));
+                    uint32_t again = 0;
+                    for (uint32_t k = 0; k < live; ++k) {
+                        if (!cont[k]) continue;
+                        double r = 0;
+                        for (int j = 0; j < 64; ++j) r = std::max(r, cs2[size_t(k)*64 + j].res);
+                        cont[k] = (std::isfinite(r) && r > opt.tolerance) ? 1 : 0;
+                        again += cont[k];
+                    }
+                    left = opt.max_iterations - res.iterations;
+                    if (0 == again || left <= 0 || restart > kRestarts) break;
+                    A43G_CUDA_TRY_RC(cudaMemcpyAsync(dp.src_active.ptr, cont.data(), nsrc, cudaMemcpyHostToDevice, st));
+                }
+                // R = B - A X64 of the continuing sources into W and U1; D = 0
+                A43G_CUDA_TRY_RC(cudaMemsetAsync(w.D.ptr, 0, n*8, st));
+                k_start64<<<p2.units, 256, 0, st>>>(dptr<double>(w.W), dptr<double>(w.U1), X64, dptr<double>(w.AU1),
+                                                   p2.c, dptr<uint8_t>(dp.src_active));
+                count_launch();
+                int const it0 = res.iterations;
+                if (!run<double>(dp, ws, w, p2, X64, left, opt.check_every, nullptr, nullptr, st, res, opt.echo, cont,
+                                 trace))
+                    return A43G_ERR_CUDA;
+                std::vector<SrcState> ss2(nsrc);
+                A43G_CUDA_TRY_RC(cudaMemcpyAsync(ss2.data(), p2.c.ss, nsrc*sizeof(SrcState), cudaMemcpyDeviceToHost, st));
+                A43G_CUDA_TRY_RC(cudaStreamSynchronize(st));
+                for (uint32_t k = 0; k < live; ++k) if (cont[k]) it1[k] += ss2[k].done ? ss2[k].it : res.iterations - it0;
+            }
         }
     } else {
         auto &v = ws.v64;
@@ -1116,8 +1187,21 @@ int solve(GreenPlan &hp, DevicePlan &dp, SolverWorkspace &ws, a43g_solve_options
         A43G_CUDA_TRY_RC(cudaMemsetAsync(X64, 0, n*8, st));
         k_set_diag<double><<<nsrc, 64, 0, st>>>(dptr<double>(v.W), dptr<double>(v.U1), dptr<uint32_t>(dp.subset_dev), nsrc);
         count_launch();
-        if (!run<double>(dp, ws, v, p, X64, opt.max_iterations, opt.check_every, nullptr, nullptr, st, res, opt.echo, mask))
+        if (!run<double>(dp, ws, v, p, X64, opt.max_iterations, opt.check_every, nullptr, nullptr, st, res, opt.echo,
+                         mask, trace))
             return A43G_ERR_CUDA;
+    }
+    if (trace) {
+        // the error of the final FP64 solution
+        A43G_CUDA_TRY_RC(cudaMemsetAsync(ws.trace_sums.ptr, 0, 16, st));
+        k_trace<<<148*8, 256, 0, st>>>(X64, nullptr, trace->Xref, n, dptr<double>(ws.trace_sums));
+        count_launch();
+        double q[2] = {0, 0};
+        A43G_CUDA_TRY_RC(cudaMemcpyAsync(q, ws.trace_sums.ptr, 16, cudaMemcpyDeviceToHost, st));
+        A43G_CUDA_TRY_RC(cudaStreamSynchronize(st));
+        trace->rows.push_back(double(res.iterations));
+        trace->rows.push_back(q[1] > 0 ? std::sqrt(q[0]/q[1]) : 0.0);
+        trace->rows.push_back(0.0);
     }
     // true residual of every column's FP64 solution (the whole operator, no source skipped), in
     // whichever FP64 scratch the solve holds
@@ -1125,7 +1209,7 @@ int solve(GreenPlan &hp, DevicePlan &dp, SolverWorkspace &ws, a43g_solve_options
     dp.retire = false;
     if (!launch_action<double>(dp, AXs, X64, dptr<uint16_t>(dp.colindx), st)) return A43G_ERR_CUDA;
     res.applications += 1;
-    k_final<<<p.units, 256, 0, st>>>(AXs, p.c);
+    k_final<<<p.units, 256, 0, st>>>(AXs, p.c, nullptr);
     count_launch();
     if (Xout) A43G_CUDA_TRY_RC(cudaMemcpyAsync(Xout, X64, n*8, cudaMemcpyDeviceToDevice, st));
     if (rho) {

@@ -22,6 +22,7 @@ struct SolverWorkspace {
     DeviceBuffer X64, AX64;          // FP64 solution, FP64 operator scratch of the FP32 recurrences
     DeviceBuffer state;              // per-column and per-source scalars, control block (solver.cu)
     DeviceBuffer part, tickets;      // fixed-order column reductions
+    DeviceBuffer trace_sums;         // |X - Xref|^2 and |Xref|^2 of a traced solve
     void *host_ctl = nullptr;        // pinned copy of the control block
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     ~SolverWorkspace();
@@ -32,6 +33,14 @@ struct SourceStats {
     uint32_t live_sources = 0;       // sources beyond this are padding of a batch, retired at the start
     std::vector<int> iterations, updates, fallback;
     std::vector<double> residual;
+};
+
+// error of the solution against a given FP64 solution, sampled while the solve runs (the
+// current solution: the FP64 solution plus the FP32 correction not yet added to it)
+struct SolveTrace {
+    double const *Xref = nullptr;    // device FP64 [nnzb][2][64][64]
+    int every = 10;                  // iterations between samples
+    std::vector<double> rows;        // per sample: iteration, |X - Xref| / |Xref|, active sources
 };
 
 // the batch plan and workspace of solve_batched, kept between calls
@@ -46,7 +55,8 @@ struct BatchCache {
 size_t solve_bytes(DevicePlan const &dp, int precision);
 
 int solve(GreenPlan &hp, DevicePlan &dp, SolverWorkspace &ws, a43g_solve_options_t const &opt,
-          void *X, double *rho, a43g_solve_stats_t *stats, cudaStream_t st, SourceStats *per_source = nullptr);
+          void *X, double *rho, a43g_solve_stats_t *stats, cudaStream_t st, SourceStats *per_source = nullptr,
+          SolveTrace *trace = nullptr);
 
 int solve_batched(GreenPlan &hp, DevicePlan &dp, BatchCache &bc, a43g_solve_options_t const &opt,
                   int32_t n, double const *energies, double const *kpoints, double dVol,

@@ -79,6 +79,23 @@ def solve(plan, X=None, want_rho=True, stream=0, **kw):
     return stats.as_dict(), (rho[..., 0] + 1j * rho[..., 1] if want_rho else None)
 
 
+def solve_traced(plan, X_reference, every=10, X=None, want_rho=False, stream=0, capacity=100000, **kw):
+    """solve() recording every `every` iterations the relative error of the current solution
+    against X_reference (CUDA float64 tensor [nnzb, 2, 64, 64]).  Returns (stats, rho, trace) with
+    trace a float64 array of rows [iteration, |X - X_reference| / |X_reference|, active sources]."""
+    opts = solve_options(**kw)
+    stats = _lib.SolveStats()
+    rho = np.zeros((plan.nCols, 64, 2)) if want_rho else None
+    tr = np.zeros((capacity, 3))
+    count = ctypes.c_int32(0)
+    st = ctypes.c_void_p(stream if isinstance(stream, int) else stream.cuda_stream)
+    check(_lib.lib().a43g_solve_traced(plan.handle, ctypes.byref(opts), ptr(X), ptr(rho), ctypes.byref(stats), st,
+                                       ptr(X_reference), int(every), ptr(tr), int(capacity), ctypes.byref(count)),
+          "a43g_solve_traced")
+    return (stats.as_dict(), (rho[..., 0] + 1j * rho[..., 1] if want_rho else None),
+            tr[:min(count.value, capacity)].copy())
+
+
 def solve_batched(plan, energies, kpoints, dVol, want_rho=False, stream=0, **kw):
     """Solves for every (energy, k-point) pair on the plan's geometry."""
     E = np.ascontiguousarray(np.stack([np.real(energies), np.imag(energies)], axis=-1), dtype=np.float64)

@@ -16,7 +16,7 @@ Isolated_Boundary, Periodic_Boundary, Vacuum_Boundary, Repeat_Boundary = 0, 1, 2
 class ActionPlan:
     """Owns an a43g plan handle (the counterpart of action_plan_t, include/action_plan.hxx:32-114)."""
 
-    def __init__(self, geometry):
+    def __init__(self, geometry, on_device=False):
         g = _lib.Geometry()
         for d in range(3):
             g.ng[d] = int(geometry.ng[d]); g.bc[d] = int(geometry.bc[d]); g.hg[d] = float(geometry.hg[d])
@@ -26,7 +26,10 @@ class ActionPlan:
         g.natoms = len(self._xyz) // 8
         g.xyzZinso = self._xyz.ctypes.data if g.natoms else None
         h = ctypes.c_void_p()
-        check(_lib.lib().a43g_plan_build(ctypes.byref(g), ctypes.byref(h)), "a43g_plan_build")
+        if on_device:
+            check(_lib.lib().a43g_plan_build_device(ctypes.byref(g), ctypes.byref(h)), "a43g_plan_build_device")
+        else:
+            check(_lib.lib().a43g_plan_build(ctypes.byref(g), ctypes.byref(h)), "a43g_plan_build")
         self.handle = h
         s = _lib.PlanSizes()
         check(_lib.lib().a43g_plan_get_sizes(self.handle, ctypes.byref(s)), "a43g_plan_get_sizes")
@@ -103,9 +106,10 @@ class ActionPlan:
         check(_lib.lib().a43g_plan_upload(self.handle), "a43g_plan_upload")
 
 
-def construct_Green_function(geometry):
-    """Build the plan (src/green_function.cxx:357-1068)."""
-    return ActionPlan(geometry)
+def construct_Green_function(geometry, on_device=False):
+    """Build the plan (src/green_function.cxx:357-1068); on_device: the atom-image x target-row
+    test of the dyadic plan on the current CUDA device (same arrays)."""
+    return ActionPlan(geometry, on_device)
 
 
 def update_potential(plan, V, atom_matrices=None, atom_offsets=None, layout="grid"):

@@ -72,6 +72,16 @@ def parse():
     ap.add_argument("--full-contour", action="store_true", help="solve all pairs (mixed+batched and plain FP64)")
     ap.add_argument("--convergence-scan", action="store_true",
                     help="FP64 iterations over the contour energies and the residual history at -0.2+0.02i")
+    ap.add_argument("--profile-case", choices=["action", "solve"], default=None,
+                    help="small case for ncu captures on the one-source 16^3 cell (4096 blocks, 134 MB per FP32 "
+                         "vector): 'action' applies the FP32 action with the CUDA-core and the tensor-core "
+                         "projector and the FP64 action, 4 times each; 'solve' runs 40 iterations of the mixed "
+                         "and of the FP64 solver")
+    ap.add_argument("--wrapped32", action="store_true",
+                    help="the wrapped 32^3-cube cell (256 atoms, 32 source cubes, 300,960 blocks) at "
+                         "E = -0.2 + 0.02i to 1e-10: plain FP64 solve, then the mixed solve with the error of "
+                         "G against it every 10 iterations")
+    ap.add_argument("--wrapped32-iterations", type=int, default=2000, help="iteration limit of --wrapped32")
     ap.add_argument("--nk", type=int, default=4, help="k-points of the contour")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
@@ -590,6 +600,86 @@ def convergence_scan(a):
                                "history_E": [-0.2, 0.02], "history": hist}})
 
 
+def profile_case(a):
+    """The small case of the ncu captures: the one-source version of the benchmark cell at
+    E = -0.2 + 0.02i (Gamma), above L2 per vector, a few launches of every kernel of the path."""
+    import torch
+    from angstromcube_b200 import _lib, green_action, green_function as gf, workloads
+    torch.cuda.set_device(0)
+    w = workloads.make("periodic16_64atoms_s1x1x1")
+    stream = torch.cuda.Stream()
+
+    def plan_for(projector):
+        os.environ["A43G_PROJECTOR"] = projector
+        p = gf.construct_Green_function(w.geometry)
+        gf.update_potential(p, w.Vcell, w.mats, w.offsets, layout="cells")
+        gf.update_energy_parameter(p, complex(-0.2, 0.02), w.dVol)
+        return p
+
+    if a.profile_case == "action":
+        g = torch.Generator(device="cuda").manual_seed(5)
+        for projector in ("simt", "tc"):
+            p = plan_for(projector)
+            x = torch.randn((p.nnzb, 2, 64, 64), device="cuda", dtype=torch.float32, generator=g)
+            y = torch.empty_like(x)
+            t0 = time_part(_lib, p, 0, _lib.A43G_F32, x, y, 4, stream)
+            t1 = time_part(_lib, p, 1, _lib.A43G_F32, x, y, 4, stream)
+            emit({"case": "action", "precision": "float32", "projector": projector, "local_ms": t0 * 1e3,
+                  "projector_ms": t1 * 1e3})
+        x = x.double()
+        y = torch.empty_like(x)
+        t0 = time_part(_lib, p, 0, _lib.A43G_F64, x, y, 4, stream)
+        t1 = time_part(_lib, p, 1, _lib.A43G_F64, x, y, 4, stream)
+        emit({"case": "action", "precision": "float64", "local_ms": t0 * 1e3, "projector_ms": t1 * 1e3})
+    else:
+        p = plan_for("simt")
+        for precision in ("float32", "float64"):
+            st, _ = green_action.solve(p, stream=stream, want_rho=False, precision=precision, tolerance=1e-8,
+                                       max_iterations=40, check_every=10)
+            emit({"case": "solve", "precision": precision, "iterations": st["iterations"],
+                  "residual": st["residual_max"], "seconds": st["seconds"]})
+
+
+def wrapped32(a):
+    """Mixed precision on the large cell: the wrapped 32^3-cube cell (128^3 points, h = 0.25 Bohr)
+    with 256 atoms on a jittered 8x8x4 lattice (numax 5, sigma 0.6), 32 source cubes (2048
+    columns), truncation radius 12 Bohr, E = -0.2 + 0.02i, tolerance 1e-10.  First the plain FP64
+    solve (no retirement, the reference's algorithm), whose solution is kept on the device, then
+    the mixed solve traced against it: the relative error of G every 10 iterations (the
+    residual-replacement gap) and at the end.  One FP64 block vector is 19.7 GB; the FP64 solve
+    holds 8 of them and the FP64 solution of the mixed solve's continuation 8 plus the reference."""
+    import torch
+    from angstromcube_b200 import green_action, green_function as gf, workloads
+    torch.cuda.set_device(0)
+    t0 = time.perf_counter()
+    w = workloads.make("wrapped32_256atoms")
+    t1 = time.perf_counter()
+    plan = gf.construct_Green_function(w.geometry)
+    t2 = time.perf_counter()
+    gf.update_potential(plan, w.Vcell, w.mats, w.offsets, layout="cells")
+    gf.update_energy_parameter(plan, w.E, w.dVol)
+    plan.upload()
+    stream = torch.cuda.Stream()
+    tune = green_action.autotune(plan, "float32", stream)
+    out = {"cell": "wrapped32_256atoms", "nnzb": plan.nnzb, "columns": 64 * plan.nCols,
+           "atoms": plan.sizes["nAtoms"], "atom_images": plan.sizes["nAtomImages"], "E": [w.E.real, w.E.imag],
+           "tolerance": 1e-10, "max_iterations": a.wrapped32_iterations,
+           "seconds_inputs": t1 - t0, "seconds_host_plan": t2 - t1, "autotune": tune.strip().splitlines()[-1:]}
+    emit({"setup": out})
+    Xref = torch.empty((plan.nnzb, 2, 64, 64), device="cuda", dtype=torch.float64)
+    st, _ = green_action.solve(plan, X=Xref, stream=stream, want_rho=False, precision="float64", tolerance=1e-10,
+                               max_iterations=a.wrapped32_iterations, check_every=10, retire=False)
+    out["fp64"] = {k: st[k] for k in ("iterations", "converged", "residual_max", "residual_estimate", "seconds")}
+    emit({"fp64": out["fp64"]})
+    st3, _, tr = green_action.solve_traced(plan, Xref, every=10, stream=stream, precision="float32",
+                                           tolerance=1e-10, max_iterations=a.wrapped32_iterations, check_every=10)
+    out["mixed"] = {k: st3[k] for k in ("iterations", "converged", "residual_max", "residual_estimate", "seconds",
+                                       "fp64_sources", "refinements")}
+    out["mixed"]["error_of_G"] = [[int(r[0]), float(r[1]), int(r[2])] for r in tr]
+    out["speedup_mixed_vs_fp64"] = st["seconds"] / max(st3["seconds"], 1e-12)
+    emit({"wrapped32": out})
+
+
 def launch_ranks(a):
     """--gpus N without a launcher: start N ranks with torch.distributed.run (one process per GPU,
     NCCL over 127.0.0.1) and return its exit code."""
@@ -614,6 +704,12 @@ def main():
         return
     if a.convergence_scan:
         convergence_scan(a)
+        return
+    if a.profile_case:
+        profile_case(a)
+        return
+    if a.wrapped32:
+        wrapped32(a)
         return
     plan, w, pairs, stream, opts, out, hbm, bf16, peak_kind, world, rank, records = our_arm(a)
     if rank == 0:

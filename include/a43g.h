@@ -113,6 +113,10 @@ const char *a43g_version(void);
 
 /* ---- plan: replaces construct_Green_function + action_plan_t (src/green_function.cxx:357-1068) */
 int a43g_plan_build(const a43g_geometry_t *geometry, a43g_plan_t **plan);
+/* the same plan, with the atom-image x target-row overlap test of the dyadic plan
+ * (src/dyadic_plan.cxx:264-401, a serial loop in the reference) evaluated on the current CUDA
+ * device; every array is identical to a43g_plan_build's */
+int a43g_plan_build_device(const a43g_geometry_t *geometry, a43g_plan_t **plan);
 int a43g_plan_destroy(a43g_plan_t *plan);
 int a43g_plan_get_sizes(const a43g_plan_t *plan, a43g_plan_sizes_t *sizes);
 int a43g_plan_export(const a43g_plan_t *plan, const a43g_plan_export_t *out);
@@ -191,11 +195,21 @@ uint64_t a43g_kernel_launches(void);
 
 /* ---- tfQMR solve of (H - E S) X = B with B the unit blocks on the diagonal (plan subset);
  * replaces tfqmrgpu::solve + action_t::solve (include/green_action.hxx:181-241).
- * X: optional device pointer real_t[nnzb][2][64][64] (precision of the options) receiving the
- * solution; rho: optional host array complex double [nCols][64][2] receiving the diagonal
+ * X: optional device pointer double[nnzb][2][64][64] receiving the FP64 solution (in both
+ * precisions); rho: optional host array complex double [nCols][64][2] receiving the diagonal
  * of the diagonal blocks divided by pi, as action_t::solve exports it. */
 int a43g_solve(a43g_plan_t *plan, const a43g_solve_options_t *opts, void *X, double *rho,
                a43g_solve_stats_t *stats, void *stream);
+
+/* the same solve, recording every `every` iterations the relative error |X - X_reference| /
+ * |X_reference| (Frobenius norms over all blocks) of the current solution (with FP32
+ * recurrences: the FP64 solution plus the FP32 correction not yet added to it) against the
+ * device FP64 block vector X_reference, for example the plain FP64 solution.  trace receives up
+ * to `capacity` rows [iteration, relative error, sources still active], the last row the error
+ * of the final solution (0 active sources); *count the number of rows recorded.  No reference counterpart (a diagnostic of the mixed-precision solver). */
+int a43g_solve_traced(a43g_plan_t *plan, const a43g_solve_options_t *opts, void *X, double *rho,
+                      a43g_solve_stats_t *stats, void *stream, const void *X_reference, int32_t every,
+                      double *trace, int32_t capacity, int32_t *count);
 
 /* ---- batched solve over (energy, k-point) pairs on one plan geometry: energies[n][2],
  * kpoints[n][3]; rho (optional) host [n][nCols][64][2]; stats[n].  No reference counterpart as

@@ -35,7 +35,7 @@ def test_density_matrices_match_reference(name):
 
 
 def test_density_matrices_refuse_periodic_images():
-    g = GEOMETRIES["wrap8"]()
+    g = GEOMETRIES["peri_xy_wrap_z"]()
     Vc, mats, offs, E, k, dVol, na = inputs_for(g)
     p = product_plan(g, Vc, mats, offs, E, k, dVol)
     assert p.sizes["nAtomImages"] > p.sizes["nAtoms"]

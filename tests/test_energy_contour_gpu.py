@@ -28,3 +28,39 @@ def test_integrate_matches_individual_solves():
             total = total + we * wk * r
     assert np.abs(rho - total.real).max() <= 1e-8 * np.abs(total.real).max()
     assert np.all(np.isfinite(resp))
+
+
+def test_integrate_matches_reference_cpu_solves():
+    """The contour density with the GPU solver against the same contour with every (E, k) point
+    solved by the reference's own CPU action (oracle/_ref) driven by the numpy tfQMR restatement:
+    two atoms in a periodic 4^3 cell, truncation radius 3 Bohr, four energy points at one k-point
+    (each reference solve takes seconds: the reference's CPU action on 64 blocks is ~80 ms)."""
+    import oracle
+    from oracle import tfqmr
+    from helpers import geometry, inputs_for, product_plan, reference_plan
+    if not oracle.ref_available():
+        pytest.skip("oracle/_ref not built")
+    g = geometry((4, 4, 4), (1, 1, 1), 3.0, (1, 1, 1), 4, 2, seed=17, sigma=0.5, numax=3)
+    Vc, mats, offs, E0, k0, dVol, na = inputs_for(g, seed=23)
+    E, W = ec.get_energy_mesh(5e-2, -1.0, 1, 1, 1, 1)
+    ks = [np.array([0.2, -0.1, 0.3])]
+    kw = [1.0]
+
+    def ref_solve(e, k):
+        r = reference_plan(g, Vc, mats, offs, e, k, dVol)
+        ex = r.export()
+        X, info = tfqmr.solve_blocks_torch(lambda z: torch.from_numpy(r.action(z.cpu().numpy())).to(z.device),
+                                           ex["subset"], ex["colindx"], r.sizes["nnzb"], r.sizes["nCols"],
+                                           tol=1e-11, maxiter=3000)
+        assert info["converged"], (e, k, info)
+        X = X.cpu().numpy()
+        d = X[ex["subset"]][:, :, np.arange(64), np.arange(64)] / np.pi      # [nCols, 2, 64]
+        return d[:, 0] + 1j * d[:, 1]
+
+    rho_ref, resp_ref, _ = ec.integrate(None, E, W, ks, kw, dVol, fermi_level=-0.1, solve=ref_solve)
+    p = product_plan(g, Vc, mats, offs, E0, k0, dVol)
+    rho, resp, stats = ec.integrate(p, E, W, ks, kw, dVol, fermi_level=-0.1, tolerance=1e-11, max_iterations=3000,
+                                    precision="float64", check_every=5)
+    assert all(s["converged"] for s in stats), stats
+    assert np.abs(rho - rho_ref).max() <= 1e-8 * np.abs(rho_ref).max()
+    assert np.abs(resp - resp_ref).max() <= 1e-8 * max(np.abs(resp_ref).max(), 1e-300)

@@ -231,3 +231,28 @@ def test_slow_convergence_at_the_single_energy_is_the_algorithms():
     X, info = tfqmr.solve_blocks_torch(action, a["subset"], a["colindx"], p.nnzb, p.nCols, tol=1e-8, maxiter=400)
     r = true_residual(X)
     assert not info["converged"] and 1e-3 < r < 1.0, (r, info)
+
+
+def test_solve_traced_error_of_G():
+    """a43g_solve_traced: against the plain FP64 solution, the FP64 solve's own trace ends at
+    exactly zero (the solver is deterministic) and the mixed solve's error of G falls to the
+    level of the tolerance."""
+    w = workloads.make("periodic4_1atom")
+    p = gf.construct_Green_function(w.geometry)
+    gf.update_potential(p, w.Vcell, w.mats, w.offsets, layout="cells")
+    gf.update_energy_parameter(p, complex(-0.3, 0.1), w.dVol)
+    stream = torch.cuda.Stream()
+    Xref = torch.zeros((p.nnzb, 2, 64, 64), device="cuda", dtype=torch.float64)
+    st, _ = green_action.solve(p, X=Xref, stream=stream, want_rho=False, precision="float64", tolerance=1e-11,
+                               max_iterations=2000, check_every=1)
+    assert st["converged"]
+    st2, _, tr = green_action.solve_traced(p, Xref, every=1, stream=stream, precision="float64", tolerance=1e-11,
+                                           max_iterations=2000, check_every=1)
+    # one row per iteration and the final row
+    assert st2["iterations"] == st["iterations"] and len(tr) == st["iterations"] + 1
+    assert np.array_equal(tr[:-1, 0], np.arange(1, len(tr))) and tr[-1, 0] == st["iterations"]
+    assert tr[-2, 1] == 0.0 and tr[-1, 1] == 0.0 and tr[-1, 2] == 0
+    st3, _, tr3 = green_action.solve_traced(p, Xref, every=5, stream=stream, precision="float32", tolerance=1e-10,
+                                            max_iterations=2000)
+    assert st3["converged"] and len(tr3) >= 2
+    assert np.all(np.diff(tr3[:-1, 0]) == 5) and tr3[0, 1] > 1e-3 and tr3[-1, 1] < 1e-6
