@@ -596,6 +596,201 @@ local_pencil_kernel(float *__restrict__ y, float const *__restrict__ x,
     }
 }
 
+// Pencil variant in FP64: the pencil kernel's mapping with the two planes on two threads.  One
+// CTA of 128 threads per (z-line, slice of 16 columns); thread (zq, plane, j) owns one plane (re
+// or im) of the four y-rows (zq, y = 0..3) of every cube of the line for column j, so a warp is
+// one z-plane: 16 consecutive columns of the real plane and the same columns of the imaginary
+// plane (two 128-byte segments per load).  The only couplings of the planes, -i Im(E) x and the
+// Bloch phases of halo cubes, take the partner plane's values by a warp shuffle (lane ^ 16).
+// Registers hold the same number of values as the FP32 kernel's, at twice the bytes.
+constexpr int kPencil64S = 16;
+constexpr int kPencil64Smem = 3*2*16*kPencil64S*32;   // bytes of the three z-slots (double4 rows)
+
+struct Quad64 { double v[16]; };                     // one plane of [y*4 + x] of one z-plane of a cube
+
+__device__ __forceinline__ void quad64_raw(double const *__restrict__ x, int32_t e, int zq, int pl, int col, Quad64 &q) {
+    if (-1 == e) {
+#pragma unroll
+        for (int i = 0; i < 16; ++i) q.v[i] = 0.0;
+        return;
+    }
+    double const *b = x + size_t(nbr_block(e))*kBlockReals + pl*4096 + (zq*16)*64 + col;
+#pragma unroll
+    for (int i = 0; i < 16; ++i) q.v[i] = __ldg(b + i*64);
+}
+
+// rotation by the Bloch phase (pr, pi) of a halo cube, uniform over the CTA: re' = pr re - pi im,
+// im' = pr im + pi re, with the other plane from the partner lane
+__device__ __forceinline__ double phase64(double v, int pl, double pr, double pi) {
+    double const w = __shfl_xor_sync(0xffffffffu, v, 16);
+    return pr*v + (pl ? pi : -pi)*w;
+}
+
+__global__ void __launch_bounds__(8*kPencil64S, 3)
+local_pencil64_kernel(double *__restrict__ y, double const *__restrict__ x,
+                      uint32_t const *__restrict__ zstart, int32_t const *__restrict__ zlist,
+                      int32_t const *__restrict__ nbr, int32_t const *__restrict__ veff,
+                      double const *__restrict__ Vcell, LocalArgs<double> a)
+{
+    constexpr int S = kPencil64S, NSL = 64/S;
+    extern __shared__ __align__(16) double4 slot64[];  // [3][2][16][S]
+    __shared__ int32_t code[kMaxLine][8];              // per step: block, x-, x+, y-, y+, veff, z-next
+    __shared__ int32_t zleft, nline;
+    int const line = blockIdx.x/NSL, slice = blockIdx.x % NSL;
+    int const tid = threadIdx.x, lane = tid & 31, zq = tid >> 5;
+    int const pl = lane >> 4, j = lane & 15, col = slice*S + j;
+    int32_t const *L = zlist + zstart[line];
+    if (0 == tid) {
+        int n = 0;
+        while (L[4 + n] > 0) ++n;                   // lists end with 4 non-positive entries
+        nline = n; zleft = list_code(L[3]);
+    }
+    __syncthreads();
+    int const n = nline;
+    if (0 == n || !line_args(a, L[4] - 1)) return;  // uniform: nothing on this line, or retired
+    for (int k = tid; k < n; k += 8*S) {
+        int32_t const b = L[4 + k] - 1;
+        int32_t const *nb = nbr + 6*size_t(b);
+        code[k][0] = b; code[k][1] = nb[0]; code[k][2] = nb[1]; code[k][3] = nb[2]; code[k][4] = nb[3];
+        code[k][5] = veff[b]; code[k][6] = list_code(L[5 + k]);
+    }
+    auto srow = [&](int slot, int plane, int row) -> double4 & { return slot64[((slot*2 + plane)*16 + row)*S + j]; };
+    auto put = [&](int slot, Quad64 const &q) {
+#pragma unroll
+        for (int yy = 0; yy < 4; ++yy)
+            srow(slot, pl, zq*4 + yy) = make_double4(q.v[yy*4], q.v[yy*4 + 1], q.v[yy*4 + 2], q.v[yy*4 + 3]);
+    };
+    auto qphase = [&](int32_t e, double pr, double pi, Quad64 &q) {
+        if (e < -1) {
+#pragma unroll
+            for (int i = 0; i < 16; ++i) q.v[i] = phase64(q.v[i], pl, pr, pi);
+        }
+    };
+    double const (&cx)[5] = a.st.c[0];
+    double const (&cy)[5] = a.st.c[1];
+    double const (&cz)[5] = a.st.c[2];
+    double const c0 = cx[0] + cy[0] + cz[0];
+    double const Eim = pl ? -a.E_im : a.E_im;       // re: + Im(E) im, im: - Im(E) re
+    __syncthreads();                                // code[] complete
+    {
+        Quad64 h;
+        quad64_raw(x, zleft, zq, pl, col, h);
+        qphase(zleft, a.ph[2][0][0], a.ph[2][0][1], h);
+        put(0, h);
+        quad64_raw(x, code[0][0], zq, pl, col, h);
+        put(1, h);
+    }
+    Quad64 nx;                                      // rows of the z-successor, one step ahead
+    quad64_raw(x, code[0][6], zq, pl, col, nx);
+    int sp = 0, sc = 1, sn = 2;
+    for (int k = 0; k < n; ++k) {
+        int32_t const b = code[k][0];
+        qphase(code[k][6], a.ph[2][1][0], a.ph[2][1][1], nx);       // only the line end has a phase
+        __syncthreads();                            // the previous step finished reading slot sn
+        put(sn, nx);
+        __syncthreads();
+        if (k + 1 < n) quad64_raw(x, code[k + 1][6], zq, pl, col, nx);   // arrives during this step
+        double cur[16];
+#pragma unroll
+        for (int yy = 0; yy < 4; ++yy) {
+            double4 const v = srow(sc, pl, zq*4 + yy);
+            cur[yy*4] = v.x; cur[yy*4 + 1] = v.y; cur[yy*4 + 2] = v.z; cur[yy*4 + 3] = v.w;
+        }
+        double acc[16];
+        // potential and centre; the other plane of the own points from the partner lane
+        int32_t const iloc = code[k][5];
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+            double const V = (iloc < 0) ? 0.0 : __ldg(Vcell + size_t(iloc)*64 + zq*16 + i);
+            double const w = __shfl_xor_sync(0xffffffffu, cur[i], 16);
+            acc[i] = (V - a.E_re)*cur[i] + Eim*w + c0*cur[i];
+        }
+        // y-stencil inside the cube
+#pragma unroll
+        for (int yy = 0; yy < 4; ++yy)
+#pragma unroll
+            for (int yo = 0; yo < 4; ++yo) {
+                if (yo == yy) continue;
+                int const d = (yo > yy) ? yo - yy : yy - yo;
+#pragma unroll
+                for (int i = 0; i < 4; ++i) acc[yy*4 + i] += cy[d]*cur[yo*4 + i];
+            }
+        // x-stencil: the rows of the x-neighbours at (zq, yy)
+        int32_t const exm = code[k][1], exp_ = code[k][2], eym = code[k][3], eyp = code[k][4];
+#pragma unroll
+        for (int yy = 0; yy < 4; ++yy) {
+            double xm[4], xp[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                xm[i] = (-1 == exm) ? 0.0 : __ldg(x + size_t(nbr_block(exm))*kBlockReals + pl*4096 + (zq*16 + yy*4 + i)*64 + col);
+                xp[i] = (-1 == exp_) ? 0.0 : __ldg(x + size_t(nbr_block(exp_))*kBlockReals + pl*4096 + (zq*16 + yy*4 + i)*64 + col);
+            }
+            if (exm < -1) {
+#pragma unroll
+                for (int i = 0; i < 4; ++i) xm[i] = phase64(xm[i], pl, a.ph[0][0][0], a.ph[0][0][1]);
+            }
+            if (exp_ < -1) {
+#pragma unroll
+                for (int i = 0; i < 4; ++i) xp[i] = phase64(xp[i], pl, a.ph[0][1][0], a.ph[0][1][1]);
+            }
+            double l[12];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) { l[i] = xm[i]; l[4 + i] = cur[yy*4 + i]; l[8 + i] = xp[i]; }
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int d = 1; d <= 4; ++d) acc[yy*4 + i] += cx[d]*(l[4 + i - d] + l[4 + i + d]);
+        }
+        // y-neighbour cubes: row yo of y- sits at y = yo - 4, row yo of y+ at y = yo + 4
+#pragma unroll
+        for (int yo = 0; yo < 4; ++yo) {
+            double ym[4], yp[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                ym[i] = (-1 == eym) ? 0.0 : __ldg(x + size_t(nbr_block(eym))*kBlockReals + pl*4096 + (zq*16 + yo*4 + i)*64 + col);
+                yp[i] = (-1 == eyp) ? 0.0 : __ldg(x + size_t(nbr_block(eyp))*kBlockReals + pl*4096 + (zq*16 + yo*4 + i)*64 + col);
+            }
+            if (eym < -1) {
+#pragma unroll
+                for (int i = 0; i < 4; ++i) ym[i] = phase64(ym[i], pl, a.ph[1][0][0], a.ph[1][0][1]);
+            }
+            if (eyp < -1) {
+#pragma unroll
+                for (int i = 0; i < 4; ++i) yp[i] = phase64(yp[i], pl, a.ph[1][1][0], a.ph[1][1][1]);
+            }
+#pragma unroll
+            for (int yy = 0; yy < 4; ++yy) {
+                if (yy <= yo) {
+#pragma unroll
+                    for (int i = 0; i < 4; ++i) acc[yy*4 + i] += cy[yy - yo + 4]*ym[i];
+                }
+                if (yy >= yo) {
+#pragma unroll
+                    for (int i = 0; i < 4; ++i) acc[yy*4 + i] += cy[yo + 4 - yy]*yp[i];
+                }
+            }
+        }
+        // z-stencil from the three staged cubes (previous, current, next)
+#pragma unroll
+        for (int yy = 0; yy < 4; ++yy)
+#pragma unroll
+            for (int d = 1; d <= 4; ++d) {
+                int const zm = zq - d, zp = zq + d;
+                int const s_m = (zm < 0) ? sp : sc, s_p = (zp > 3) ? sn : sc;
+                int const r_m = (zm & 3)*4 + yy, r_p = (zp & 3)*4 + yy;
+                double4 const m = srow(s_m, pl, r_m), p = srow(s_p, pl, r_p);
+                acc[yy*4 + 0] += cz[d]*(m.x + p.x);
+                acc[yy*4 + 1] += cz[d]*(m.y + p.y);
+                acc[yy*4 + 2] += cz[d]*(m.z + p.z);
+                acc[yy*4 + 3] += cz[d]*(m.w + p.w);
+            }
+        double *yb = y + size_t(b)*kBlockReals + pl*4096 + (zq*16)*64 + col;
+#pragma unroll
+        for (int i = 0; i < 16; ++i) yb[i*64] = acc[i];
+        int const t = sp; sp = sc; sc = sn; sn = t;  // rotate the z-slots
+    }
+}
+
 // Pencils with staged lateral cubes (FP32): the thread mapping and arithmetic of
 // local_pencil_kernel, but the four x- and y-neighbour cubes of step k + 1 are copied into shared
 // memory with 16-byte cp.async while step k is computed, so the stencil reads only shared memory
@@ -1196,6 +1391,7 @@ bool prepare_local_kernels() {
     // the pencil kernel's three z-slots are 48 KB of dynamic shared memory beside its static part
     A43G_CUDA_TRY(cudaFuncSetAttribute(local_pencil_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kPencilSmem));
     A43G_CUDA_TRY(cudaFuncSetAttribute(local_stage_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kStageSmem));
+    A43G_CUDA_TRY(cudaFuncSetAttribute(local_pencil64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kPencil64Smem));
     return true;
 }
 
@@ -1234,6 +1430,16 @@ bool launch_local(DevicePlan &dp, T *y, T const *x, cudaStream_t st) {
             }
             if (dp.nlists[2] && dp.max_zline <= kMaxLine && (2 == dp.local_variant || 3 == dp.local_variant)) {
                 local_pencil_kernel<<<dp.nlists[2]*(64/kPencilS), 4*kPencilS, kPencilSmem, st>>>(y, x,
+                    dptr<uint32_t>(dp.lists_start[2]), dptr<int32_t>(dp.lists[2]), dptr<int32_t>(dp.nbr),
+                    dptr<int32_t>(dp.veff_index), vcell<T>(dp), a);
+                count_launch();
+                A43G_CUDA_TRY(cudaGetLastError());
+                return true;
+            }
+        }
+        if constexpr (sizeof(T) == 8) {
+            if (dp.nlists[2] && dp.max_zline <= kMaxLine && dp.local64_pencils) {
+                local_pencil64_kernel<<<dp.nlists[2]*(64/kPencil64S), 8*kPencil64S, kPencil64Smem, st>>>(y, x,
                     dptr<uint32_t>(dp.lists_start[2]), dptr<int32_t>(dp.lists[2]), dptr<int32_t>(dp.nbr),
                     dptr<int32_t>(dp.veff_index), vcell<T>(dp), a);
                 count_launch();

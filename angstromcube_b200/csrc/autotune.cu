@@ -9,6 +9,7 @@
 //   * local_variant: FP32 local kernel on rows with one-step-ahead loads, on plain rows, on
 //                   y-pencils, or on y-pencils with staged neighbour cubes     {0, 1, 2, 3}
 //   * use_tc      : FP32 projector on the tensor cores (3xTF32) or on the CUDA cores
+//   * local64_pencils: FP64 local kernel on pencils (planes on two threads) or on rows
 // Each parameter is tuned in turn (coordinate descent), every candidate timed with CUDA events
 // on the caller's stream: two untimed applications, then the mean of three.  Scratch vectors
 // for x and y are allocated for the duration of the call.
@@ -108,6 +109,16 @@ bool autotune(GreenPlan const &hp, DevicePlan &dp, cudaStream_t st, std::string 
             if (t[v] < t[best]) best = v;
         }
         dp.local_variant = best;
+    }
+    if (sizeof(T) == 8 && dp.fused_local) {
+        float t[2] = {0, 0};
+        for (int v = 0; v < 2; ++v) {
+            dp.local64_pencils = (1 == v);
+            if (!time_part<T>(dp, 0, y, x, ci, st, t[v])) return false;
+            std::snprintf(line, sizeof(line), "FP64 local kernel, %s: %.3f ms\n", v ? "pencils" : "rows", t[v]);
+            report += line;
+        }
+        dp.local64_pencils = t[1] <= t[0];
     }
     std::snprintf(line, sizeof(line), "chosen: projector chunk %u, addition %u blocks per CTA, local %s, %s projector\n",
                   dp.prj_chunk, dp.add_blocks, local_name[dp.local_variant],

@@ -166,6 +166,9 @@ bool upload_plan(GreenPlan const &hp, DevicePlan &dp) {
         char const *l = std::getenv("A43G_LOCAL");
         dp.local_variant = (l && 0 == std::strcmp(l, "plain")) ? 1 : ((l && 0 == std::strcmp(l, "rows")) ? 0 :
                            ((l && 0 == std::strcmp(l, "staged")) ? 3 : 2));
+        // FP64 local kernel: "pencils" (default) or "rows"
+        char const *l64 = std::getenv("A43G_LOCAL64");
+        dp.local64_pencils = !(l64 && 0 == std::strcmp(l64, "rows"));
     }
     if (!dp.aac.alloc(std::max<size_t>(16, size_t(dp.ncoeffA)*dp.nCols*128*sizeof(double)))) return false;
     if (!dp.cadd.alloc(std::max<size_t>(16, size_t(dp.ncoeffA)*dp.nCols*128*sizeof(double)))) return false;

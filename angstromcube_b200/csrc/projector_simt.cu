@@ -80,8 +80,10 @@ __device__ __forceinline__ void cp_async8(void *dst, void const *src) {
 // every item stores its partial sums in part[w] and the last item of the group to finish (ticket
 // counter) adds the partials in item order, so the result does not depend on the order in which
 // the items ran, and resets the counter for the next call.
-template <typename T, int L>
-__global__ void __launch_bounds__(kThreads, Occ<T>::project)
+// ZS threads share a column and split its z-planes (FP64: one CTA of 128 threads per SM would
+// leave one warp per scheduler); their partial coefficients are added in a fixed order at the end.
+template <typename T, int L, int ZS = int(sizeof(T))/4>
+__global__ void __launch_bounds__(kThreads*ZS, Occ<T>::project)
 sho_project_simt_kernel(T *__restrict__ apc, T const *__restrict__ x, uint32_t nrhs,
                        uint32_t const *__restrict__ items, uint32_t const *__restrict__ prj_col,
                        uint64_t const *__restrict__ prj_coloff, uint32_t const *__restrict__ prj_slot,
@@ -96,7 +98,8 @@ sho_project_simt_kernel(T *__restrict__ apc, T const *__restrict__ x, uint32_t n
     uint32_t const a = item[0], s = item[1], k0 = item[2], k1 = item[3];
     uint32_t const g_first = item[4], g_count = item[5], g_id = item[6], g_part = item[7];
     if (active && !active[s]) return;                 // uniform: a retired source
-    int const tid = threadIdx.x, reim = tid >> 6, j = tid & 63;
+    constexpr int NT = kThreads*ZS, NZ = 4/ZS;         // threads, z-planes per thread
+    int const tid = threadIdx.x, zh = tid/kThreads, reim = (tid >> 6) & 1, j = tid & 63;
     uint64_t const off = prj_coloff[s];
 
     __shared__ __align__(16) T tbuf[2][(L + 1)*12];       // 1D tables of the staged blocks' slots
@@ -107,13 +110,13 @@ sho_project_simt_kernel(T *__restrict__ apc, T const *__restrict__ x, uint32_t n
         char const *src = reinterpret_cast<char const*>(x + size_t(b)*kBlk);
         char *dst = reinterpret_cast<char*>(xs + buf*kBlk);
 #pragma unroll
-        for (int r = 0; r < kBlk*int(sizeof(T))/(16*kThreads); ++r) {
-            int const o = (r*kThreads + tid)*16;
+        for (int r = 0; r < kBlk*int(sizeof(T))/(16*NT); ++r) {
+            int const o = (r*NT + tid)*16;
             cp_async16(dst + o, src + o);
         }
         constexpr int TE = 16/int(sizeof(T));          // table elements per 16-byte copy
         if (tid < (L + 1)*12/TE) cp_async16(&tbuf[buf][tid*TE], slot_H + size_t(slot)*stride + tid*TE);
-        if (tid == kThreads - 1) cp_async8(&mbuf[buf], slot_mask + slot);
+        if (tid == NT - 1) cp_async8(&mbuf[buf], slot_mask + slot);
     };
 
     T acc[NS];
@@ -136,8 +139,9 @@ sho_project_simt_kernel(T *__restrict__ apc, T const *__restrict__ x, uint32_t n
         uint64_t const mask = mbuf[buf];
         T const *xb = xs + buf*kBlk + reim*4096 + j;
 #pragma unroll
-        for (int z = 0; z < 4; ++z) {
-            if (0 == ((mask >> (16*z)) & 0xffffu)) continue;     // uniform: plane outside the sphere
+        for (int zl = 0; zl < NZ; ++zl) {
+            int const z = zh*NZ + zl;
+            if (0 == ((mask >> (16*z)) & 0xffffu)) continue;     // uniform per thread: plane outside the sphere
             T byx[N2];
 #pragma unroll
             for (int i = 0; i < N2; ++i) byx[i] = T(0);
@@ -173,6 +177,22 @@ sho_project_simt_kernel(T *__restrict__ apc, T const *__restrict__ x, uint32_t n
         }
         __syncthreads();                             // buffer buf is free for block k + 2
     }
+    if constexpr (ZS > 1) {
+        // the partial sums of the other z-planes, through the (now free) block stage, added in
+        // the order of the planes
+        cp_async_wait0();
+        __syncthreads();
+        if (zh > 0) {
+#pragma unroll
+            for (int sho = 0; sho < NS; ++sho) xs[(size_t(zh - 1)*NS + sho)*128 + reim*64 + j] = acc[sho];
+        }
+        __syncthreads();
+        if (zh > 0) return;
+        for (int h = 1; h < ZS; ++h) {
+#pragma unroll
+            for (int sho = 0; sho < NS; ++sho) acc[sho] += xs[(size_t(h - 1)*NS + sho)*128 + reim*64 + j];
+        }
+    }
     T *out = apc + (size_t(img_starts[a])*nrhs + s)*128 + reim*64 + j;
     if (1 == g_count) {
 #pragma unroll
@@ -186,9 +206,16 @@ sho_project_simt_kernel(T *__restrict__ apc, T const *__restrict__ x, uint32_t n
     for (int sho = 0; sho < NS; ++sho) mine[size_t(sho)*128] = acc[sho];
     __threadfence();                                  // partials visible before the ticket
     __shared__ uint32_t ticket;
-    __syncthreads();
-    if (0 == tid) ticket = atomicAdd(&tickets[g_id], 1u);
-    __syncthreads();
+    if constexpr (ZS > 1) {
+        // the remaining threads of the first z-group only (the others have returned)
+        asm volatile("bar.sync 1, %0;" :: "n"(kThreads) : "memory");
+        if (0 == tid) ticket = atomicAdd(&tickets[g_id], 1u);
+        asm volatile("bar.sync 1, %0;" :: "n"(kThreads) : "memory");
+    } else {
+        __syncthreads();
+        if (0 == tid) ticket = atomicAdd(&tickets[g_id], 1u);
+        __syncthreads();
+    }
     if (ticket + 1 != g_count) return;                // uniform: not the last item of the group
     __threadfence();
     T const *pg = part + size_t(g_part)*NS*128 + reim*64 + j;
@@ -395,7 +422,7 @@ void launch_project_L(DevicePlan &dp, T const *x, cudaStream_t st) {
     auto const &g = dp.prj_items[L];
     if (0 == g.count) return;
     constexpr int smem = 2*kBlk*int(sizeof(T));         // double-buffered block stage
-    sho_project_simt_kernel<T, L><<<g.count, kThreads, smem, st>>>(
+    sho_project_simt_kernel<T, L><<<g.count, kThreads*(int(sizeof(T))/4), smem, st>>>(
         dptr<T>(dp.apc), x, dp.nCols, dptr<uint32_t>(g.items8), dptr<uint32_t>(dp.prj_col),
         dptr<uint64_t>(dp.prj_coloff), dptr<uint32_t>(dp.prj_slot), simt_table<T>(dp),
         dptr<uint64_t>(dp.slot_mask), dp.table_stride, dptr<uint32_t>(dp.img_starts),

@@ -47,9 +47,9 @@ def test_action_fp64_fp32_vs_oracle(name):
 @pytest.mark.parametrize("variant", ["rows", "plain", "pencils", "staged"])
 @pytest.mark.parametrize("name", sorted(GEOMETRIES))
 def test_action_fp32_local_variants_vs_oracle(name, variant, monkeypatch):
-    """Every FP32 local kernel (rows with loads ahead; plain rows; y-pencils; y-pencils with staged
-    neighbour cubes, the default) matches the oracle on every boundary condition, with Bloch
-    phases (k != 0)."""
+    """Every FP32 local kernel (rows with loads ahead; plain rows; y-pencils, the default;
+    y-pencils with staged neighbour cubes) matches the oracle on every boundary condition, with
+    Bloch phases (k != 0)."""
     g = GEOMETRIES[name]()
     Vc, mats, offs, E, k, dVol, na = inputs_for(g)
     monkeypatch.setenv("A43G_LOCAL", variant)
@@ -57,6 +57,20 @@ def test_action_fp32_local_variants_vs_oracle(name, variant, monkeypatch):
     x = np.random.default_rng(3).standard_normal((p.nnzb, 2, 64, 64))
     y_ref = oracle.RestatedOracle(p.export(), Vc, E).action(x)
     assert rel_err(apply(p, x, np.float32), y_ref) < FP32_TOL
+
+
+@pytest.mark.parametrize("variant", ["rows", "pencils"])
+@pytest.mark.parametrize("name", sorted(GEOMETRIES))
+def test_action_fp64_local_variants_vs_oracle(name, variant, monkeypatch):
+    """Both FP64 local kernels (rows; pencils with the two planes on two threads, the default)
+    match the oracle to 1e-12 on every boundary condition, with Bloch phases (k != 0)."""
+    g = GEOMETRIES[name]()
+    Vc, mats, offs, E, k, dVol, na = inputs_for(g)
+    monkeypatch.setenv("A43G_LOCAL64", variant)
+    p = product_plan(g, Vc, mats, offs, E, k, dVol)
+    x = np.random.default_rng(4).standard_normal((p.nnzb, 2, 64, 64))
+    y_ref = oracle.RestatedOracle(p.export(), Vc, E).action(x)
+    assert rel_err(apply(p, x, np.float64), y_ref) < FP64_TOL
 
 
 def test_action_matches_reference_build():

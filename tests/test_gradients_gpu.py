@@ -52,7 +52,13 @@ def test_autograd_gradient_vs_central_differences():
     assert abs(L.item() - prob.value(V, H, S, R)) <= 1e-12 * abs(L.item())
     rng = np.random.default_rng(32)
     nsho = [h.shape[0] for h in H]
-    a = 5                                              # the atom whose matrices are varied
+    # the atom whose matrices are varied: the one nearest the source cube (the derivatives of the
+    # farther atoms are orders of magnitude smaller, below what central differences of solves to
+    # 1e-12 resolve to 1e-6)
+    from angstromcube_b200 import green_function as gf
+    cc = gf.construct_Green_function(prob.geometry).export()["colCubePos"].reshape(-1, 4)[0, :3]
+    centre = (cc.astype(np.float64) * 4 + 2) * np.asarray(prob.geometry.hg)
+    a = int(np.argmin(np.linalg.norm(R - centre, axis=1)))
     off = sum(n * n for n in nsho[:a])
     n = nsho[a]
 
