@@ -1289,6 +1289,70 @@ sho_broadcast_kernel(T *__restrict__ cad, double const *__restrict__ cadd, uint3
     }
 }
 
+// The atom-matrix chain in one kernel (collect, multiply, broadcast of the three kernels above),
+// per (atom, source, half of the 64 columns): the coefficients of the atom's images summed with
+// their Bloch phases into shared memory, multiplied by M_A (complex, FP64) and written to every
+// image with the conjugate phase.  Warp g of the four works on rows g, g + 4, ... (M_A's rows are
+// uniform over a warp), lane j on column half*32 + j.  Plans without periodic images take no
+// phases (the reference's direct path).  nSHO <= 56.
+constexpr int kAtomRows = 56;
+
+template <typename T>
+__global__ void __launch_bounds__(128)
+sho_atom_kernel(T *__restrict__ cad, T const *__restrict__ apc, uint32_t nrhs,
+                int8_t const *__restrict__ atom_lmax, uint32_t const *__restrict__ sum_start,
+                uint32_t const *__restrict__ sum_col, uint32_t const *__restrict__ img_starts,
+                double const *__restrict__ img_phase, double const *__restrict__ mats,
+                uint32_t const *__restrict__ mat_off, int use_phase, DyadicPairs const bp)
+{
+    __shared__ double sre[kAtomRows][32], sim[kAtomRows][32];
+    int const A = blockIdx.x, s = blockIdx.y, half = blockIdx.z;
+    int const j = threadIdx.x & 31, g = threadIdx.x >> 5, col = half*32 + j;
+    if (bp.active && !bp.active[s]) return;
+    img_phase += (s/bp.nsrc_pair)*bp.img_stride;
+    mats += (s/bp.nsrc_pair)*bp.mat_stride;
+    int const nc = nsho_c(atom_lmax[A]);
+    uint32_t const k0 = sum_start[A], k1 = sum_start[A + 1];
+    for (int c = g; c < nc; c += 4) {
+        double re = 0, im = 0;
+        for (uint32_t k = k0; k < k1; ++k) {
+            uint32_t const i = sum_col[k];
+            T const *src = apc + ((size_t(img_starts[i]) + c)*nrhs + s)*128;
+            double const xr = double(src[col]), xi = double(src[64 + col]);
+            if (use_phase) {
+                double const pr = img_phase[4*i], pi = img_phase[4*i + 1];
+                re += pr*xr - pi*xi;
+                im += pr*xi + pi*xr;
+            } else {
+                re += xr; im += xi;
+            }
+        }
+        sre[c][j] = re; sim[c][j] = im;
+    }
+    __syncthreads();
+    double const *Mr = mats + mat_off[A], *Mi = Mr + nc*nc;
+    for (int r = g; r < nc; r += 4) {
+        double re = 0, im = 0;
+        for (int k = 0; k < nc; ++k) {
+            double const mr = __ldg(Mr + r*nc + k), mi = __ldg(Mi + r*nc + k);
+            double const xr = sre[k][j], xi = sim[k][j];
+            re += mr*xr - mi*xi;
+            im += mr*xi + mi*xr;
+        }
+        for (uint32_t k = k0; k < k1; ++k) {
+            uint32_t const i = sum_col[k];
+            T *dst = cad + ((size_t(img_starts[i]) + r)*nrhs + s)*128;
+            if (use_phase) {
+                double const pr = img_phase[4*i], pi = -img_phase[4*i + 1];
+                dst[col] = T(pr*re - pi*im);
+                dst[64 + col] = T(pr*im + pi*re);
+            } else {
+                dst[col] = T(re); dst[64 + col] = T(im);
+            }
+        }
+    }
+}
+
 // y[b] += sum over the images a near block b of the masked projector functions times
 // cad[a, rhs(b)] (include/green_dyadic.hxx:325-518); sum-factorized over z, y, x.
 // One CTA per block, 128 threads = (reim, column); only masked points are written.
@@ -1509,7 +1573,13 @@ bool launch_dyadic(DevicePlan &dp, T *y, T const *x, uint16_t const *colIndex, c
         launch_project_L<T, 6>(dp, x, st); launch_project_L<T, 7>(dp, x, st);
     }
     dim3 const ga(dp.nAtoms, dp.nCols);
-    if (dp.nAI > dp.nAtoms) {
+    if (dp.lmax_max <= 5 && !dp.atom_chain3) {
+        sho_atom_kernel<T><<<dim3(dp.nAtoms, dp.nCols, 2), 128, 0, st>>>(dptr<T>(dp.cad), dptr<T>(dp.apc), dp.nCols,
+            dptr<int8_t>(dp.atom_lmax), dptr<uint32_t>(dp.sum_start), dptr<uint32_t>(dp.sum_col),
+            dptr<uint32_t>(dp.img_starts), dptr<double>(dp.img_phase), dptr<double>(dp.atom_mat),
+            dptr<uint32_t>(dp.atom_mat_off), dp.nAI > dp.nAtoms ? 1 : 0, dyadic_pairs(dp));
+        count_launch();
+    } else if (dp.nAI > dp.nAtoms) {
         sho_collect_kernel<T><<<ga, 64, 0, st>>>(dptr<double>(dp.aac), dptr<T>(dp.apc), dp.nCols,
             dptr<uint32_t>(dp.atom_starts), dptr<int8_t>(dp.atom_lmax), dptr<uint32_t>(dp.sum_start),
             dptr<uint32_t>(dp.sum_col), dptr<uint32_t>(dp.img_starts), dptr<double>(dp.img_phase), dyadic_pairs(dp));

@@ -120,6 +120,16 @@ bool autotune(GreenPlan const &hp, DevicePlan &dp, cudaStream_t st, std::string 
         }
         dp.local64_pencils = t[1] <= t[0];
     }
+    if (sizeof(T) == 8 && dp.nAI > 0 && dp.nCols > 0) {
+        float t[2] = {0, 0};
+        for (int v = 0; v < 2; ++v) {
+            dp.add64_unrolled = (1 == v);
+            if (!time_part<T>(dp, 1, y, x, ci, st, t[v])) return false;
+            std::snprintf(line, sizeof(line), "FP64 projector, addition %s: %.3f ms\n", v ? "unrolled" : "rolled", t[v]);
+            report += line;
+        }
+        dp.add64_unrolled = t[1] <= t[0];
+    }
     std::snprintf(line, sizeof(line), "chosen: projector chunk %u, addition %u blocks per CTA, local %s, %s projector\n",
                   dp.prj_chunk, dp.add_blocks, local_name[dp.local_variant],
                   dp.use_tc ? "tensor-core" : "CUDA-core");

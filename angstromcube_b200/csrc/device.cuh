@@ -49,6 +49,8 @@ struct DevicePlan {
     uint32_t add_blocks = 16;        // blocks per CTA of the FP32 addition
     int local_variant = 2;           // FP32: 0 rows with one-step-ahead loads, 1 plain rows, 2 pencils, 3 staged pencils
     bool local64_pencils = true;     // FP64: pencils with the planes on two threads, else the row kernel
+    bool add64_unrolled = true;      // FP64 addition: z-orders unrolled, else one at a time
+    bool atom_chain3 = false;        // atom matrices by the collect/multiply/broadcast kernels instead of one
     uint32_t nlists[3] = {0, 0, 0};
 
     DeviceBuffer veff_index;     // int32 [nnzb]

@@ -169,6 +169,12 @@ bool upload_plan(GreenPlan const &hp, DevicePlan &dp) {
         // FP64 local kernel: "pencils" (default) or "rows"
         char const *l64 = std::getenv("A43G_LOCAL64");
         dp.local64_pencils = !(l64 && 0 == std::strcmp(l64, "rows"));
+        // FP64 addition: z-orders "unrolled" (default) or "rolled"
+        char const *a64 = std::getenv("A43G_ADD64");
+        dp.add64_unrolled = !(a64 && 0 == std::strcmp(a64, "rolled"));
+        // atom-matrix chain: one kernel (default) or "three" (collect, multiply, broadcast)
+        char const *ac = std::getenv("A43G_ATOM_CHAIN");
+        dp.atom_chain3 = (ac && 0 == std::strcmp(ac, "three"));
     }
     if (!dp.aac.alloc(std::max<size_t>(16, size_t(dp.ncoeffA)*dp.nCols*128*sizeof(double)))) return false;
     if (!dp.cadd.alloc(std::max<size_t>(16, size_t(dp.ncoeffA)*dp.nCols*128*sizeof(double)))) return false;

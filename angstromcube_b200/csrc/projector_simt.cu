@@ -136,6 +136,12 @@ sho_project_simt_kernel(T *__restrict__ apc, T const *__restrict__ x, uint32_t n
         __syncthreads();                             // ... and everybody else's
         Tables<T, L> t;
         t.load(tbuf[buf]);
+        // the x-functions of the slot in registers (FP64 reads the other tables in place)
+        T tx[L + 1][4];
+#pragma unroll
+        for (int ix = 0; ix <= L; ++ix)
+#pragma unroll
+            for (int xx = 0; xx < 4; ++xx) tx[ix][xx] = t(ix, 0, xx);
         uint64_t const mask = mbuf[buf];
         T const *xb = xs + buf*kBlk + reim*4096 + j;
 #pragma unroll
@@ -155,7 +161,7 @@ sho_project_simt_kernel(T *__restrict__ apc, T const *__restrict__ x, uint32_t n
                     int const p = (z*4 + yy)*4 + xx;
                     T const v = ((mask >> p) & 1u) ? xb[p*64] : T(0);
 #pragma unroll
-                    for (int ix = 0; ix <= L; ++ix) ax[ix] = fmat(v, t(ix, 0, xx), ax[ix]);
+                    for (int ix = 0; ix <= L; ++ix) ax[ix] = fmat(v, tx[ix][xx], ax[ix]);
                 }
 #pragma unroll
                 for (int iy = 0, iyx = 0; iy <= L; ++iy) {
@@ -235,10 +241,12 @@ sho_project_simt_kernel(T *__restrict__ apc, T const *__restrict__ x, uint32_t n
 // fit the registers): thread zh owns x = zh*(4/ZS) ... of every (z, y) row, so each stage of
 // the contraction (x, then y, then z) is split between them without repeating any work.  The
 // sums are ordered acc[(z*4 + y)*(4/ZS) + x - zh*(4/ZS)].
-template <typename T, int L, bool FULL, int ZS>
+// UZ: the z-orders unrolled (tables and coefficient offsets known at compile time) or one at a
+// time (fewer registers)
+template <typename T, int L, bool FULL, int ZS, bool UZ>
 __device__ __forceinline__ void add_image(T (&acc)[64/ZS], Tables<T, L> const &t, uint64_t mask,
                                           T const *__restrict__ c, size_t cstride, int zh) {
-    constexpr int kUnrollZ = (8 == sizeof(T)) ? 1 : L + 1;     // FP64: one z-order at a time (registers)
+    constexpr int kUnrollZ = UZ ? L + 1 : 1;
     constexpr int NX = 4/ZS;                                   // x-points of this thread
     int const x0 = (1 == ZS) ? 0 : zh*NX;
     int sho = 0;
@@ -278,13 +286,13 @@ __device__ __forceinline__ void add_image(T (&acc)[64/ZS], Tables<T, L> const &t
     }
 }
 
-template <typename T, int L, int ZS>
+template <typename T, int L, int ZS, bool UZ>
 __device__ __forceinline__ void add_image_L(T (&acc)[64/ZS], T const *__restrict__ tab, uint64_t mask,
                                             T const *__restrict__ c, size_t cstride, int zh) {
     Tables<T, L> t;
     t.load(tab);
-    if (~0ull == mask) add_image<T, L, true, ZS>(acc, t, mask, c, cstride, zh);
-    else add_image<T, L, false, ZS>(acc, t, mask, c, cstride, zh);
+    if (~0ull == mask) add_image<T, L, true, ZS, UZ>(acc, t, mask, c, cstride, zh);
+    else add_image<T, L, false, ZS, UZ>(acc, t, mask, c, cstride, zh);
 }
 
 // LMAX: largest basis size of the plan (the instantiation has no larger one).  One CTA walks the
@@ -292,7 +300,7 @@ __device__ __forceinline__ void add_image_L(T (&acc)[64/ZS], T const *__restrict
 // stream: the coefficients, table and mask of the next pair are staged while the current pair is
 // applied, and the y values of the next block with atoms are staged during the whole of the
 // current block, so neither the start of a block nor its final y update waits for memory.
-template <typename T, int LMAX, int ZS = int(sizeof(T))/4>
+template <typename T, int LMAX, int ZS = int(sizeof(T))/4, bool UZ = true>
 __global__ void __launch_bounds__(kThreads*ZS, Occ<T>::add)
 sho_add_simt_kernel(T *__restrict__ y, T const *__restrict__ cad, uint32_t nrhs, uint32_t nnzb,
                     uint32_t blocks_per_cta, uint16_t const *__restrict__ colIndex,
@@ -377,14 +385,14 @@ sho_add_simt_kernel(T *__restrict__ y, T const *__restrict__ cad, uint32_t nrhs,
             T const *tab = tbuf[buf];
             T const *c = cbuf + buf*NCMAX*128 + reim*64 + j;
             int const L = int(cur.z);                      // uniform over the CTA
-            if (L == LMAX) add_image_L<T, LMAX, ZS>(acc, tab, mask, c, 128, zh);
-            else if (LMAX > 0 && L == 0) add_image_L<T, 0, ZS>(acc, tab, mask, c, 128, zh);
-            else if (LMAX > 1 && L == 1) add_image_L<T, (LMAX > 1 ? 1 : 0), ZS>(acc, tab, mask, c, 128, zh);
-            else if (LMAX > 2 && L == 2) add_image_L<T, (LMAX > 2 ? 2 : 0), ZS>(acc, tab, mask, c, 128, zh);
-            else if (LMAX > 3 && L == 3) add_image_L<T, (LMAX > 3 ? 3 : 0), ZS>(acc, tab, mask, c, 128, zh);
-            else if (LMAX > 4 && L == 4) add_image_L<T, (LMAX > 4 ? 4 : 0), ZS>(acc, tab, mask, c, 128, zh);
-            else if (LMAX > 5 && L == 5) add_image_L<T, (LMAX > 5 ? 5 : 0), ZS>(acc, tab, mask, c, 128, zh);
-            else if (LMAX > 6 && L == 6) add_image_L<T, (LMAX > 6 ? 6 : 0), ZS>(acc, tab, mask, c, 128, zh);
+            if (L == LMAX) add_image_L<T, LMAX, ZS, UZ>(acc, tab, mask, c, 128, zh);
+            else if (LMAX > 0 && L == 0) add_image_L<T, 0, ZS, UZ>(acc, tab, mask, c, 128, zh);
+            else if (LMAX > 1 && L == 1) add_image_L<T, (LMAX > 1 ? 1 : 0), ZS, UZ>(acc, tab, mask, c, 128, zh);
+            else if (LMAX > 2 && L == 2) add_image_L<T, (LMAX > 2 ? 2 : 0), ZS, UZ>(acc, tab, mask, c, 128, zh);
+            else if (LMAX > 3 && L == 3) add_image_L<T, (LMAX > 3 ? 3 : 0), ZS, UZ>(acc, tab, mask, c, 128, zh);
+            else if (LMAX > 4 && L == 4) add_image_L<T, (LMAX > 4 ? 4 : 0), ZS, UZ>(acc, tab, mask, c, 128, zh);
+            else if (LMAX > 5 && L == 5) add_image_L<T, (LMAX > 5 ? 5 : 0), ZS, UZ>(acc, tab, mask, c, 128, zh);
+            else if (LMAX > 6 && L == 6) add_image_L<T, (LMAX > 6 ? 6 : 0), ZS, UZ>(acc, tab, mask, c, 128, zh);
         }
         cur = nxt; nxt = after;
         if (t + 1 == bend) {
@@ -433,9 +441,12 @@ void launch_project_L(DevicePlan &dp, T const *x, cudaStream_t st) {
 template <typename T, int LMAX>
 void launch_add_L(DevicePlan &dp, T *y, uint16_t const *colIndex, cudaStream_t st) {
     constexpr int smem = (2*nsho_of(LMAX)*128 + kBlk)*int(sizeof(T));
+    constexpr int ZS = int(sizeof(T))/4;
     uint32_t const per_cta = std::max<uint32_t>(1, dp.add_blocks);
     unsigned const grid = (dp.nnzb + per_cta - 1)/per_cta;
-    sho_add_simt_kernel<T, LMAX><<<grid, kThreads*(int(sizeof(T))/4), smem, st>>>(y, dptr<T>(dp.cad), dp.nCols, dp.nnzb, per_cta,
+    auto *k = sho_add_simt_kernel<T, LMAX, ZS, true>;
+    if (sizeof(T) == 8 && !dp.add64_unrolled) k = sho_add_simt_kernel<T, LMAX, ZS, false>;
+    k<<<grid, kThreads*ZS, smem, st>>>(y, dptr<T>(dp.cad), dp.nCols, dp.nnzb, per_cta,
         colIndex, dptr<uint32_t>(dp.add_start), dptr<uint4>(dp.add_info), simt_table<T>(dp),
         dptr<uint64_t>(dp.slot_mask), dp.table_stride, dp.retire ? dptr<uint8_t>(dp.src_active) : nullptr);
 }
@@ -444,8 +455,11 @@ template <typename T, int L>
 void set_smem_attributes() {
     cudaFuncSetAttribute(sho_project_simt_kernel<T, L>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          2*kBlk*int(sizeof(T)));
-    cudaFuncSetAttribute(sho_add_simt_kernel<T, L>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaFuncSetAttribute(sho_add_simt_kernel<T, L, int(sizeof(T))/4, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (2*nsho_of(L)*128 + kBlk)*int(sizeof(T)));
+    if (sizeof(T) == 8)
+        cudaFuncSetAttribute(sho_add_simt_kernel<T, L, int(sizeof(T))/4, false>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (2*nsho_of(L)*128 + kBlk)*int(sizeof(T)));
 }
 
 } // namespace

@@ -195,7 +195,7 @@ def cpu_action_seconds(workload, E, procs=None, reps=1):
     return max(times), procs
 
 
-def _ref_configs0_solve(_):
+def _ref_small_cell_solve(_):
     """The CPU-runnable configuration solved for real: the reference's CPU action inside the
     numpy restatement of tfQMR (oracle/tfqmr.py), FP64 to 1e-9.  Returns (iterations, seconds)."""
     devnull = os.open(os.devnull, os.O_WRONLY)
@@ -249,7 +249,7 @@ def reference_arm(a):
     value = sum(vals) / len(vals)
     # the CPU-runnable configuration solved for real on every core
     with mp.get_context("spawn").Pool(min(cores, 8)) as pool:
-        sol = pool.map(_ref_configs0_solve, range(min(cores, 8)))
+        sol = pool.map(_ref_small_cell_solve, range(min(cores, 8)))
     it0, s0, ok0 = sol[0]
     sample = ("reference action_t<double,2,1>::multiply (oracle/_ref CPU build, -O3 x86-64-v3) of the contour "
               "cell with one source cube per process, %d processes, %.2f s per action; a solve = 8 sources x 2 x "
@@ -263,7 +263,7 @@ def reference_arm(a):
         "impl": "reference",
         "cpu_baseline": {"value": value, "unit": "solves/s", "cores": cores, "kind": "reference", "sample": sample},
         "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "configs0_cpu_solve": {"iterations": it0, "seconds": s0, "converged": ok0, "processes": len(sol),
+        "small_cell_cpu_solve": {"iterations": it0, "seconds": s0, "converged": ok0, "processes": len(sol),
                                "solves_per_s": len(sol) / max(s[1] for s in sol),
                                "what": "periodic 4^3-cube cell, one atom: reference CPU action inside the numpy "
                                        "tfQMR restatement, FP64 to 1e-9, one solve per process"},
@@ -422,7 +422,7 @@ def our_arm(a):
     # k-points in, the pairs' densities out; one wave per step, timed on the host around synchronized work
     Vpin = torch.from_numpy(w.Vcell).pin_memory().numpy()
     Mpin = torch.from_numpy(w.mats).pin_memory().numpy()
-    ke2e = 0 if a.no_e2e else max(1, a.steps // 2)
+    ke2e = 0 if a.no_e2e else a.steps              # the same pairs as the timed steps
     torch.cuda.synchronize()
     te = time.perf_counter()
     conv_e2e = 0
@@ -443,7 +443,7 @@ def our_arm(a):
                "warmup": a.warmup, "ms_per_step": 1e3 * tmax / a.steps, "higher_is_better": True, "scaling": "weak",
                "vs_baseline": None, "dtype": "f32 recurrences and operator, f64 solution and residual replacement",
                "data": "synthetic (seeded)",
-               "config": {"workload": "batched contour (configs 3): %s, 32 Gauss-Legendre energies on the semicircle "
+               "config": {"workload": "batched contour: %s, 32 Gauss-Legendre energies on the semicircle "
                                       "-1..0 Ha x %d k-points, 8 source cubes, tolerance %g" % (WORKLOAD, a.nk, TOLERANCE),
                           "cell_cubes": [16, 16, 16], "sources": plan.nCols, "rhs_columns": plan.nCols * 64,
                           "atoms": w.natoms, "numax": 5, "nnzb_per_pair": plan.nnzb, "one_plan_for_all_radii": one_plan,
@@ -628,9 +628,18 @@ def profile_case(a):
                   "projector_ms": t1 * 1e3})
         x = x.double()
         y = torch.empty_like(x)
-        t0 = time_part(_lib, p, 0, _lib.A43G_F64, x, y, 4, stream)
-        t1 = time_part(_lib, p, 1, _lib.A43G_F64, x, y, 4, stream)
-        emit({"case": "action", "precision": "float64", "local_ms": t0 * 1e3, "projector_ms": t1 * 1e3})
+        for name, env in (("pencils, addition unrolled", {}), ("rows, addition rolled",
+                                                               {"A43G_LOCAL64": "rows", "A43G_ADD64": "rolled"})):
+            for k in ("A43G_LOCAL64", "A43G_ADD64"):
+                os.environ.pop(k, None)
+            os.environ.update(env)
+            p = plan_for("simt")
+            t0 = time_part(_lib, p, 0, _lib.A43G_F64, x, y, 4, stream)
+            t1 = time_part(_lib, p, 1, _lib.A43G_F64, x, y, 4, stream)
+            emit({"case": "action", "precision": "float64", "kernels": name, "local_ms": t0 * 1e3,
+                  "projector_ms": t1 * 1e3})
+        for k in ("A43G_LOCAL64", "A43G_ADD64"):
+            os.environ.pop(k, None)
     else:
         p = plan_for("simt")
         for precision in ("float32", "float64"):
@@ -718,7 +727,12 @@ def main():
         # pairs one at a time: the metric's comparison on matched solves
         sel = [i for s, _ in records for i in s][:max(1, a.fp64_pairs)]
         r64 = fp64_plain(plan, w, pairs, sel, stream, opts)
-        rmx = mixed_single(plan, w, pairs, sel, stream, opts)
+        if a.wave == 1:
+            # the timed solves of these pairs (one pair per wave, device-timed by the solver)
+            timed = {i: st for s_, sts in records for i, st in zip(s_, sts)}
+            rmx = [(bool(timed[i]["converged"]), timed[i]["iterations"], timed[i]["seconds"]) for i in sel]
+        else:
+            rmx = mixed_single(plan, w, pairs, sel, stream, opts)
         t64, tmx = sum(r[2] for r in r64), sum(r[2] for r in rmx)
         c64, cmx = sum(r[0] for r in r64), sum(r[0] for r in rmx)
         out["fp64_plain"] = {"pairs": sel, "solves_per_s": c64 / t64, "seconds": t64, "converged": c64,

@@ -59,18 +59,27 @@ def test_action_fp32_local_variants_vs_oracle(name, variant, monkeypatch):
     assert rel_err(apply(p, x, np.float32), y_ref) < FP32_TOL
 
 
-@pytest.mark.parametrize("variant", ["rows", "pencils"])
+@pytest.mark.parametrize("variant", ["rows", "pencils", "rolled", "chain3"])
 @pytest.mark.parametrize("name", sorted(GEOMETRIES))
 def test_action_fp64_local_variants_vs_oracle(name, variant, monkeypatch):
-    """Both FP64 local kernels (rows; pencils with the two planes on two threads, the default)
-    match the oracle to 1e-12 on every boundary condition, with Bloch phases (k != 0)."""
+    """Both FP64 local kernels (rows; pencils with the two planes on two threads, the default),
+    both FP64 additions (z-orders unrolled, the default; "rolled": one at a time) and both
+    atom-matrix chains (one kernel, the default; "chain3": collect, multiply, broadcast) match the
+    oracle (FP64 to 1e-12, FP32 to 3e-5) on every boundary condition, with Bloch phases (k != 0)."""
     g = GEOMETRIES[name]()
     Vc, mats, offs, E, k, dVol, na = inputs_for(g)
-    monkeypatch.setenv("A43G_LOCAL64", variant)
+    if variant == "rolled":
+        monkeypatch.setenv("A43G_ADD64", "rolled")
+    elif variant == "chain3":
+        monkeypatch.setenv("A43G_ATOM_CHAIN", "three")
+    else:
+        monkeypatch.setenv("A43G_LOCAL64", variant)
     p = product_plan(g, Vc, mats, offs, E, k, dVol)
     x = np.random.default_rng(4).standard_normal((p.nnzb, 2, 64, 64))
     y_ref = oracle.RestatedOracle(p.export(), Vc, E).action(x)
     assert rel_err(apply(p, x, np.float64), y_ref) < FP64_TOL
+    if variant == "chain3":
+        assert rel_err(apply(p, x, np.float32), y_ref) < FP32_TOL
 
 
 def test_action_matches_reference_build():
