@@ -122,6 +122,9 @@ struct Ctx {
     double tol, delta;
     int32_t gap, mixed, retire;
     int32_t stall_limit;         // replacements without progress of the true residual before FP64
+    double stall_gap;            // > 0: a replacement counts as a stall only if the true residual
+                                 // exceeds the QMR estimate by this factor (the recurrences lost
+                                 // accuracy, rather than converging slowly)
     int32_t abs_tol;             // the tolerance is absolute (the FP64 continuation of unit columns)
 };
 
@@ -388,19 +391,22 @@ __device__ void step_alpha(Ctx const &c, uint32_t s, double const (&r)[2]) {
 
 // residual replacement: r = |B - A X64|^2, rt^H W with the new W
 __device__ void step_replace(Ctx const &c, uint32_t s, double const (&r)[3]) {
-    __shared__ double resmax[64];
+    __shared__ double resmax[64], gapmax[64];
     int const j = threadIdx.x;
     bool act = false;
     if (j < 64) {
         uint32_t const col = s*64 + j;
         ColState st = c.cs[col];
         double const res = (st.bnorm > 0) ? sqrt(r[0])/st.bnorm : 0.0;
+        double gap = 0.0;
         if (0 == st.status) {
             st.res = res;
             if (res <= c.tol) {
                 st.status = 1; freeze(st);
             } else {
                 double const est = st.tau*sqrt(double(st.m) + 1.0)/st.bnorm;
+                // the gap opened since the previous replacement (whose gap is in scale)
+                gap = res/fmax(est*st.scale, 1e-300);
                 st.scale = fmax(1.0, res/fmax(est, 1e-300));
                 double const rnr = r[1], rni = r[2];
                 if (rnr*rnr + rni*rni == 0.0) {
@@ -415,19 +421,23 @@ __device__ void step_replace(Ctx const &c, uint32_t s, double const (&r)[3]) {
         store_coef(c, col, st);
         act = (0 == st.status);
         resmax[j] = act ? res : 0.0;
+        gapmax[j] = act ? gap : 0.0;
     }
     bool any = __syncthreads_or(act);
     __shared__ int fb;
     if (0 == threadIdx.x) {
-        double e = 0;
+        double e = 0, g = 0;
         bool finite = true;
-        for (int k = 0; k < 64; ++k) { e = fmax(e, resmax[k]); finite = finite && isfinite(resmax[k]); }
+        for (int k = 0; k < 64; ++k) {
+            e = fmax(e, resmax[k]); g = fmax(g, gapmax[k]); finite = finite && isfinite(resmax[k]);
+        }
         SrcState &src = c.ss[s];
         src.est_ref = e;
         src.updates += 1;
         // progress: the largest true residual halved since the best one so far (slower progress
         // is slower than the FP64 recurrences, whose iterations cost 2.7 times as much)
-        if (e < 0.5*src.best) { src.best = e; src.stall = 0; } else src.stall += 1;
+        if (e < 0.5*src.best) { src.best = e; src.stall = 0; }
+        else if (!(c.stall_gap > 0) || g >= c.stall_gap) src.stall += 1;
         fb = any && (!finite || src.stall >= c.stall_limit);
         if (fb) { src.fallback = 1; src.nonfinite = !finite; }
     }
@@ -881,6 +891,11 @@ bool prepare(DevicePlan &dp, SolverWorkspace &ws, a43g_solve_options_t const &op
     c.mixed = mixed ? 1 : 0;
     c.retire = retire ? 1 : 0;
     c.stall_limit = 3;
+    {
+        // experiment switch: the gap rule above (off by default)
+        char const *g = std::getenv("A43G_STALL_GAP");
+        c.stall_gap = g ? std::atof(g) : 0.0;
+    }
     c.abs_tol = 0;
     p.units = units;
     return true;

@@ -82,6 +82,8 @@ def parse():
                          "E = -0.2 + 0.02i to 1e-10: plain FP64 solve, then the mixed solve with the error of "
                          "G against it every 10 iterations")
     ap.add_argument("--wrapped32-iterations", type=int, default=2000, help="iteration limit of --wrapped32")
+    ap.add_argument("--wrapped32-energy", type=complex, default=complex(-0.2, 0.02),
+                    help="energy of --wrapped32 (Python complex literal, e.g. -0.2+0.1j)")
     ap.add_argument("--nk", type=int, default=4, help="k-points of the contour")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
@@ -652,7 +654,8 @@ def profile_case(a):
 def wrapped32(a):
     """Mixed precision on the large cell: the wrapped 32^3-cube cell (128^3 points, h = 0.25 Bohr)
     with 256 atoms on a jittered 8x8x4 lattice (numax 5, sigma 0.6), 32 source cubes (2048
-    columns), truncation radius 12 Bohr, E = -0.2 + 0.02i, tolerance 1e-10.  First the plain FP64
+    columns), truncation radius 12 Bohr, E = -0.2 + 0.02i (or --wrapped32-energy), tolerance
+    1e-10.  First the plain FP64
     solve (no retirement, the reference's algorithm), whose solution is kept on the device, then
     the mixed solve traced against it: the relative error of G every 10 iterations (the
     residual-replacement gap) and at the end.  One FP64 block vector is 19.7 GB; the FP64 solve
@@ -665,13 +668,14 @@ def wrapped32(a):
     t1 = time.perf_counter()
     plan = gf.construct_Green_function(w.geometry)
     t2 = time.perf_counter()
+    E = complex(a.wrapped32_energy)
     gf.update_potential(plan, w.Vcell, w.mats, w.offsets, layout="cells")
-    gf.update_energy_parameter(plan, w.E, w.dVol)
+    gf.update_energy_parameter(plan, E, w.dVol)
     plan.upload()
     stream = torch.cuda.Stream()
     tune = green_action.autotune(plan, "float32", stream)
     out = {"cell": "wrapped32_256atoms", "nnzb": plan.nnzb, "columns": 64 * plan.nCols,
-           "atoms": plan.sizes["nAtoms"], "atom_images": plan.sizes["nAtomImages"], "E": [w.E.real, w.E.imag],
+           "atoms": plan.sizes["nAtoms"], "atom_images": plan.sizes["nAtomImages"], "E": [E.real, E.imag],
            "tolerance": 1e-10, "max_iterations": a.wrapped32_iterations,
            "seconds_inputs": t1 - t0, "seconds_host_plan": t2 - t1, "autotune": tune.strip().splitlines()[-1:]}
     emit({"setup": out})
