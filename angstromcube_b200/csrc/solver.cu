@@ -122,10 +122,8 @@ struct Ctx {
     double tol, delta;
     int32_t gap, mixed, retire;
     int32_t stall_limit;         // replacements without progress of the true residual before FP64
-    double stall_gap;            // > 0: a replacement counts as a stall only if the true residual
-                                 // exceeds the QMR estimate by this factor (the recurrences lost
-                                 // accuracy, rather than converging slowly)
     int32_t abs_tol;             // the tolerance is absolute (the FP64 continuation of unit columns)
+    int32_t vec16;               // K_A, K_C, K_E with 16-byte accesses (else the scalar kernels)
 };
 
 __device__ __forceinline__ uint32_t mix32(uint32_t h) {
@@ -180,15 +178,30 @@ __device__ bool reduce_source(Ctx const &c, uint32_t u, uint32_t s, double const
     __syncthreads();
     if (ticket + 1 != c.nch) return false;            // uniform over the CTA
     __threadfence();
-    // thread (q, j) adds the units q, q + 4, ... of the source, then the four partial sums
-    double acc[NC];
+    // thread (q, j) adds the units q, q + 4, ... of the source into four interleaved partial
+    // sums (independent loads in flight), combined in a fixed order, then the four q's sums
+    double acc4[4][NC];
 #pragma unroll
-    for (int k = 0; k < NC; ++k) acc[k] = 0;
-    for (uint32_t i = q; i < c.nch; i += 4) {
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int k = 0; k < NC; ++k) acc4[u][k] = 0;
+    uint32_t i = q;
+    for (; i + 12 < c.nch; i += 16) {
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            size_t const base = size_t(s)*c.nch + i + 4*u;
+#pragma unroll
+            for (int k = 0; k < NC; ++k) acc4[u][k] += __ldcg(&c.part[(base*kSlots + k)*64 + j]);
+        }
+    }
+    for (; i < c.nch; i += 4) {
         size_t const base = size_t(s)*c.nch + i;
 #pragma unroll
-        for (int k = 0; k < NC; ++k) acc[k] += __ldcg(&c.part[(base*kSlots + k)*64 + j]);
+        for (int k = 0; k < NC; ++k) acc4[0][k] += __ldcg(&c.part[(base*kSlots + k)*64 + j]);
     }
+    double acc[NC];
+#pragma unroll
+    for (int k = 0; k < NC; ++k) acc[k] = ((acc4[0][k] + acc4[1][k]) + acc4[2][k]) + acc4[3][k];
     __syncthreads();
 #pragma unroll
     for (int k = 0; k < NC; ++k) red[q][j][k] = acc[k];
@@ -391,22 +404,19 @@ __device__ void step_alpha(Ctx const &c, uint32_t s, double const (&r)[2]) {
 
 // residual replacement: r = |B - A X64|^2, rt^H W with the new W
 __device__ void step_replace(Ctx const &c, uint32_t s, double const (&r)[3]) {
-    __shared__ double resmax[64], gapmax[64];
+    __shared__ double resmax[64];
     int const j = threadIdx.x;
     bool act = false;
     if (j < 64) {
         uint32_t const col = s*64 + j;
         ColState st = c.cs[col];
         double const res = (st.bnorm > 0) ? sqrt(r[0])/st.bnorm : 0.0;
-        double gap = 0.0;
         if (0 == st.status) {
             st.res = res;
             if (res <= c.tol) {
                 st.status = 1; freeze(st);
             } else {
                 double const est = st.tau*sqrt(double(st.m) + 1.0)/st.bnorm;
-                // the gap opened since the previous replacement (whose gap is in scale)
-                gap = res/fmax(est*st.scale, 1e-300);
                 st.scale = fmax(1.0, res/fmax(est, 1e-300));
                 double const rnr = r[1], rni = r[2];
                 if (rnr*rnr + rni*rni == 0.0) {
@@ -421,23 +431,19 @@ __device__ void step_replace(Ctx const &c, uint32_t s, double const (&r)[3]) {
         store_coef(c, col, st);
         act = (0 == st.status);
         resmax[j] = act ? res : 0.0;
-        gapmax[j] = act ? gap : 0.0;
     }
     bool any = __syncthreads_or(act);
     __shared__ int fb;
     if (0 == threadIdx.x) {
-        double e = 0, g = 0;
+        double e = 0;
         bool finite = true;
-        for (int k = 0; k < 64; ++k) {
-            e = fmax(e, resmax[k]); g = fmax(g, gapmax[k]); finite = finite && isfinite(resmax[k]);
-        }
+        for (int k = 0; k < 64; ++k) { e = fmax(e, resmax[k]); finite = finite && isfinite(resmax[k]); }
         SrcState &src = c.ss[s];
         src.est_ref = e;
         src.updates += 1;
         // progress: the largest true residual halved since the best one so far (slower progress
         // is slower than the FP64 recurrences, whose iterations cost 2.7 times as much)
-        if (e < 0.5*src.best) { src.best = e; src.stall = 0; }
-        else if (!(c.stall_gap > 0) || g >= c.stall_gap) src.stall += 1;
+        if (e < 0.5*src.best) { src.best = e; src.stall = 0; } else src.stall += 1;
         fb = any && (!finite || src.stall >= c.stall_limit);
         if (fb) { src.fallback = 1; src.nonfinite = !finite; }
     }
@@ -660,6 +666,166 @@ __global__ void __launch_bounds__(256) k_E(T *V, T const *AU1, T const *AU2, Ctx
         v[0] += double(dr); v[1] += double(di);
     }
     double out[2];
+    if (reduce_source<2>(c, blockIdx.x, s, v, out)) step_alpha(c, s, out);
+}
+
+// ------------------------------------------------------------------ 16-byte vector kernels
+// K_A, K_C and K_E with 16-byte accesses (the scalar kernels above move 4 or 8 bytes per thread
+// and access): thread (row group rg, column group cg) owns N = 16/sizeof(T) consecutive columns
+// of RP rows of every block of its unit.  The column sums of the row groups are folded in a fixed
+// order into the (q, j) layout of reduce_source, so the results are reproducible.
+template <typename T> struct Lanes {
+    static constexpr int N = 16/int(sizeof(T));       // columns per thread
+    static constexpr int CG = 64/N, RG = 256/CG;       // column groups, row groups
+    static constexpr int RP = 64/RG;                   // rows per thread and block
+    T v[N];
+};
+template <typename T> __device__ __forceinline__ Lanes<T> ldl(T const *p) {
+    Lanes<T> r;
+    if constexpr (sizeof(T) == 4) { float4 const a = *reinterpret_cast<float4 const*>(p); r.v[0] = a.x; r.v[1] = a.y; r.v[2] = a.z; r.v[3] = a.w; }
+    else { double2 const a = *reinterpret_cast<double2 const*>(p); r.v[0] = a.x; r.v[1] = a.y; }
+    return r;
+}
+template <typename T> __device__ __forceinline__ void stl(T *p, Lanes<T> const &r) {
+    if constexpr (sizeof(T) == 4) *reinterpret_cast<float4*>(p) = make_float4(r.v[0], r.v[1], r.v[2], r.v[3]);
+    else *reinterpret_cast<double2*>(p) = make_double2(r.v[0], r.v[1]);
+}
+template <typename T> __device__ __forceinline__ Lanes<T> coefl(Ctx const &c, int i, uint32_t col) {
+    if constexpr (sizeof(T) == 4) return ldl<float>(c.cf + size_t(i)*c.ncol + col);
+    else return ldl<double>(c.cd + size_t(i)*c.ncol + col);
+}
+
+// a[n][k]: this thread's sums of its column n; v[k]: thread (q, j)'s share for reduce_source
+template <typename T, int NC>
+__device__ __forceinline__ void fold_lanes(double const (&a)[Lanes<T>::N][NC], double (&v)[NC]) {
+    using L = Lanes<T>;
+    __shared__ double sm[L::RG][64][NC];
+    int const cg = threadIdx.x % L::CG, rg = threadIdx.x/L::CG;
+#pragma unroll
+    for (int n = 0; n < L::N; ++n)
+#pragma unroll
+        for (int k = 0; k < NC; ++k) sm[rg][cg*L::N + n][k] = a[n][k];
+    __syncthreads();
+    int const j = threadIdx.x & 63, q = threadIdx.x >> 6;
+    constexpr int PER = L::RG/4;                       // row groups per q
+#pragma unroll
+    for (int k = 0; k < NC; ++k) {
+        double t = sm[q*PER][j][k];
+#pragma unroll
+        for (int r = 1; r < PER; ++r) t += sm[q*PER + r][j][k];
+        v[k] = t;
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256, 2) k_A16(T *U2, T const *U1, T const *V, T const *W, T const *AU1, Ctx const c) {
+    using L = Lanes<T>;
+    uint32_t s, lo, hi;
+    if (!unit_range(c, c.active, blockIdx.x, s, lo, hi)) return;
+    int const cg = threadIdx.x % L::CG, rg = threadIdx.x/L::CG, j0 = cg*L::N;
+    uint32_t const col = s*64 + j0;
+    L const ar = coefl<T>(c, 0, col), ai = coefl<T>(c, 1, col);
+    double a[L::N][1] = {};
+    for (uint32_t k = lo; k < hi; ++k) {
+        size_t const b = c.src_blocks[k];
+        T n2[L::N] = {};
+#pragma unroll 2
+        for (int i = rg*L::RP; i < rg*L::RP + L::RP; ++i) {
+            size_t const o = b*kBlk + i*64 + j0;
+            L const vr = ldl(V + o), vi = ldl(V + o + 4096), u1r = ldl(U1 + o), u1i = ldl(U1 + o + 4096);
+            L const ur = ldl(AU1 + o), ui = ldl(AU1 + o + 4096), wr = ldl(W + o), wi = ldl(W + o + 4096);
+            L u2r, u2i;
+#pragma unroll
+            for (int n = 0; n < L::N; ++n) {
+                u2r.v[n] = fma(ai.v[n], vi.v[n], fma(-ar.v[n], vr.v[n], u1r.v[n]));
+                u2i.v[n] = fma(-ai.v[n], vr.v[n], fma(-ar.v[n], vi.v[n], u1i.v[n]));
+                T const xr = fma(ai.v[n], ui.v[n], fma(-ar.v[n], ur.v[n], wr.v[n]));
+                T const xi = fma(-ai.v[n], ur.v[n], fma(-ar.v[n], ui.v[n], wi.v[n]));
+                n2[n] = fma(xr, xr, fma(xi, xi, n2[n]));
+            }
+            stl(U2 + o, u2r); stl(U2 + o + 4096, u2i);
+        }
+#pragma unroll
+        for (int n = 0; n < L::N; ++n) a[n][0] += double(n2[n]);
+    }
+    double v[1], out[1];
+    fold_lanes<T, 1>(a, v);
+    if (reduce_source<1>(c, blockIdx.x, s, v, out)) step_half1(c, s, out);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256, 2) k_C16(T *W, T const *AU1, T const *AU2, Ctx const c) {
+    using L = Lanes<T>;
+    uint32_t s, lo, hi;
+    if (!unit_range(c, c.active, blockIdx.x, s, lo, hi)) return;
+    int const cg = threadIdx.x % L::CG, rg = threadIdx.x/L::CG, j0 = cg*L::N;
+    uint32_t const col = s*64 + j0;
+    L const ar = coefl<T>(c, 0, col), ai = coefl<T>(c, 1, col);
+    double a[L::N][3] = {};
+    for (uint32_t k = lo; k < hi; ++k) {
+        size_t const b = c.src_blocks[k];
+        T n2[L::N] = {}, dr[L::N] = {}, di[L::N] = {};
+#pragma unroll 2
+        for (int i = rg*L::RP; i < rg*L::RP + L::RP; ++i) {
+            size_t const o = b*kBlk + i*64 + j0;
+            L const a1r = ldl(AU1 + o), a1i = ldl(AU1 + o + 4096), a2r = ldl(AU2 + o), a2i = ldl(AU2 + o + 4096);
+            L wr = ldl(W + o), wi = ldl(W + o + 4096);
+#pragma unroll
+            for (int n = 0; n < L::N; ++n) {
+                T const sr = a1r.v[n] + a2r.v[n], si = a1i.v[n] + a2i.v[n];
+                T const xr = fma(ai.v[n], si, fma(-ar.v[n], sr, wr.v[n]));
+                T const xi = fma(-ai.v[n], sr, fma(-ar.v[n], si, wi.v[n]));
+                wr.v[n] = xr; wi.v[n] = xi;
+                uint32_t const idx = uint32_t(o) + uint32_t(n);
+                T const tr = shadow_t<T>(c.seed, idx), ti = shadow_t<T>(c.seed, idx + 4096u);
+                n2[n] = fma(xr, xr, fma(xi, xi, n2[n]));
+                dr[n] = fma(tr, xr, fma(ti, xi, dr[n])); di[n] = fma(tr, xi, fma(-ti, xr, di[n]));
+            }
+            stl(W + o, wr); stl(W + o + 4096, wi);
+        }
+#pragma unroll
+        for (int n = 0; n < L::N; ++n) { a[n][0] += double(n2[n]); a[n][1] += double(dr[n]); a[n][2] += double(di[n]); }
+    }
+    double v[3], out[3];
+    fold_lanes<T, 3>(a, v);
+    if (reduce_source<3>(c, blockIdx.x, s, v, out)) step_half2(c, s, out);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256, 2) k_E16(T *V, T const *AU1, T const *AU2, Ctx const c) {
+    using L = Lanes<T>;
+    uint32_t s, lo, hi;
+    if (!unit_range(c, c.active, blockIdx.x, s, lo, hi)) return;
+    int const cg = threadIdx.x % L::CG, rg = threadIdx.x/L::CG, j0 = cg*L::N;
+    uint32_t const col = s*64 + j0;
+    L const fr = coefl<T>(c, 2, col), fi = coefl<T>(c, 3, col);
+    double a[L::N][2] = {};
+    for (uint32_t k = lo; k < hi; ++k) {
+        size_t const b = c.src_blocks[k];
+        T dr[L::N] = {}, di[L::N] = {};
+#pragma unroll 2
+        for (int i = rg*L::RP; i < rg*L::RP + L::RP; ++i) {
+            size_t const o = b*kBlk + i*64 + j0;
+            L vr = ldl(V + o), vi = ldl(V + o + 4096);
+            L const a1r = ldl(AU1 + o), a1i = ldl(AU1 + o + 4096), a2r = ldl(AU2 + o), a2i = ldl(AU2 + o + 4096);
+#pragma unroll
+            for (int n = 0; n < L::N; ++n) {
+                T const t1r = fma(-fi.v[n], vi.v[n], fma(fr.v[n], vr.v[n], a2r.v[n]));
+                T const t1i = fma(fi.v[n], vr.v[n], fma(fr.v[n], vi.v[n], a2i.v[n]));
+                T const sr = fma(-fi.v[n], t1i, fma(fr.v[n], t1r, a1r.v[n]));
+                T const si = fma(fi.v[n], t1r, fma(fr.v[n], t1i, a1i.v[n]));
+                vr.v[n] = sr; vi.v[n] = si;
+                uint32_t const idx = uint32_t(o) + uint32_t(n);
+                T const tr = shadow_t<T>(c.seed, idx), ti = shadow_t<T>(c.seed, idx + 4096u);
+                dr[n] = fma(tr, sr, fma(ti, si, dr[n])); di[n] = fma(tr, si, fma(-ti, sr, di[n]));
+            }
+            stl(V + o, vr); stl(V + o + 4096, vi);
+        }
+#pragma unroll
+        for (int n = 0; n < L::N; ++n) { a[n][0] += double(dr[n]); a[n][1] += double(di[n]); }
+    }
+    double v[2], out[2];
+    fold_lanes<T, 2>(a, v);
     if (reduce_source<2>(c, blockIdx.x, s, v, out)) step_alpha(c, s, out);
 }
 
@@ -892,9 +1058,9 @@ bool prepare(DevicePlan &dp, SolverWorkspace &ws, a43g_solve_options_t const &op
     c.retire = retire ? 1 : 0;
     c.stall_limit = 3;
     {
-        // experiment switch: the gap rule above (off by default)
-        char const *g = std::getenv("A43G_STALL_GAP");
-        c.stall_gap = g ? std::atof(g) : 0.0;
+        // vector kernels with 16-byte accesses (default) or the scalar ones ("0")
+        char const *v = std::getenv("A43G_VEC16");
+        c.vec16 = (v && 0 == std::strcmp(v, "0")) ? 0 : 1;
     }
     c.abs_tol = 0;
     p.units = units;
@@ -951,10 +1117,12 @@ bool run(DevicePlan &dp, SolverWorkspace &ws, TfqmrVectors &v, Prepared &p, T *X
     }
     count_launch();
     auto iteration = [&]() -> bool {
-        k_A<T><<<p.units, 256, 0, st>>>(U2, U1, V, W, AU1, c);
+        if (c.vec16) k_A16<T><<<p.units, 256, 0, st>>>(U2, U1, V, W, AU1, c);
+        else k_A<T><<<p.units, 256, 0, st>>>(U2, U1, V, W, AU1, c);
         count_launch();
         if (!apply<T>(dp, AU2, U2, nullptr, retire, st)) return false;
-        k_C<T><<<p.units, 256, 0, st>>>(W, AU1, AU2, c);
+        if (c.vec16) k_C16<T><<<p.units, 256, 0, st>>>(W, AU1, AU2, c);
+        else k_C<T><<<p.units, 256, 0, st>>>(W, AU1, AU2, c);
         count_launch();
         if constexpr (sizeof(T) == 4) k_DX32<<<p.units, 256, 0, st>>>(X, D, U1, U2, W, c);
         else k_DX<T><<<p.units, 256, 0, st>>>(X, D, U1, U2, W, c);
@@ -974,7 +1142,8 @@ bool run(DevicePlan &dp, SolverWorkspace &ws, TfqmrVectors &v, Prepared &p, T *X
             }
         }
         if (!apply<T>(dp, AU1, U1, nullptr, retire, st)) return false;
-        k_E<T><<<p.units, 256, 0, st>>>(V, AU1, AU2, c);
+        if (c.vec16) k_E16<T><<<p.units, 256, 0, st>>>(V, AU1, AU2, c);
+        else k_E<T><<<p.units, 256, 0, st>>>(V, AU1, AU2, c);
         count_launch();
         return true;
     };

@@ -256,3 +256,22 @@ def test_solve_traced_error_of_G():
                                             max_iterations=2000)
     assert st3["converged"] and len(tr3) >= 2
     assert np.all(np.diff(tr3[:-1, 0]) == 5) and tr3[0, 1] > 1e-3 and tr3[-1, 1] < 1e-6
+
+
+@pytest.mark.parametrize("precision", ["float64", "float32"])
+def test_vector_kernels_16_byte_and_scalar_agree(precision, monkeypatch):
+    """The tfQMR vector kernels with 16-byte accesses (the default) and the scalar ones
+    (A43G_VEC16=0) give the same densities to the tolerance of the solve."""
+    w = workloads.make("periodic4_1atom")
+    out = []
+    for flag in ("1", "0"):
+        monkeypatch.setenv("A43G_VEC16", flag)
+        p = gf.construct_Green_function(w.geometry)
+        gf.update_potential(p, w.Vcell, w.mats, w.offsets, layout="cells")
+        gf.update_energy_parameter(p, complex(-0.3, 0.1), w.dVol)
+        gf.update_phases(p, np.array([0.1, 0.0, 0.2]))
+        st, rho = green_action.solve(p, stream=torch.cuda.Stream(), tolerance=1e-10, max_iterations=2000,
+                                     precision=precision, check_every=1)
+        assert st["converged"], (flag, st)
+        out.append(rho)
+    assert np.abs(out[0] - out[1]).max() <= 1e-8 * np.abs(out[1]).max()
