@@ -1306,6 +1306,9 @@ sho_atom_kernel(T *__restrict__ cad, T const *__restrict__ apc, uint32_t nrhs,
                 uint32_t const *__restrict__ mat_off, int use_phase, DyadicPairs const bp)
 {
     __shared__ double sre[kAtomRows][32], sim[kAtomRows][32];
+    constexpr int kImg = 32;                          // images of the atom staged in shared memory
+    __shared__ uint32_t simg[kImg];
+    __shared__ double sph[kImg][2];
     int const A = blockIdx.x, s = blockIdx.y, half = blockIdx.z;
     int const j = threadIdx.x & 31, g = threadIdx.x >> 5, col = half*32 + j;
     if (bp.active && !bp.active[s]) return;
@@ -1313,14 +1316,26 @@ sho_atom_kernel(T *__restrict__ cad, T const *__restrict__ apc, uint32_t nrhs,
     mats += (s/bp.nsrc_pair)*bp.mat_stride;
     int const nc = nsho_c(atom_lmax[A]);
     uint32_t const k0 = sum_start[A], k1 = sum_start[A + 1];
+    // the atom's images (their coefficient start and phase) once, instead of a chain of three
+    // dependent loads per row and image
+    for (uint32_t k = k0 + threadIdx.x; k < k1 && k < k0 + kImg; k += blockDim.x) {
+        uint32_t const i = sum_col[k];
+        simg[k - k0] = img_starts[i];
+        sph[k - k0][0] = img_phase[4*i]; sph[k - k0][1] = img_phase[4*i + 1];
+    }
+    __syncthreads();
+    auto image = [&](uint32_t k, uint32_t &start, double &pr, double &pi) {
+        if (k - k0 < uint32_t(kImg)) { start = simg[k - k0]; pr = sph[k - k0][0]; pi = sph[k - k0][1]; }
+        else { uint32_t const i = sum_col[k]; start = img_starts[i]; pr = img_phase[4*i]; pi = img_phase[4*i + 1]; }
+    };
     for (int c = g; c < nc; c += 4) {
         double re = 0, im = 0;
         for (uint32_t k = k0; k < k1; ++k) {
-            uint32_t const i = sum_col[k];
-            T const *src = apc + ((size_t(img_starts[i]) + c)*nrhs + s)*128;
+            uint32_t start; double pr, pi;
+            image(k, start, pr, pi);
+            T const *src = apc + ((size_t(start) + c)*nrhs + s)*128;
             double const xr = double(src[col]), xi = double(src[64 + col]);
             if (use_phase) {
-                double const pr = img_phase[4*i], pi = img_phase[4*i + 1];
                 re += pr*xr - pi*xi;
                 im += pr*xi + pi*xr;
             } else {
@@ -1340,10 +1355,11 @@ sho_atom_kernel(T *__restrict__ cad, T const *__restrict__ apc, uint32_t nrhs,
             im += mr*xi + mi*xr;
         }
         for (uint32_t k = k0; k < k1; ++k) {
-            uint32_t const i = sum_col[k];
-            T *dst = cad + ((size_t(img_starts[i]) + r)*nrhs + s)*128;
+            uint32_t start; double pr, pi;
+            image(k, start, pr, pi);
+            pi = -pi;
+            T *dst = cad + ((size_t(start) + r)*nrhs + s)*128;
             if (use_phase) {
-                double const pr = img_phase[4*i], pi = -img_phase[4*i + 1];
                 dst[col] = T(pr*re - pi*im);
                 dst[64 + col] = T(pr*im + pi*re);
             } else {
