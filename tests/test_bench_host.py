@@ -15,8 +15,9 @@ def load_bench():
 
 def test_traffic_table_has_the_local_kernels():
     b = load_bench()
-    assert b.read_traffic("local_pencil_kernel_f32") == 65234
+    assert b.read_traffic("local_pencil_kernel_f32") == 66275
     assert b.read_traffic("local_fused_pf_kernel_f32") == 70326
+    assert b.read_traffic("local_pencil64_kernel_f64") == 159058
     assert b.read_traffic("no_such_kernel") is None
 
 
