@@ -20,7 +20,9 @@
 //    or after update_gap iterations.  The CGS-type recurrences of tfQMR amplify the FP32
 //    rounding strongly where the energy lies close to the spectrum: a source cube whose largest
 //    true residual has not halved over stall_limit replacements (or is not finite) leaves the FP32
-//    recurrences, and all such sources then continue as FP64 tfQMR from their FP64 solution.
+//    recurrences, and all such sources then continue as FP64 tfQMR from their FP64 solution
+//    (on A d = B - A X64, to half the tolerance; sources whose true residual is then still above
+//    the tolerance restart from their solution, at most kRestarts times).
 //
 // One iteration = two operator applications.  The BLAS-1 work is fused so that every vector
 // is streamed as few times as possible:
@@ -30,6 +32,8 @@
 //   K_E   V  = AU1 + b (AU2 + b V)      and rt^H V
 // (U1 = y_{2n-1}, U2 = y_{2n}, AU1 = A y_{2n-1}, AU2 = A y_{2n}, V = v_{n-1} in Freund's
 // notation).  The shadow residual rt is a counter-based random vector regenerated on the fly.
+// K_A, K_C and K_E move 16 bytes per thread and access (K_A16 ...; K_DX32 in the FP32
+// recurrences); the scalar kernels remain as alternatives.
 //
 // Work units and reductions: every vector kernel runs one CTA per (source cube, chunk of its
 // blocks); the column sums of a unit go to a slot of their own, and the last CTA of a source to
