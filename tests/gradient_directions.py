@@ -10,7 +10,7 @@ The gradient is the backward pass of tests/green_autograd.py (adjoint solves at 
 vector-Jacobian products of a43g_vjp); each finite difference takes 16 FP64 solves to 1e-12.
 Steps: 1e-5 Ha for V, H and S (H and S directions symmetric, every atom's matrices at once),
 1e-4 Bohr for R (with the projection radius at 8 sigma, so that no grid point crosses the
-cut-off sphere by a visible jump).  A standalone GPU script (a few minutes on a B200), not a
+cut-off sphere by a visible jump).  A standalone GPU script (about 15 minutes on a B200), not a
 pytest case:
 
     python tests/gradient_directions.py > gradient_directions.log
