@@ -480,6 +480,9 @@ def measure_kernels(plan, stream, out, hbm, bf16, peak_kind):
                        "traffic": traffic * nnzb if traffic is not None else None}
     t_dyadic = time_part(_lib, plan, 1, _lib.A43G_F32, x, y, 10, stream)
     nsho = 56
+    L = 5
+    sf_flops = 2.0 * 2 * (64 * (L + 1) + 16 * (L + 1) * (L + 2) // 2 + 4 * nsho) * 128 * plan.sizes["SHOadd_nnz"]
+    fma_peak = 148 * 128 * 2 * 1.965 / 1e3    # TFLOP/s: SMs x FP32 lanes x 2 flops x GHz
     flops = 4.0 * nsho * 64 * 128 * plan.sizes["SHOadd_nnz"]
     tf32_peak = bf16 / 2
     tc = os.environ.get("A43G_PROJECTOR", "") == "tc"
@@ -490,7 +493,13 @@ def measure_kernels(plan, stream, out, hbm, bf16, peak_kind):
                                  "unit": "TFLOP/s", "frac": flops / t_dyadic / 1e12 / tf32_peak,
                                  "peak_kind": "dense TF32 = half of the %s bf16 peak" % peak_kind,
                                  "algorithmic_flops_per_launch": flops, "ms_per_launch": t_dyadic * 1e3,
-                                 "note": "flops of the dense contraction P (64 x 64 per block and image) x X (64 x 128)"}
+                                 "note": "flops of the dense contraction P (64 x 64 per block and image) x X (64 x 128)",
+                                 # the kernels do the sum-factorized work: 64 (L+1) + 16 (L+1)(L+2)/2 + 4 nSHO
+                                 # FMAs per column and (image, block) pair, for the projection and the addition
+                                 "sum_factorized_flops_per_launch": sf_flops,
+                                 "sum_factorized_tflops": sf_flops / t_dyadic / 1e12,
+                                 "fp32_fma_peak_tflops": fma_peak,
+                                 "fp32_fma_frac": sf_flops / t_dyadic / 1e12 / fma_peak}
     x64 = torch.randn((nnzb, 2, 64, 64), device="cuda", dtype=torch.float64)
     y64 = torch.empty_like(x64)
     del x, y
