@@ -14,6 +14,7 @@
 #ifndef A43G_H
 #define A43G_H
 
+#include <stddef.h>
 #include <stdint.h>
 
 #ifdef __cplusplus
@@ -86,7 +87,7 @@ typedef struct {
                                  solution, convergence checked on the FP64 residual (residual replacement) */
     double   update_factor;   /* A43G_F32: a source cube replaces its residual when its largest estimate has
                                  fallen by this factor since its last replacement (0: default 0.1) */
-    int32_t  update_gap;      /* A43G_F32: at most this many iterations between replacements (0: default 50) */
+    int32_t  update_gap;      /* A43G_F32: at most this many iterations between replacements (0: default 10) */
     int32_t  check_every;     /* iterations between convergence checks on the host */
     uint64_t seed;            /* seed of the random shadow residual */
     int32_t  echo;            /* log level: > 0 prints one line per solve, > 1 one per convergence check */
