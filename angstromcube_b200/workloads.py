@@ -72,13 +72,16 @@ def _potential_cells(ng, hg, centres, depth, width, noise, rng):
     ng = np.asarray(ng); hg = np.asarray(hg, dtype=np.float64)
     L = ng * hg
     axes = [(np.arange(ng[d]) - ng[d] / 2 + 0.5) * hg[d] for d in range(3)]
-    Z, Y, X = np.meshgrid(axes[2], axes[1], axes[0], indexing="ij")
-    V = np.zeros(Z.shape)
-    for c in centres:
-        dx = X - c[0]; dx -= L[0] * np.round(dx / L[0])
-        dy = Y - c[1]; dy -= L[1] * np.round(dy / L[1])
-        dz = Z - c[2]; dz -= L[2] * np.round(dz / L[2])
-        V += depth * np.exp(-(dx * dx + dy * dy + dz * dz) / (2 * width * width))
+    # the Gaussians are separable: per centre and direction the 1D factor of the minimum-image
+    # distance, then V[z, y, x] = depth * sum_c gz[c, z] gy[c, y] gx[c, x] as one matrix product
+    c = np.asarray(centres, dtype=np.float64).reshape(-1, 3)
+    g = []
+    for d in range(3):
+        dd = axes[d][None, :] - c[:, d:d + 1]
+        dd -= L[d] * np.round(dd / L[d])
+        g.append(np.exp(-(dd * dd) / (2 * width * width)))
+    gzy = (g[2][:, :, None] * g[1][:, None, :]).reshape(len(c), -1)          # [c, z*y]
+    V = depth * (gzy.T @ g[0]).reshape(ng[2], ng[1], ng[0])
     V += rng.uniform(-noise, noise, size=V.shape)
     nb = ng // 4
     # [iz, iy, ix] -> [bz, i4z, by, i4y, bx, i4x] -> cells (bz, by, bx) x points (i4z, i4y, i4x)
