@@ -6,9 +6,10 @@ residual |B - A X| / |B| of the FP32 iterate is computed with the reference's FP
 printed beside the recurrence's own estimate (tfQMR: its QMR bound tau sqrt(m + 1); BiCGStab:
 its recursive residual).  Where the true residual stops while the estimate keeps falling, the
 recurrence has lost accuracy: the floor that residual replacement and the FP64 continuation of
-the mixed solver work around.  No GPU; about a minute:
+the mixed solver work around.  With --variants: tfQMR with only the action or only the
+vectors in FP32.  No GPU; a minute or two:
 
-    python tests/fp32_floor_emulation.py
+    python tests/fp32_floor_emulation.py [--variants]
 """
 import json
 import os
@@ -46,10 +47,14 @@ def to_c(x):
     return x[:, 0] + 1j * x[:, 1]
 
 
-def run(kind, maxit=300):
+def run(kind, maxit=300, vec=np.complex64, op32=True):
+    """kind "tfqmr" or "bicgstab"; vec: the vectors' type; op32: the FP32 (else FP64) action."""
     r, ci, ncols, B = setup()
-    A32 = lambda z: to_c(r.action(to_r(z, np.float32))).astype(np.complex64)
     A64 = lambda z: to_c(r.action(to_r(z, np.float64)))
+    if op32:
+        A32 = lambda z: to_c(r.action(to_r(z, np.float32))).astype(vec)
+    else:
+        A32 = lambda z: A64(z).astype(vec)
 
     def dot(a, b):                          # per column, FP64 accumulation
         out = np.zeros((ncols, 64), np.complex128)
@@ -57,15 +62,15 @@ def run(kind, maxit=300):
         return out
 
     def col(s):
-        return s[ci][:, None, :].astype(np.complex64)
+        return s[ci][:, None, :].astype(vec)
 
     def true_res(X):
         R = B - A64(X.astype(np.complex128))
         return float(np.sqrt(dot(R, R).real).max())      # |b| = 1 per column
 
     rng = np.random.default_rng(7)
-    rt = (rng.uniform(-1, 1, B.shape) + 1j * rng.uniform(-1, 1, B.shape)).astype(np.complex64)
-    b32 = B.astype(np.complex64)
+    rt = (rng.uniform(-1, 1, B.shape) + 1j * rng.uniform(-1, 1, B.shape)).astype(vec)
+    b32 = B.astype(vec)
     X = np.zeros_like(b32)
     hist = []
     if kind == "tfqmr":
@@ -113,6 +118,16 @@ def run(kind, maxit=300):
 
 
 if __name__ == "__main__":
+    if "--variants" in sys.argv:
+        # which rounding sets the floor: FP64 vectors with the FP32 action, FP32 vectors with the
+        # FP64 action, everything FP64
+        for name, vec, op32 in (("fp64 vectors, fp32 action", np.complex128, True),
+                                ("fp32 vectors, fp64 action", np.complex64, False),
+                                ("fp64 vectors, fp64 action", np.complex128, False)):
+            h = run("tfqmr", vec=vec, op32=op32)
+            print(json.dumps({"variant": name, "floor": min(t for _, t, _ in h),
+                              "history": [(it, tr) for it, tr, _ in h]}), flush=True)
+        sys.exit(0)
     out = {}
     for kind in ("tfqmr", "bicgstab"):
         h = run(kind)
