@@ -53,6 +53,7 @@ class PlanExport(ctypes.Structure):
 
 
 A43G_SOLVE_NO_RETIRE = 1
+A43G_SOLVE_PRECONDITION = 2
 
 
 class SolveOptions(ctypes.Structure):

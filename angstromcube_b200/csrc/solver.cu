@@ -1086,6 +1086,18 @@ bool apply(DevicePlan &dp, T *y, T const *x, uint8_t const *sel, bool retire, cu
     return ok;
 }
 
+// the solver's operator: A, or A M^-1 with the cube-diagonal preconditioner from the right
+// (M^-1 x into the workspace's scratch of the precision, on the same sources)
+template <typename T>
+bool apply_op(DevicePlan &dp, SolverWorkspace &ws, T *y, T const *x, uint8_t const *sel, bool retire,
+              cudaStream_t st) {
+    if (!ws.use_pc) return apply<T>(dp, y, x, sel, retire, st);
+    T *t = (sizeof(T) == 8) ? reinterpret_cast<T*>(ws.PT64.ptr) : reinterpret_cast<T*>(ws.PT32.ptr);
+    uint8_t const *act = sel ? sel : (retire ? dptr<uint8_t>(dp.src_active) : nullptr);
+    if (!precond_apply<T>(dp, ws.pc, t, x, act, st)) return false;
+    return apply<T>(dp, y, t, sel, retire, st);
+}
+
 struct Result { int iterations = 0; double applications = 0; };
 
 // tfQMR on vectors of precision T whose W, U1 hold B and D, X are zero; mixed: X is X32 and the
@@ -1111,7 +1123,7 @@ bool run(DevicePlan &dp, SolverWorkspace &ws, TfqmrVectors &v, Prepared &p, T *X
     A43G_CUDA_TRY(cudaMemsetAsync(ws.tickets.ptr, 0, size_t(nsrc)*sizeof(uint32_t), st));
     A43G_CUDA_TRY(cudaMemcpyAsync(dp.src_active.ptr, mask.data(), nsrc, cudaMemcpyHostToDevice, st));
     // V = A U1
-    if (!apply<T>(dp, AU1, U1, nullptr, retire, st)) return false;
+    if (!apply_op<T>(dp, ws, AU1, U1, nullptr, retire, st)) return false;
     A43G_CUDA_TRY(cudaMemcpyAsync(V, AU1, v.n*sizeof(T), cudaMemcpyDeviceToDevice, st));
     res.applications += 1;
     {   // the sources outside the mask are skipped by the initial reductions too
@@ -1124,7 +1136,7 @@ bool run(DevicePlan &dp, SolverWorkspace &ws, TfqmrVectors &v, Prepared &p, T *X
         if (c.vec16) k_A16<T><<<p.units, 256, 0, st>>>(U2, U1, V, W, AU1, c);
         else k_A<T><<<p.units, 256, 0, st>>>(U2, U1, V, W, AU1, c);
         count_launch();
-        if (!apply<T>(dp, AU2, U2, nullptr, retire, st)) return false;
+        if (!apply_op<T>(dp, ws, AU2, U2, nullptr, retire, st)) return false;
         if (c.vec16) k_C16<T><<<p.units, 256, 0, st>>>(W, AU1, AU2, c);
         else k_C<T><<<p.units, 256, 0, st>>>(W, AU1, AU2, c);
         count_launch();
@@ -1137,15 +1149,15 @@ bool run(DevicePlan &dp, SolverWorkspace &ws, TfqmrVectors &v, Prepared &p, T *X
                 // sources' units return at once)
                 k_flush<<<p.units, 256, 0, st>>>(X64, X, c, c.upd);
                 count_launch();
-                if (!apply<double>(dp, AX64, X64, c.upd, retire, st)) return false;
-                if (!apply<float>(dp, AU1, D, c.upd, retire, st)) return false;    // A d (AU1 is free here)
+                if (!apply_op<double>(dp, ws, AX64, X64, c.upd, retire, st)) return false;
+                if (!apply_op<float>(dp, ws, AU1, D, c.upd, retire, st)) return false;    // A d (AU1 is free here)
                 k_replace<<<p.units, 256, 0, st>>>(W, AX64, AU1, c);
                 count_launch();
                 k_U1<<<p.units, 256, 0, st>>>(U1, W, U2, c);
                 count_launch();
             }
         }
-        if (!apply<T>(dp, AU1, U1, nullptr, retire, st)) return false;
+        if (!apply_op<T>(dp, ws, AU1, U1, nullptr, retire, st)) return false;
         if (c.vec16) k_E16<T><<<p.units, 256, 0, st>>>(V, AU1, AU2, c);
         else k_E<T><<<p.units, 256, 0, st>>>(V, AU1, AU2, c);
         count_launch();
@@ -1246,11 +1258,13 @@ bool ensure_vectors(SolverWorkspace &ws, DevicePlan &dp, bool mixed) {
 
 } // namespace
 
-size_t solve_bytes(DevicePlan const &dp, int precision) {
+size_t solve_bytes(DevicePlan const &dp, int precision, bool precondition) {
     // FP64: X64 and 7 recurrence vectors; FP32: 8 FP32 vectors, X64 and AX64, or, for sources
-    // continued in FP64, X64 and 7 FP64 vectors (the larger of the two)
+    // continued in FP64, X64 and 7 FP64 vectors (the larger of the two); the preconditioner's
+    // scratch: one vector of each precision in use
     size_t const n = size_t(dp.nnzb)*kBlk;
-    return (A43G_F32 == precision) ? n*std::max(8*4 + 2*8, 8 + 7*8) : n*(8*8);
+    size_t const pc = precondition ? ((A43G_F32 == precision) ? n*(8 + 4) : n*8) : 0;
+    return pc + ((A43G_F32 == precision) ? n*std::max(8*4 + 2*8, 8 + 7*8) : n*(8*8));
 }
 
 int solve(GreenPlan &hp, DevicePlan &dp, SolverWorkspace &ws, a43g_solve_options_t const &opt,
@@ -1271,6 +1285,14 @@ int solve(GreenPlan &hp, DevicePlan &dp, SolverWorkspace &ws, a43g_solve_options
     std::fill(mask.begin(), mask.begin() + live, uint8_t(1));
     if (!ensure_vectors(ws, dp, mixed)) return A43G_ERR_MEMORY;
     if (trace && (!trace->Xref || !ws.trace_sums.alloc(16))) return trace->Xref ? A43G_ERR_MEMORY : A43G_ERR_ARGUMENT;
+    // right preconditioning: the recurrences see A M^-1 and the solution is M^-1 of theirs
+    ws.use_pc = 0 != (opt.flags & A43G_SOLVE_PRECONDITION);
+    if (ws.use_pc) {
+        if (trace) { set_error("a traced solve takes no preconditioner"); return A43G_ERR_UNSUPPORTED; }
+        size_t const nr = size_t(dp.nnzb)*kBlk;
+        if (!ws.PT64.alloc(nr*8) || (mixed && !ws.PT32.alloc(nr*4))) return A43G_ERR_MEMORY;
+        if (!precond_setup(hp, dp, ws.pc, st)) return A43G_ERR_CUDA;
+    }
     // projector scratch for both precisions before the iteration is captured (no allocation
     // may happen inside a stream capture)
     if (!ensure_dyadic_scratch(dp, 8) || !ensure_prj_part(dp, 8)) return A43G_ERR_MEMORY;
@@ -1330,7 +1352,7 @@ int solve(GreenPlan &hp, DevicePlan &dp, SolverWorkspace &ws, a43g_solve_options
             for (int restart = 0; ; ++restart) {
                 // A X64 of the continuing sources (their blocks only) into AU1
                 A43G_CUDA_TRY_RC(cudaMemcpyAsync(dp.src_active.ptr, cont.data(), nsrc, cudaMemcpyHostToDevice, st));
-                if (!apply<double>(dp, dptr<double>(w.AU1), X64, nullptr, true, st)) return A43G_ERR_CUDA;
+                if (!apply_op<double>(dp, ws, dptr<double>(w.AU1), X64, nullptr, true, st)) return A43G_ERR_CUDA;
                 res.applications += 1;
                 if (restart > 0) {
                     // the true residual of each source the last run finished: sources still above
@@ -1390,6 +1412,10 @@ int solve(GreenPlan &hp, DevicePlan &dp, SolverWorkspace &ws, a43g_solve_options
         trace->rows.push_back(double(res.iterations));
         trace->rows.push_back(q[1] > 0 ? std::sqrt(q[0]/q[1]) : 0.0);
         trace->rows.push_back(0.0);
+    }
+    if (ws.use_pc) {
+        // the solution of the original system: X = M^-1 Y (in place, every block)
+        if (!precond_apply<double>(dp, ws.pc, X64, X64, nullptr, st)) return A43G_ERR_CUDA;
     }
     // true residual of every column's FP64 solution (the whole operator, no source skipped), in
     // whichever FP64 scratch the solve holds
@@ -1481,8 +1507,9 @@ int solve_batched(GreenPlan &hp, DevicePlan &dp, BatchCache &bc, a43g_solve_opti
         // as many pairs as fit 85 % of the free memory next to what the batch plan holds already
         size_t freeb = 0, total = 0;
         if (cudaSuccess != cudaMemGetInfo(&freeb, &total)) { set_error("cudaMemGetInfo"); return A43G_ERR_CUDA; }
-        size_t const held = bc.npairs ? solve_bytes(*bc.dev, opt.precision) : 0;
-        size_t const per = solve_bytes(dp, opt.precision) + size_t(dp.nnzb)*kBlk*2 + (size_t(64) << 20);
+        bool const pcf = 0 != (opt.flags & A43G_SOLVE_PRECONDITION);
+        size_t const held = bc.npairs ? solve_bytes(*bc.dev, opt.precision, pcf) : 0;
+        size_t const per = solve_bytes(dp, opt.precision, pcf) + size_t(dp.nnzb)*kBlk*2 + (size_t(64) << 20);
         wave = uint32_t(std::max<size_t>(1, (size_t(0.85*double(freeb + held)))/per));
     }
     wave = std::min<uint32_t>(wave, uint32_t(n));

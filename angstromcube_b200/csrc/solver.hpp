@@ -2,6 +2,7 @@
 #pragma once
 
 #include "device.cuh"
+#include "precond.hpp"
 #include "../../include/a43g.h"
 
 #include <memory>
@@ -23,6 +24,9 @@ struct SolverWorkspace {
     DeviceBuffer state;              // per-column and per-source scalars, control block (solver.cu)
     DeviceBuffer part, tickets;      // fixed-order column reductions
     DeviceBuffer trace_sums;         // |X - Xref|^2 and |Xref|^2 of a traced solve
+    BlockPreconditioner pc;          // cube-diagonal preconditioner (A43G_SOLVE_PRECONDITION)
+    bool use_pc = false;
+    DeviceBuffer PT64, PT32;         // M^-1 x ahead of the operator
     void *host_ctl = nullptr;        // pinned copy of the control block
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     ~SolverWorkspace();
@@ -52,7 +56,7 @@ struct BatchCache {
 };
 
 // peak device bytes of the solver vectors of one solve of this plan in the given precision
-size_t solve_bytes(DevicePlan const &dp, int precision);
+size_t solve_bytes(DevicePlan const &dp, int precision, bool precondition = false);
 
 int solve(GreenPlan &hp, DevicePlan &dp, SolverWorkspace &ws, a43g_solve_options_t const &opt,
           void *X, double *rho, a43g_solve_stats_t *stats, cudaStream_t st, SourceStats *per_source = nullptr,

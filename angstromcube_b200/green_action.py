@@ -46,12 +46,13 @@ class action_t:
 
 
 def solve_options(tolerance=1e-9, max_iterations=500, precision="float64", update_factor=0.0, update_gap=0,
-                  check_every=10, seed=1, echo=0, retire=True, batch=0):
+                  check_every=10, seed=1, echo=0, retire=True, batch=0, precondition=False):
     """Options of a43g_solve (include/a43g.h): precision "float64" is plain FP64 tfQMR,
     "float32" the FP32 recurrences with the FP64 solution and residual replacement (a
     replacement when a source's estimate fell by update_factor or after update_gap iterations;
     0 takes the library defaults 0.1 and 10); retire=False keeps computing on finished source
-    cubes (as the reference's solver library does); batch: pairs per wave of solve_batched."""
+    cubes (as the reference's solver library does); batch: pairs per wave of solve_batched;
+    precondition: right preconditioning by the cube-diagonal local operator (A43G_SOLVE_PRECONDITION)."""
     o = _lib.SolveOptions()
     o.tolerance = tolerance
     o.max_iterations = max_iterations
@@ -61,7 +62,7 @@ def solve_options(tolerance=1e-9, max_iterations=500, precision="float64", updat
     o.check_every = check_every
     o.seed = seed
     o.echo = echo
-    o.flags = 0 if retire else _lib.A43G_SOLVE_NO_RETIRE
+    o.flags = (0 if retire else _lib.A43G_SOLVE_NO_RETIRE) | (_lib.A43G_SOLVE_PRECONDITION if precondition else 0)
     o.batch = batch
     return o
 

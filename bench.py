@@ -37,6 +37,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 WORKLOAD = "periodic16_64atoms_s2x2x2"
+PRECONDITION = True          # our solver: right preconditioning by the cube-diagonal local operator
 TOLERANCE = 1e-8
 MAX_ITERATIONS = 1500
 STRIDE = 37            # walk of the 128 pairs: 37*i mod 128 (37 is coprime with 128)
@@ -358,7 +359,8 @@ def our_arm(a):
     stream = torch.cuda.Stream()
     # schedule of the FP32 action chosen by timing, outside the timed region
     tune_report = green_action.autotune(plan, "float32", stream)
-    opts = dict(tolerance=TOLERANCE, max_iterations=MAX_ITERATIONS, precision="float32", check_every=1)
+    opts = dict(tolerance=TOLERANCE, max_iterations=MAX_ITERATIONS, precision="float32", check_every=1,
+                precondition=PRECONDITION)
     order = pair_order(len(pairs))
     nsteps_total = a.warmup + a.steps
 
@@ -450,6 +452,7 @@ def our_arm(a):
                           "cell_cubes": [16, 16, 16], "sources": plan.nCols, "rhs_columns": plan.nCols * 64,
                           "atoms": w.natoms, "numax": 5, "nnzb_per_pair": plan.nnzb, "one_plan_for_all_radii": one_plan,
                           "wave": a.wave, "pairs_timed": len(per_pair), "max_iterations": MAX_ITERATIONS,
+                          "preconditioner": "cube-diagonal local operator, from the right" if PRECONDITION else None,
                           "parallelism": "dp%d ((E, k) pairs per rank)" % world,
                           "l2": "inputs larger than L2 (%.2f GB per FP32 vector and pair)" % (plan.nnzb * 32768 / 1e9)},
                "solve": {"converged": int(conv.item()), "pairs": len(per_pair) * world, "wall_s_per_step": wall / a.steps,
@@ -516,6 +519,7 @@ def fp64_plain(plan, w, pairs, sel, stream, opts):
     from angstromcube_b200 import green_action, green_function as gf
     o64 = dict(opts)
     o64["precision"] = "float64"
+    o64["precondition"] = False               # the reference's solver has no preconditioner
     res = []
     for i in sel:
         E, k = pairs[i][0], pairs[i][1]
@@ -553,7 +557,8 @@ def full_contour(a):
     plan.upload()
     stream = torch.cuda.Stream()
     green_action.autotune(plan, "float32", stream)
-    opts = dict(tolerance=TOLERANCE, max_iterations=MAX_ITERATIONS, precision="float32", check_every=1)
+    opts = dict(tolerance=TOLERANCE, max_iterations=MAX_ITERATIONS, precision="float32", check_every=1,
+                precondition=PRECONDITION)
     Es = [p[0] for p in pairs]
     Ks = [p[1] for p in pairs]
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -753,8 +758,10 @@ def main():
                              "mixed_same_pairs": {"solves_per_s": cmx / tmx, "seconds": tmx, "converged": cmx,
                                                   "iterations": [r[1] for r in rmx]},
                              "speedup_mixed_vs_fp64": (cmx / tmx) / (c64 / t64) if c64 and cmx else None,
-                             "what": "the same (E, k) pairs: plain FP64 tfQMR without retirement, one pair at a "
-                                     "time, against the mixed solver one pair per wave"}
+                             "what": "the same (E, k) pairs: plain FP64 tfQMR without retirement or preconditioner "
+                                     "(the reference's algorithm), one pair at a time, against our solver (mixed "
+                                     "precision, retirement%s) one pair per wave" % (
+                                         ", cube-diagonal preconditioner" if PRECONDITION else "")}
         if world == 1 and not a.no_cpu:
             from oracle import ref_available
             if ref_available():

@@ -76,8 +76,14 @@ typedef struct {
 
 /* Solver options and per-solve statistics (tfQMR, Freund 1993, per-column scalars) */
 enum {
-    A43G_SOLVE_NO_RETIRE = 1  /* FP64 solves: keep computing on finished source cubes (the reference's
-                                 tfQMRgpu does); FP32 recurrences always retire them */
+    A43G_SOLVE_NO_RETIRE = 1,    /* FP64 solves: keep computing on finished source cubes (the reference's
+                                    tfQMRgpu does); FP32 recurrences always retire them */
+    A43G_SOLVE_PRECONDITION = 2  /* right preconditioning by the cube-diagonal local operator: M^-1 of
+                                    the finite-difference kinetic energy inside each 4x4x4 cube plus its
+                                    mean potential minus E, applied by three 4-point transforms and a
+                                    scaling (no reference counterpart: the reference's action reports
+                                    has_preconditioner() false); residuals and the solution are those
+                                    of the original system.  Not with a43g_solve_traced */
 };
 
 typedef struct {

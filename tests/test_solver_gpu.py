@@ -276,3 +276,47 @@ def test_vector_kernels_16_byte_and_scalar_agree(precision, monkeypatch):
         assert st["converged"], (flag, st)
         out.append(rho)
     assert np.abs(out[0] - out[1]).max() <= 1e-8 * np.abs(out[1]).max()
+
+
+@pytest.mark.parametrize("precision", ["float64", "float32"])
+def test_preconditioned_solve_same_solution_fewer_iterations(precision):
+    """Right preconditioning by the cube-diagonal local operator (A43G_SOLVE_PRECONDITION): the
+    returned X is the solution of the original system (its true residual with the oracle's FP64
+    action below twice the tolerance), its densities equal the unpreconditioned solve's, and it
+    takes fewer iterations."""
+    w = workloads.make("periodic8_8atoms_s2x2x1")
+    E, k = complex(-0.3, 0.1), np.array([0.1, 0.0, 0.2])
+    p = gf.construct_Green_function(w.geometry)
+    gf.update_potential(p, w.Vcell, w.mats, w.offsets, layout="cells")
+    gf.update_energy_parameter(p, E, w.dVol)
+    gf.update_phases(p, k)
+    stream = torch.cuda.Stream()
+    opts = dict(tolerance=1e-10, max_iterations=3000, precision=precision, check_every=1, stream=stream)
+    st0, rho0 = green_action.solve(p, **opts)
+    X = torch.zeros((p.nnzb, 2, 64, 64), device="cuda", dtype=torch.float64)
+    st1, rho1 = green_action.solve(p, X=X, precondition=True, **opts)
+    assert st0["converged"] and st1["converged"], (st0, st1)
+    assert st1["iterations"] < st0["iterations"], (st0["iterations"], st1["iterations"])
+    assert np.abs(rho1 - rho0).max() <= 1e-7 * np.abs(rho0).max()
+    we = workloads.Workload(w.name, w.geometry, w.Vcell, w.mats, w.offsets, E, k, w.dVol, 1e-10, 3000)
+    assert true_residual(p, we, X.cpu().numpy()) <= 2e-10
+
+
+def test_preconditioned_batched_matches_individual():
+    """Batched and individual preconditioned solves (each pair with its own energy in the
+    preconditioner's scaling) give the same densities."""
+    w = workloads.make("periodic4_1atom")
+    p = gf.construct_Green_function(w.geometry)
+    gf.update_potential(p, w.Vcell, w.mats, w.offsets, layout="cells")
+    energies = [complex(-0.4, 0.08), complex(-0.2, 0.2), complex(0.1, 0.15)]
+    kpoints = [np.zeros(3), np.array([0.1, 0.0, 0.2]), np.array([0.25, 0.25, 0.0])]
+    opts = dict(tolerance=1e-10, max_iterations=2000, precision="float64", check_every=1, precondition=True)
+    stream = torch.cuda.Stream()
+    stats, rho = green_action.solve_batched(p, energies, kpoints, w.dVol, want_rho=True, batch=2, stream=stream, **opts)
+    for i, (E, k) in enumerate(zip(energies, kpoints)):
+        assert stats[i]["converged"], (i, stats[i])
+        gf.update_energy_parameter(p, E, w.dVol)
+        gf.update_phases(p, k)
+        st, rho0 = green_action.solve(p, stream=stream, **opts)
+        assert st["converged"], (i, st)
+        assert np.abs(rho[i] - rho0).max() <= 1e-8 * np.abs(rho0).max()
