@@ -37,8 +37,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 WORKLOAD = "periodic16_64atoms_s2x2x2"
-PRECONDITION = False         # right preconditioning by the cube-diagonal local operator (off: it did
-                             # not lower the iteration counts on the atom-rich cells measured)
+PRECONDITION = True          # right preconditioning by the cube-diagonal local operator
 TOLERANCE = 1e-8
 MAX_ITERATIONS = 1500
 STRIDE = 37            # walk of the 128 pairs: 37*i mod 128 (37 is coprime with 128)
