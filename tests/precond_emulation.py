@@ -1,13 +1,17 @@
 """The cube-diagonal preconditioner in a CPU emulation: FP64 tfQMR (numpy, per column) with the
 reference's own FP64 action (oracle/_ref), without and with right preconditioning, on the
-CPU-runnable cell (periodic 4^3 cubes, one atom, one source cube) at five energies.  Two
+CPU-runnable cell (periodic 4^3 cubes, one atom, one source cube) at five energies, or with
+--cell NAME --energy E [--kpoint kx,ky,kz] on another workload at one energy (the 8^3 cell with
+eight atoms and one source cube: hours, at some 0.6 s per action).  Two
 preconditioners: the exact local operator of each cube (finite differences inside the cube plus
 its potential minus E, inverted densely) and the separable one the solver uses (the cube's mean
 potential, applied through the eigenbases of the 4-point difference matrices).  Prints the
 iterations to 1e-9 and the true residuals.  No GPU; a few minutes:
 
     python tests/precond_emulation.py
+    python tests/precond_emulation.py --cell periodic8_8atoms_s1x1x1 --energy=-0.3+0.25j --kpoint 0.1,0,0.2
 """
+import argparse
 import json
 import os
 import sys
@@ -21,9 +25,37 @@ from fp32_floor_emulation import setup, to_c, to_r  # noqa: E402
 from angstromcube_b200 import workloads  # noqa: E402
 
 
+def cell_setup(name, E, k):
+    import oracle
+    w = workloads.make(name)
+    r = oracle.RefGreen(w.geometry)
+    r.set_potential(w.Vcell)
+    r.set_atom_matrices(w.mats, w.offsets)
+    r.set_energy(E, w.dVol)
+    r.set_kpoint(np.asarray(k, dtype=np.float64))
+    ex = r.export()
+    ci = np.asarray(ex["colindx"], np.int64)
+    B = np.zeros((r.sizes["nnzb"], 64, 64), np.complex128)
+    for b in ex["subset"]:
+        B[b][np.arange(64), np.arange(64)] = 1.0
+    return w, r, ci, r.sizes["nCols"], B
+
+
 def main():
-    r, ci, ncols, B = setup()
-    w = workloads.make("periodic4_1atom")
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--cell", default=None)
+    ap.add_argument("--energy", type=complex, default=None)
+    ap.add_argument("--kpoint", default="0,0,0")
+    a = ap.parse_args()
+    energies = (complex(-0.3, 0.05), complex(-0.0066, 0.081), complex(-0.6, 0.49), complex(-0.99, 0.117),
+                complex(-0.2, 0.02))
+    kpt = [float(v) for v in a.kpoint.split(",")]
+    if a.cell:
+        energies = (a.energy if a.energy is not None else complex(-0.3, 0.05),)
+        w, r, ci, ncols, B = cell_setup(a.cell, energies[0], kpt)
+    else:
+        r, ci, ncols, B = setup()
+        w = workloads.make("periodic4_1atom")
     ex = r.export()
     veff = ex["veff_index"]
     A64 = lambda z: to_c(r.action(to_r(z, np.float64)))
@@ -69,8 +101,7 @@ def main():
         R = B - A64(X)
         return float(np.sqrt(dot(R, R).real).max())
 
-    for E in (complex(-0.3, 0.05), complex(-0.0066, 0.081), complex(-0.6, 0.49), complex(-0.99, 0.117),
-              complex(-0.2, 0.02)):
+    for E in energies:
         r.set_energy(E, w.dVol)
         Minv = {}
 
