@@ -28,6 +28,7 @@ per energy, the 8^3 cell with eight atoms in tens of minutes per method (some 0.
     python tests/krylov_emulation.py --cell periodic8_8atoms_s1x1x1 --energy=-0.3+0.25j \\
         --kpoint 0.1,0,0.2 --methods idr4
     python tests/krylov_emulation.py --fp32 --kpoint 0,0,0 --methods cocg,idr4 --limit 300
+    python tests/krylov_emulation.py --fp32 --replace 1e-2 --methods idr4,idr8 --limit 1500
 """
 import argparse
 import json
@@ -53,6 +54,7 @@ class System:
         self.cplx = np.complex64 if fp32 else np.complex128
         self.B = self.B64.astype(self.cplx)
         self.history = []                            # (applications, true, recursive) in FP32 runs
+        self.replacements = []                       # (applications, true, recursive) at replacements
         self.fp32 = fp32
         ex = self.ref.export()
         veff = ex["veff_index"]
@@ -148,7 +150,12 @@ def bicgstab(S, tol, limit):
     return X, {}
 
 
-def idr(S, tol, limit, s=4, kappa=0.7):
+def idr(S, tol, limit, s=4, kappa=0.7, replace=None):
+    """IDR(s); with replace (FP32 runs): the solution is accumulated in FP64 and, at the start of
+    a cycle once the recursive residual has fallen by the factor replace since the last
+    replacement (or below the tolerance), replaced by the true residual of that solution computed
+    with the FP64 action; the run ends when that true residual is below the tolerance.  G, U and
+    P^H G are kept across a replacement."""
     B, dot, col = S.B, S.dot, S.col
     rng = np.random.default_rng(7)
     P = [rng.standard_normal(B.shape) + 1j * rng.standard_normal(B.shape) for _ in range(s)]
@@ -164,7 +171,18 @@ def idr(S, tol, limit, s=4, kappa=0.7):
     for i in range(s):
         Mm[..., i, i] = 1.0
     om = np.ones(shp, complex)
+    X64 = np.zeros(B.shape, np.complex128); ref = 1.0
     while S.applications < limit:
+        if replace is not None:
+            rn = S.norm(R)
+            if rn <= replace * ref or rn <= tol:
+                X64 = X64 + X.astype(np.complex128); X = np.zeros_like(B)
+                Rt = S.B64 - to_c(S.ref.action(to_r(X64, np.float64)))
+                S.replacements.append((S.applications, S.norm(Rt), rn))
+                ref = S.replacements[-1][1]
+                if ref <= tol:
+                    break
+                R = Rt.astype(S.cplx)
         f = np.stack([dot(P[i], R) for i in range(s)], axis=-1)
         for k in range(s):
             c = np.zeros(shp + (s - k,), complex)    # M[k:, k:] c = f[k:], forward substitution
@@ -189,7 +207,7 @@ def idr(S, tol, limit, s=4, kappa=0.7):
                 Mm[..., i, k] = dot(P[i], Gk)
             beta = f[..., k] / Mm[..., k, k]
             R = R - col(beta) * Gk; X = X + col(beta) * Uk
-            if S.converged(X, S.norm(R), tol):
+            if replace is None and S.converged(X, S.norm(R), tol):
                 return X, {}
             for i in range(k + 1, s):
                 f[..., i] -= beta * Mm[..., i, k]
@@ -199,8 +217,11 @@ def idr(S, tol, limit, s=4, kappa=0.7):
         rho = np.abs(tr) / (np.sqrt(tt) * np.sqrt(dot(R, R).real))
         om = np.where(rho < kappa, o * kappa / np.maximum(rho, 1e-300), o)
         X = X + col(om) * v; R = R - col(om) * t
-        if S.converged(X, S.norm(R), tol):
+        if replace is None and S.converged(X, S.norm(R), tol):
             break
+    if replace is not None:
+        return X64 + X.astype(np.complex128), {"fp64_applications": len(S.replacements),
+                                               "replacements": S.replacements}
     return X, {}
 
 
@@ -229,6 +250,9 @@ def main():
                     help="complex64 vectors, the reference's FP32 action and an FP32 preconditioner "
                          "(inner products in FP64); prints the true and recursive residuals every "
                          "10 applications and the lowest true residual (the floor)")
+    ap.add_argument("--replace", type=float, default=None,
+                    help="with --fp32, IDR(s) with residual replacement: the FP64 true residual "
+                         "replaces the recursive one once that has fallen by this factor")
     a = ap.parse_args()
     k = [float(v) for v in a.kpoint.split(",")]
     out = {"cell": a.cell, "E": [a.energy.real, a.energy.imag], "k": k}
@@ -237,11 +261,11 @@ def main():
         if m == "cocg" and any(k):
             raise SystemExit("cocg needs the Gamma point (the action is complex symmetric only there)")
         if m.startswith("idr"):
-            X, extra = idr(S, a.tolerance, a.limit, s=int(m[3:]))
+            X, extra = idr(S, a.tolerance, a.limit, s=int(m[3:]), replace=a.replace if a.fp32 else None)
         else:
             X, extra = {"tfqmr": tfqmr, "bicgstab": bicgstab, "cocg": cocg}[m](S, a.tolerance, a.limit)
         out[m] = dict(applications=S.applications, true_residual=S.true_residual(X), **extra)
-        if a.fp32:
+        if a.fp32 and S.history:
             out[m]["floor"] = min(t for _, t, _ in S.history)
             out[m]["history"] = [(n, float("%.3g" % t), float("%.3g" % r)) for n, t, r in S.history]
         print(json.dumps({m: out[m]}), flush=True)
