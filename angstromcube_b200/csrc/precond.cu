@@ -154,7 +154,18 @@ k_precond(T *y, T const *x, uint32_t nnzb, int32_t const *__restrict__ veff, uin
 
 } // namespace
 
-bool precond_setup(GreenPlan const &hp, DevicePlan const &dp, BlockPreconditioner &pc, cudaStream_t st) {
+namespace {
+bool upload_tables(BlockPreconditioner &pc, std::vector<double> const &t64, std::vector<float> const &t32,
+                   cudaStream_t st) {
+    size_t const n = t64.size();
+    A43G_CUDA_TRY(cudaMemcpyAsync(pc.tab64.ptr, t64.data(), n*8, cudaMemcpyHostToDevice, st));
+    A43G_CUDA_TRY(cudaMemcpyAsync(pc.tab32.ptr, t32.data(), n*4, cudaMemcpyHostToDevice, st));
+    A43G_CUDA_TRY(cudaStreamSynchronize(st));      // the host tables go out of scope
+    return true;
+}
+} // namespace
+
+int precond_setup(GreenPlan const &hp, DevicePlan const &dp, BlockPreconditioner &pc, cudaStream_t st) {
     (void)dp;
     double lam[3][4];
     for (int d = 0; d < 3; ++d) {
@@ -188,17 +199,21 @@ bool precond_setup(GreenPlan const &hp, DevicePlan const &dp, BlockPreconditione
                 for (int yy = 0; yy < 4; ++yy)
                     for (int xx = 0; xx < 4; ++xx) {
                         int const p = (z*4 + yy)*4 + xx;
-                        std::complex<double> const v = 1.0/std::complex<double>(lam[2][z] + lam[1][yy] + lam[0][xx] + vbar[c] - Er, -Ei);
+                        std::complex<double> const den(lam[2][z] + lam[1][yy] + lam[0][xx] + vbar[c] - Er, -Ei);
+                        std::complex<double> const v = (0.0 == std::abs(den)) ? std::complex<double>(INFINITY, 0) : 1.0/den;
+                        if (!std::isfinite(v.real()) || !std::isfinite(v.imag()) ||
+                            !std::isfinite(float(v.real())) || !std::isfinite(float(v.imag()))) {
+                            set_error("preconditioner: the cube model is singular at this energy "
+                                      "(a real energy on one of its eigenvalues)");
+                            return A43G_ERR_ARGUMENT;
+                        }
                         size_t const o = ((size_t(pr)*(ncells + 1) + c)*64 + p)*2;
                         t64[o] = v.real(); t64[o + 1] = v.imag();
                         t32[o] = float(v.real()); t32[o + 1] = float(v.imag());
                     }
     }
-    if (!pc.tab64.alloc(n*8) || !pc.tab32.alloc(n*4)) return false;
-    A43G_CUDA_TRY(cudaMemcpyAsync(pc.tab64.ptr, t64.data(), n*8, cudaMemcpyHostToDevice, st));
-    A43G_CUDA_TRY(cudaMemcpyAsync(pc.tab32.ptr, t32.data(), n*4, cudaMemcpyHostToDevice, st));
-    A43G_CUDA_TRY(cudaStreamSynchronize(st));      // the host tables go out of scope
-    return true;
+    if (!pc.tab64.alloc(n*8) || !pc.tab32.alloc(n*4)) return A43G_ERR_MEMORY;
+    return upload_tables(pc, t64, t32, st) ? A43G_OK : A43G_ERR_CUDA;
 }
 
 template <typename T>

@@ -12,6 +12,7 @@
 #pragma once
 
 #include "device.cuh"
+#include "../../include/a43g.h"
 
 namespace a43g {
 
@@ -26,8 +27,10 @@ struct BlockPreconditioner {
 };
 
 // the eigenbases and the scaling tables of the plan's current potential and energies (each pair
-// of a batch plan with its own energy); the last cell slot serves blocks without potential
-bool precond_setup(GreenPlan const &hp, DevicePlan const &dp, BlockPreconditioner &pc, cudaStream_t st);
+// of a batch plan with its own energy); the last cell slot serves blocks without potential.
+// Returns an a43g status: A43G_ERR_ARGUMENT when a cube model is singular or its inverse not
+// finite (a real energy on one of its eigenvalues), A43G_ERR_MEMORY, A43G_ERR_CUDA.
+int precond_setup(GreenPlan const &hp, DevicePlan const &dp, BlockPreconditioner &pc, cudaStream_t st);
 
 // y = M^-1 x over the blocks of the active sources (active == nullptr: every block); y may be x
 template <typename T>

@@ -1291,7 +1291,7 @@ int solve(GreenPlan &hp, DevicePlan &dp, SolverWorkspace &ws, a43g_solve_options
         if (trace) { set_error("a traced solve takes no preconditioner"); return A43G_ERR_UNSUPPORTED; }
         size_t const nr = size_t(dp.nnzb)*kBlk;
         if (!ws.PT64.alloc(nr*8) || (mixed && !ws.PT32.alloc(nr*4))) return A43G_ERR_MEMORY;
-        if (!precond_setup(hp, dp, ws.pc, st)) return A43G_ERR_CUDA;
+        if (int const rc = precond_setup(hp, dp, ws.pc, st); A43G_OK != rc) return rc;
     }
     // projector scratch for both precisions before the iteration is captured (no allocation
     // may happen inside a stream capture)

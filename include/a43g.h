@@ -83,7 +83,9 @@ enum {
                                     mean potential minus E, applied by three 4-point transforms and a
                                     scaling (no reference counterpart: the reference's action reports
                                     has_preconditioner() false); residuals and the solution are those
-                                    of the original system.  Not with a43g_solve_traced */
+                                    of the original system.  Not with a43g_solve_traced; refused
+                                    (A43G_ERR_ARGUMENT) where a cube model is singular, a real
+                                    energy on one of its eigenvalues */
 };
 
 typedef struct {
